@@ -1,0 +1,480 @@
+"""UW12 energy + Fock benchmark (one JSON line on rank 0).
+
+Workload: the unrestricted medium system N=500 AO, M=1500 DF, R=2000 RI,
+n_alpha=40, n_beta=38 (all-electron), scale factors (1.0, 0.5), seeded
+synthetic inputs (three-index N(0,1) exp(-|m-n|/30), metrics B B^T + 1e-6 I,
+S-orthonormal orbitals), FP64 throughout.  One step = one energy + Fock
+evaluation (uw12 form_fock with the integrals resident in HBM).
+
+``value`` is seconds per evaluation for the whole job (max-over-ranks device
+time / evaluations of all ranks); ranks evaluate independent molecules
+(weak scaling, no collective on the data path).  ``e2e`` is the same metric
+through the C-ABI from pinned host buffers: integral upload, on-device metric
+and overlap eigensolves, evaluation and Fock read-back per step.
+
+``--impl reference`` times the CPU restatement of libuw12's algorithm (the
+oracle; libuw12 itself cannot be built here) on the host cores for the same
+workload: every heavy loop of the reference (its parallel_for /
+parallel_sum / parallel_sum_2d over aux functions and orbital pairs) runs a
+bounded number of iterations and its time is extrapolated to the full count.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "UW12 energy+Fock s/eval (FP64 plain GPU path vs reference CPU algorithm)"
+CONFIGS = {
+    # name: N, M, R, n_occ per spin, decay
+    "c0": (24, 84, 116, (5,), 8.0),
+    "c1": (500, 1500, 2000, (40, 38), 30.0),
+    "c2": (1200, 3600, 4800, (100,), 30.0),
+}
+
+
+# --------------------------------------------------------------------------
+# canonical FLOPs (algorithmic work of one evaluation, dense-GEMM FLOPs)
+# --------------------------------------------------------------------------
+def canonical_flops(N, M, R, occ, act, same_spin=True, fock=True):
+    Rp = N + R
+    Np = N * (N + 1) // 2
+    tot = 0.0
+    for o, a in zip(occ, act):
+        f = 2 * (2 * N * N * o * M + 2 * N * o * M * M)          # T1, W and V
+        f += 2 * (2 * R * N * a * M + 2 * R * a * M * M)         # T2
+        f += 2 * (2 * a * N * o * M)                             # T3
+        f += 4 * Np * M                                          # 2-el direct
+        f += 2 * M * M * a * o                                   # 4-el t
+        f += 2 * Rp * Rp * a * M + 2 * M * M * Rp * a            # 3-el X_AB
+        if fock:
+            f += 2 * N * o * M * M + 2 * N * N * o * M + (2 * N * N * a * M if a < o else 0)
+            f += 2 * N * o * M * M + 2 * N * N * o * M + (2 * N * N * a * M if a < o else 0)
+            f += 4 * M ** 3 + 2 * (Np + R * N) * M * M + 2 * Rp * Rp * N * M + 2 * N * N * Rp * M
+        if same_spin:
+            f += 4 * N * N * a * M + 2 * N * a * M * M + 2 * a * a * N * M
+            f += 4 * (a * o) ** 2 * M + (4 * N * o * a * o * M + 2 * N * N * a * a * o
+                                          + (2 * N * N * o * o * a if a < o else 0) if fock else 0)
+            f += 4 * Rp * a * a * o * M + 2 * Rp * a * a * o
+            if fock:
+                f += 2 * Rp * Rp * a * M + 2 * (4 * N * Rp * a * o * M + 2 * N * N * Rp * a * o
+                                                 + 2 * a * o * M * M)
+                f += 4 * Rp * a * a * N * M + 2 * N * N * Rp * a * a
+        tot += f
+    return float(tot)
+
+
+# --------------------------------------------------------------------------
+# clocks
+# --------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# inputs
+# --------------------------------------------------------------------------
+def _tag(name: str) -> int:
+    import hashlib
+    return int.from_bytes(hashlib.sha256(name.encode()).digest()[:8], "little")
+
+
+def make_device_inputs(cfg, seed, device):
+    """Three-index tensors generated on the device (library synth kernel);
+    metrics, overlap and orbitals generated with torch on the device."""
+    import torch
+    import libuw12_b200 as L
+    N, M, R, occ, L_decay = cfg
+    np_ = N * (N + 1) // 2
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    t = {}
+    for nm in ("W3", "V3", "WV3"):
+        t[nm] = torch.empty(np_ * M, dtype=torch.float64, device=device)
+        L.synth_three_index(t[nm].data_ptr(), 0, N, 0, M, seed, _tag(nm), L_decay)
+    for nm in ("W3_ri", "V3_ri"):
+        t[nm] = torch.empty(R * N * M, dtype=torch.float64, device=device)
+        L.synth_three_index(t[nm].data_ptr(), 1, N, R, M, seed, _tag(nm), L_decay)
+    for nm in ("W2", "V2", "WV2"):
+        B = torch.randn(M, M, dtype=torch.float64, device=device, generator=g) / math.sqrt(M)
+        J = B @ B.T + 1e-6 * torch.eye(M, dtype=torch.float64, device=device)
+        t[nm] = (0.5 * (J + J.T)).contiguous()  # symmetric: row/column-major agree
+    n = N + R
+    A = torch.randn(n, n, dtype=torch.float64, device=device, generator=g) / math.sqrt(n)
+    S = A @ A.T + 0.1 * torch.eye(n, dtype=torch.float64, device=device)
+    t["S"] = (0.5 * (S + S.T)).contiguous()
+    Sao = t["S"][:N, :N]
+    orbs = []
+    for s, o in enumerate(occ):
+        C = torch.randn(N, o, dtype=torch.float64, device=device, generator=g)
+        G = C.T @ Sao @ C
+        Lc = torch.linalg.cholesky(0.5 * (G + G.T))
+        C = torch.linalg.solve_triangular(Lc, C.T, upper=False).T
+        orbs.append(np.asfortranarray(C.cpu().numpy()))
+    torch.cuda.synchronize(device)
+    per = 2.0 if len(occ) == 1 else 1.0
+    occs = [np.full(o, per) for o in occ]
+    return t, orbs, occs
+
+
+def fp64_peak_tflops(device) -> float:
+    """cuBLAS DGEMM 8192^3 burst (best of 5), the FP64 roofline denominator."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    for _ in range(2):
+        a @ b
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def read_profile_traffic():
+    """Per-launch DRAM traffic of the GEMM kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "dgemm_dmma_traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_gflop:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+# --------------------------------------------------------------------------
+# CPU baseline (oracle restatement of libuw12's algorithm, sampled loops)
+# --------------------------------------------------------------------------
+def cpu_reference_eval(host, cfg, s_os, s_ss, max_iters):
+    """One sampled evaluation of the reference algorithm; returns
+    (extrapolated seconds per eval, measured seconds, description)."""
+    from oracle import uw12_oracle as O
+    N, M, R, occ, _ = cfg
+    samp = O.Sampler(max_iters)
+    t0 = time.perf_counter()
+    W = O.BaseIntegrals(host["W3"], host["W2"], host["W3_ri"])
+    V = O.BaseIntegrals(host["V3"], host["V2"], host["V3_ri"])
+    WV = O.BaseIntegrals(host["WV3"], host["WV2"])
+    absp = O.calculate_abs_projectors(host["S"], N, R)
+    t_setup = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    O.uw12_fock(W, V, WV, absp, host["orbitals"], host["occ"], list(occ), s_os, s_ss,
+                sampler=samp)
+    t_eval = time.perf_counter() - t1
+    return t_eval + samp.extra_seconds, t_setup, t_eval, samp
+
+
+def host_inputs_numpy(cfg, seed):
+    from oracle import synth
+    N, M, R, occ, Ld = cfg
+    h = {}
+    for nm in ("W3", "V3", "WV3"):
+        h[nm] = synth.fast_three_index(seed, nm, N * (N + 1) // 2, M, synth.ao_damping(N, Ld))
+    for nm in ("W3_ri", "V3_ri"):
+        h[nm] = synth.fast_three_index(seed, nm, R * N, M, synth.ri_damping(N, R, Ld))
+    for nm in ("W2", "V2", "WV2"):
+        h[nm] = synth.metric(seed, nm, M)
+    h["S"] = synth.overlap(seed, N, R)
+    h["orbitals"] = [synth.orbitals(seed, h["S"][:N, :N], o, f"C{s}") for s, o in enumerate(occ)]
+    per = 2.0 if len(occ) == 1 else 1.0
+    h["occ"] = [np.full(o, per) for o in occ]
+    return h
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    cfg = CONFIGS[args.config]
+    N, M, R, occ, _ = cfg
+    cores = os.cpu_count() or 1
+    t_gen = time.perf_counter()
+    host = host_inputs_numpy(cfg, 11)
+    t_gen = time.perf_counter() - t_gen
+    small = host_inputs_numpy(CONFIGS["c0"], 11)
+    for _ in range(args.warmup):  # warm BLAS threads / imports on the small case
+        cpu_reference_eval(small, CONFIGS["c0"], 1.0, 0.5, None)
+    vals, setups = [], []
+    for _ in range(args.steps):
+        v, ts, te, samp = cpu_reference_eval(host, cfg, args.s_os, args.s_ss, args.ref_iters)
+        vals.append(v)
+        setups.append(ts)
+    value = float(np.median(vals))
+    sample = (f"{args.config}: every reference loop over aux functions / orbital pairs capped at "
+              f"{args.ref_iters} iterations, loop time extrapolated to full counts; setup "
+              f"(3 metric eigensolves + ABS projectors, {np.median(setups):.1f} s) excluded")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "s/eval",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded, numpy PCG64 streams)",
+        "config": config_dict(args),
+        "cpu_baseline": {"value": value, "unit": "s/eval", "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "s/eval", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "notes": f"input generation {t_gen:.1f} s (untimed)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(args):
+    N, M, R, occ, Ld = CONFIGS[args.config]
+    return {"workload": f"uw12 energy+Fock {args.config}: N={N} AO, M={M} DF, R={R} RI, "
+                        f"n_occ={list(occ)} ({'UHF' if len(occ) == 2 else 'closed shell'}), "
+                        f"all-electron, scales (s_os, s_ss)=({args.s_os}, {args.s_ss})",
+            "n_ao": N, "n_df": M, "n_ri": R, "n_occ": list(occ), "decay": Ld,
+            "precision": "fp64", "l2": "inputs (28.6 GB at c1) exceed the 126 MB L2"}
+
+
+# --------------------------------------------------------------------------
+# main arm
+# --------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c1", choices=sorted(CONFIGS))
+    ap.add_argument("--s-os", dest="s_os", type=float, default=1.0)
+    ap.add_argument("--s-ss", dest="s_ss", type=float, default=0.5)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--ref-iters", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=device)
+
+    import libuw12_b200 as L
+    L.lib()
+    stream = torch.cuda.current_stream(device)
+    L.set_stream(stream.cuda_stream)
+
+    cfg = CONFIGS[args.config]
+    N, M, R, occ, _ = cfg
+    act = list(occ)
+    t, orbs, occs = make_device_inputs(cfg, 11 + rank, device)
+    peak = fp64_peak_tflops(device)
+
+    W = L.setup_base_integrals(t["W3"].data_ptr(), t["W2"].data_ptr(), t["W3_ri"].data_ptr(),
+                               n_ao=N, n_df=M, n_ri=R, device=True)
+    V = L.setup_base_integrals(t["V3"].data_ptr(), t["V2"].data_ptr(), t["V3_ri"].data_ptr(),
+                               n_ao=N, n_df=M, n_ri=R, device=True)
+    WV = L.setup_base_integrals(t["WV3"].data_ptr(), t["WV2"].data_ptr(), None, n_ao=N, n_df=M,
+                                device=True)
+    A = L.setup_abs_projectors(t["S"].data_ptr(), N, R, device=True)
+    fock_dev = torch.empty(N * N * len(occ), dtype=torch.float64, device=device)
+    indirect = abs(args.s_ss) > 4 * np.finfo(float).eps
+
+    def step():
+        return L.form_fock(W, V, WV, A, orbs, occs, act, indirect, True, args.s_os, args.s_ss,
+                           fock_out=fock_dev.data_ptr())[0]
+
+    for _ in range(args.warmup):
+        energy = step()
+    torch.cuda.synchronize(device)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    L.profile_enable(True)
+    n0 = L.launch_count()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        energy = step()
+    ev1.record(stream)
+    torch.cuda.synchronize(device)
+    if world > 1:
+        dist.barrier()
+    launches = L.launch_count() - n0
+    prof = L.profile_read()
+    L.profile_enable(False)
+    clk = clocks.stop()
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    if world > 1:
+        tt = torch.tensor([elapsed], dtype=torch.float64, device=device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed = float(tt.item())
+    s_per_eval = elapsed / (args.steps * world)
+
+    # ---- end to end through the C-ABI from pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        host = {k: torch.empty(v.numel(), dtype=torch.float64, pin_memory=True)
+                for k, v in t.items()}
+        for k, v in t.items():
+            host[k].copy_(v.reshape(-1))
+        h2d = sum(v.numel() * 8 for v in t.values()) + sum(o.nbytes for o in orbs)
+        d2h = N * N * len(occ) * 8
+        # free the device inputs and handles so the e2e arm holds its own copies
+        for h in (W, V, WV, A):
+            h.close()
+        del t
+        torch.cuda.empty_cache()
+        np_ = N * (N + 1) // 2
+        hp = {k: v.numpy() for k, v in host.items()}
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            We = L.setup_base_integrals(hp["W3"].reshape((np_, M), order="F"),
+                                        hp["W2"].reshape((M, M)),
+                                        hp["W3_ri"].reshape((R * N, M), order="F"))
+            Ve = L.setup_base_integrals(hp["V3"].reshape((np_, M), order="F"),
+                                        hp["V2"].reshape((M, M)),
+                                        hp["V3_ri"].reshape((R * N, M), order="F"))
+            WVe = L.setup_base_integrals(hp["WV3"].reshape((np_, M), order="F"),
+                                         hp["WV2"].reshape((M, M)))
+            Ae = L.setup_abs_projectors(hp["S"].reshape((N + R, N + R)), N, R)
+            e_e2e, fock_host = L.uw12_fock(We, Ve, WVe, Ae, orbs, occs, act, args.s_os, args.s_ss)
+            for h in (We, Ve, WVe, Ae):
+                h.close()
+        torch.cuda.synchronize(device)
+        te = time.perf_counter() - t0
+        if world > 1:
+            tt = torch.tensor([te], dtype=torch.float64, device=device)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        e2e = {"value": te / (args.e2e_steps * world), "unit": "s/eval",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "includes": "H2D of all integrals from pinned host memory, metric/overlap "
+                           "eigensolves, evaluation, Fock D2H",
+               "energy_rel_diff_vs_value_arm": abs(e_e2e - energy) / abs(energy)}
+
+    # ---- CPU baseline on a bounded sample (rank 0, N = 1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.no_e2e:
+        hostd = {k: hp[k] for k in hp}
+        hb = {"W3": hostd["W3"].reshape((N * (N + 1) // 2, M), order="F"),
+              "V3": hostd["V3"].reshape((N * (N + 1) // 2, M), order="F"),
+              "WV3": hostd["WV3"].reshape((N * (N + 1) // 2, M), order="F"),
+              "W3_ri": hostd["W3_ri"].reshape((R * N, M), order="F"),
+              "V3_ri": hostd["V3_ri"].reshape((R * N, M), order="F"),
+              "W2": hostd["W2"].reshape((M, M)), "V2": hostd["V2"].reshape((M, M)),
+              "WV2": hostd["WV2"].reshape((M, M)), "S": hostd["S"].reshape((N + R, N + R)),
+              "orbitals": orbs, "occ": occs}
+        v, ts, te_, samp = cpu_reference_eval(hb, cfg, args.s_os, args.s_ss, args.ref_iters)
+        cpu = {"value": v, "unit": "s/eval", "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"{args.config}: reference loops over aux functions / orbital pairs capped "
+                         f"at {args.ref_iters} iterations each, loop time extrapolated "
+                         f"(measured {te_:.1f} s); numpy/OpenBLAS on all host threads"}
+
+    flops = canonical_flops(N, M, R, occ, act, same_spin=indirect, fock=True)
+    gemm_tf = prof["flops"] / (prof["ms"] / 1e3) / 1e12 if prof["ms"] > 0 else None
+    bpg = read_profile_traffic()
+    avg_launch_flops = prof["flops"] / max(1, prof["launches"])
+    roof = {"bound": "tensor", "kernel": "dgemm_dmma (mma.sync m16n8k4 f64)",
+            "achieved": gemm_tf, "peak": peak, "unit": "TFLOP/s",
+            "frac": (gemm_tf / peak) if gemm_tf else None,
+            "peak_source": "cuBLAS DGEMM 8192^3 burst measured in this run (MEASURED_PEAKS.json "
+                           "has no FP64 figure)",
+            "traffic": (bpg * avg_launch_flops / 1e9) if bpg else None,
+            "launches": prof["launches"], "kernel_ms": prof["ms"],
+            "share_of_step": (prof["ms"] / 1e3) / elapsed if elapsed > 0 else None}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": s_per_eval, "unit": "s/eval", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generators; integrals generated on device)",
+            "config": config_dict(args),
+            "tflops_canonical": flops / s_per_eval / 1e12,
+            "canonical_flops_per_eval": flops,
+            "energy": energy,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,146 @@
+/*
+ * uw12_c.h -- C-ABI of the B200-native UW12 energy + Fock library.
+ *
+ * Plain pointers and sizes only.  Every entry point returns a status code
+ * (UW12C_OK on success); the message of the last failure on the calling host
+ * thread is available through uw12c_last_error().  Status codes map onto the
+ * exception classes libuw12 throws: UW12C_ERR_RUNTIME <-> std::runtime_error
+ * (user-input errors), UW12C_ERR_LOGIC <-> std::logic_error (shape errors).
+ *
+ * Layouts are libuw12's (column-major throughout):
+ *   X3     packed three-index integrals (rho sigma|A): n_ao(n_ao+1)/2 x n_df,
+ *          row i(i+1)/2 + j holds the pair (i, j <= i);
+ *   X2     two-index metric (A|B): n_df x n_df;
+ *   X3_ri  three-index RI integrals (mu rho|A): (n_ri * n_ao) x n_df, row
+ *          nu + n_ri * mu;
+ *   S      overlap of the combined AO+RI space, AO functions first;
+ *   C      orbitals n_ao x (n_orb * n_spin), alpha columns then beta;
+ *   occ    occupations packed alpha || beta;
+ *   fock   n_ao x (n_ao * n_spin), spin blocks side by side.
+ * All compute runs on the current CUDA device; there is no CPU fallback.
+ */
+#ifndef UW12_C_H
+#define UW12_C_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UW12C_OK 0
+#define UW12C_ERR_RUNTIME 1
+#define UW12C_ERR_LOGIC 2
+#define UW12C_ERR_CUDA 3
+#define UW12C_ERR_ALLOC 4
+#define UW12C_ERR_INVALID 5
+
+#define UW12C_MEM_HOST 0
+#define UW12C_MEM_DEVICE 1
+
+typedef struct uw12c_integrals uw12c_integrals;
+typedef struct uw12c_abs uw12c_abs;
+
+/* Status of the last call on this host thread; copies its message into buf
+ * (truncated, NUL-terminated) when buf != NULL. */
+int uw12c_last_error(char* buf, size_t len);
+
+/* Library version string (static storage). */
+const char* uw12c_version(void);
+
+/* Replaces uw12::setup_base_integrals(X3, X2, X3_ri, n_ao, n_df, n_ri, copy)
+ * (libuw12.hpp:42-50, libuw12.cpp:22-36) and, with X3_ri == NULL, the no-RI
+ * overload (libuw12.hpp:65-71, libuw12.cpp:38-49).  The tensors are copied to
+ * the device (mem_kind says where the caller's pointers live) and the metric
+ * is diagonalised there: P2 = Q pinv(Lambda), df_vals = Lambda
+ * (src/integrals/base_integrals.cpp:155-166). */
+int uw12c_integrals_create(const double* X3, const double* X2, const double* X3_ri, size_t n_ao,
+                           size_t n_df, size_t n_ri, int mem_kind, uw12c_integrals** out);
+int uw12c_integrals_destroy(uw12c_integrals* h);
+/* BaseIntegrals::get_number_ao/df/ri (base_integrals.hpp:209-216). */
+int uw12c_integrals_dims(const uw12c_integrals* h, size_t* n_ao, size_t* n_df, size_t* n_ri);
+/* BaseIntegrals::get_df_vals (base_integrals.hpp:168-171): n_df values, host. */
+int uw12c_integrals_df_vals(const uw12c_integrals* h, double* out);
+
+/* Replaces uw12::setup_abs_projectors(S, n_ao, n_ri) (libuw12.hpp:81,
+ * libuw12.cpp:51-56 -> src/three_electron/ri_utils.hpp:45-74). */
+int uw12c_abs_create(const double* S, size_t n_ao, size_t n_ri, int mem_kind, uw12c_abs** out);
+int uw12c_abs_destroy(uw12c_abs* h);
+/* The four ABSProjectors blocks (ri_utils.hpp:20-29) copied to host buffers
+ * (any may be NULL): ri_ri R x R, ri_ao R x N, ao_ri N x R, ao_ao N x N. */
+int uw12c_abs_blocks(const uw12c_abs* h, double* ri_ri, double* ri_ao, double* ao_ri,
+                     double* ao_ao);
+
+/* Replaces uw12::form_fock (src/uw12.hpp:129-142, src/uw12.cpp:22-119) with
+ * per-spin orbital blocks: C_alpha (n_ao x n_orb[0]) and, for n_spin == 2,
+ * C_beta, each with leading dimension ldc[s]; occ[s] holds n_occ[s]
+ * occupations.  energy receives the total, terms (may be NULL) the two-,
+ * three- and four-electron energies, fock (may be NULL) the Fock matrix. */
+int uw12c_form_fock(const uw12c_integrals* W, const uw12c_integrals* V,
+                    const uw12c_integrals* WV, const uw12c_abs* abs, size_t n_ao, size_t n_spin,
+                    const double* const* C, const size_t* ldc, const size_t* n_orb,
+                    const double* const* occ, const size_t* n_occ, const size_t* n_active,
+                    int indirect_term, int calculate_fock, double scale_opp_spin,
+                    double scale_same_spin, size_t print_level, double* energy, double* terms,
+                    double* fock, int fock_mem_kind);
+
+/* Replaces uw12::uw12_fock(double* fock, ...) (libuw12.hpp:155-167,
+ * libuw12.cpp:184-214) in its raw-pointer form: C is the setup_orbitals
+ * buffer (n_ao x n_orb*n_spin), occ the setup_occupations buffer
+ * (n_occ_alpha [+ n_occ_beta] values; n_occ_beta ignored for n_spin == 1),
+ * n_active has n_spin entries.  The same-spin term runs when
+ * |scale_same_spin| > 4 DBL_EPSILON (libuw12.cpp:138). */
+int uw12c_fock(double* fock, const uw12c_integrals* W, const uw12c_integrals* V,
+               const uw12c_integrals* WV, const uw12c_abs* abs, const double* C, size_t n_ao,
+               size_t n_orb, size_t n_spin, const double* occ, size_t n_occ_alpha,
+               size_t n_occ_beta, const size_t* n_active, double scale_opp_spin,
+               double scale_same_spin, size_t print_level, double* energy);
+
+/* Replaces uw12::uw12_energy (libuw12.hpp:134-144, libuw12.cpp:156-182). */
+int uw12c_energy(const uw12c_integrals* W, const uw12c_integrals* V, const uw12c_integrals* WV,
+                 const uw12c_abs* abs, const double* C, size_t n_ao, size_t n_orb, size_t n_spin,
+                 const double* occ, size_t n_occ_alpha, size_t n_occ_beta,
+                 const size_t* n_active, double scale_opp_spin, double scale_same_spin,
+                 size_t print_level, double* energy);
+
+/* Execution control (no counterpart in libuw12, whose calls are synchronous
+ * CPU code): the CUDA stream (a cudaStream_t, NULL = legacy default) used by
+ * this host thread, the byte budget for chunked intermediates (0 = 45% of free
+ * device memory), and counters of this library's kernel launches and of the
+ * FP64 GEMM kernel's time and FLOPs (events recorded around each launch while
+ * profiling is on). */
+int uw12c_set_stream(void* stream);
+int uw12c_set_memory_budget(size_t bytes);
+unsigned long long uw12c_launch_count(void);
+int uw12c_profile_enable(int on);
+int uw12c_profile_read(unsigned long long* gemm_launches, double* gemm_ms, double* gemm_flops);
+
+/* The FP64 tensor-core GEMM engine on device pointers (no counterpart in
+ * libuw12, which calls BLAS dgemm through Armadillo):
+ *   C[bo] = alpha * sum_{r1<nbr1, r2<nbr2} op(A) op(B) + beta * C[bo],
+ * A m x k with element (i, kk) at A[i + lda*kk] (a_kcontig = 0) or
+ * A[kk + lda*i]; B k x n with (kk, j) at B[kk + ldb*j] (b_ncontig = 0) or
+ * B[j + ldb*kk]; C column-major.  Output batch (bo1 < nbo1, bo2 < nbo2)
+ * offsets A/B/C by so = {sAo1, sAo2, sBo1, sBo2, sCo1, sCo2}; reduction batch
+ * (r1, r2) offsets A/B by sr = {sAr1, sAr2, sBr1, sBr2}.  split = 0 chooses
+ * split-K automatically. */
+int uw12c_dgemm(long long m, long long n, long long k, double alpha, const double* A,
+                long long lda, int a_kcontig, const double* B, long long ldb, int b_ncontig,
+                double beta, double* C, long long ldc, long long nbo1, long long nbo2,
+                const long long* so, long long nbr1, long long nbr2, const long long* sr,
+                int split);
+
+/* Deterministic synthetic three-index tensors written on the device (no
+ * counterpart in libuw12; benchmark input generation).  Element e of the
+ * stream (seed, tag) is the Box-Muller normal of two SplitMix64 draws, times
+ * exp(-|p - q| / decay) for the element's index pair (p, q).
+ * kind 0: packed AO tensor n_ao(n_ao+1)/2 x n_df; kind 1: RI tensor
+ * (n_ri*n_ao) x n_df. */
+int uw12c_synth_three_index(double* out_device, int kind, size_t n_ao, size_t n_ri, size_t n_df,
+                            unsigned long long seed, unsigned long long tag, double decay);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* UW12_C_H */

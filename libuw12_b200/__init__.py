@@ -1,0 +1,391 @@
+"""libuw12_b200 -- B200-native UW12 energy + Fock behind libuw12's API.
+
+The compute lives in ``_lib/libuw12_b200.so`` (hand-written sm_100a CUDA
+behind the C-ABI declared in ``include/uw12_c.h``).  This module is a thin
+ctypes mirror of libuw12's public C++ API (``libuw12.hpp``) for Python
+callers and tests: ``setup_base_integrals``, ``setup_abs_projectors``,
+``setup_orbitals``, ``setup_occupations``, ``uw12_energy``, ``uw12_fock`` and
+the lower-level ``form_fock`` (``src/uw12.hpp:129-142``).  There is no CPU
+path: if the shared library is missing or no CUDA device is usable, calls
+raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+__all__ = [
+    "UW12Error", "UW12RuntimeError", "UW12LogicError", "UW12CudaError",
+    "BaseIntegrals", "ABSProjectors", "setup_base_integrals", "setup_abs_projectors",
+    "setup_orbitals", "setup_occupations", "uw12_energy", "uw12_fock", "form_fock",
+    "lib", "library_path",
+]
+
+_HERE = Path(__file__).resolve().parent
+_LIB_PATH = _HERE / "_lib" / "libuw12_b200.so"
+_lib = None
+
+OK, ERR_RUNTIME, ERR_LOGIC, ERR_CUDA, ERR_ALLOC, ERR_INVALID = range(6)
+MEM_HOST, MEM_DEVICE = 0, 1
+
+
+class UW12Error(Exception):
+    """Base class of errors reported by the CUDA library."""
+
+
+class UW12RuntimeError(UW12Error, RuntimeError):
+    """libuw12 raises std::runtime_error (user-input errors)."""
+
+
+class UW12LogicError(UW12Error, ValueError):
+    """libuw12 raises std::logic_error (shape errors)."""
+
+
+class UW12CudaError(UW12Error):
+    """CUDA / cuSOLVER failure or invalid argument."""
+
+
+def library_path() -> Path:
+    return _LIB_PATH
+
+
+def lib():
+    """Loads the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not _LIB_PATH.exists():
+        raise ImportError(
+            f"{_LIB_PATH} not found: build it with `python -m libuw12_b200.build` "
+            "(there is no CPU fallback)")
+    L = ctypes.CDLL(str(_LIB_PATH))
+    c_d = ctypes.c_double
+    c_sz = ctypes.c_size_t
+    P = ctypes.c_void_p
+    PD = ctypes.POINTER(c_d)
+    PSZ = ctypes.POINTER(c_sz)
+    L.uw12c_last_error.argtypes = [ctypes.c_char_p, c_sz]
+    L.uw12c_last_error.restype = ctypes.c_int
+    L.uw12c_version.restype = ctypes.c_char_p
+    L.uw12c_integrals_create.argtypes = [P, P, P, c_sz, c_sz, c_sz, ctypes.c_int,
+                                         ctypes.POINTER(P)]
+    L.uw12c_integrals_destroy.argtypes = [P]
+    L.uw12c_integrals_dims.argtypes = [P, PSZ, PSZ, PSZ]
+    L.uw12c_integrals_df_vals.argtypes = [P, PD]
+    L.uw12c_abs_create.argtypes = [P, c_sz, c_sz, ctypes.c_int, ctypes.POINTER(P)]
+    L.uw12c_abs_destroy.argtypes = [P]
+    L.uw12c_abs_blocks.argtypes = [P, P, P, P, P]
+    L.uw12c_form_fock.argtypes = [P, P, P, P, c_sz, c_sz, ctypes.POINTER(P), PSZ, PSZ,
+                                  ctypes.POINTER(P), PSZ, PSZ, ctypes.c_int, ctypes.c_int, c_d,
+                                  c_d, c_sz, PD, PD, P, ctypes.c_int]
+    L.uw12c_fock.argtypes = [P, P, P, P, P, P, c_sz, c_sz, c_sz, P, c_sz, c_sz, PSZ, c_d, c_d,
+                             c_sz, PD]
+    L.uw12c_energy.argtypes = [P, P, P, P, P, c_sz, c_sz, c_sz, P, c_sz, c_sz, PSZ, c_d, c_d,
+                               c_sz, PD]
+    L.uw12c_set_stream.argtypes = [P]
+    L.uw12c_set_memory_budget.argtypes = [c_sz]
+    L.uw12c_launch_count.restype = ctypes.c_ulonglong
+    L.uw12c_profile_enable.argtypes = [ctypes.c_int]
+    L.uw12c_profile_read.argtypes = [ctypes.POINTER(ctypes.c_ulonglong), PD, PD]
+    LL = ctypes.c_longlong
+    L.uw12c_dgemm.argtypes = [LL, LL, LL, c_d, P, LL, ctypes.c_int, P, LL, ctypes.c_int, c_d, P,
+                              LL, LL, LL, ctypes.POINTER(LL), LL, LL, ctypes.POINTER(LL),
+                              ctypes.c_int]
+    L.uw12c_synth_three_index.argtypes = [P, ctypes.c_int, c_sz, c_sz, c_sz, ctypes.c_ulonglong,
+                                          ctypes.c_ulonglong, c_d]
+    _lib = L
+    return L
+
+
+def _check(status: int):
+    if status == OK:
+        return
+    buf = ctypes.create_string_buffer(1024)
+    lib().uw12c_last_error(buf, 1024)
+    msg = buf.value.decode(errors="replace")
+    if status == ERR_RUNTIME:
+        raise UW12RuntimeError(msg)
+    if status == ERR_LOGIC:
+        raise UW12LogicError(msg)
+    raise UW12CudaError(f"status {status}: {msg}")
+
+
+def _fptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else ctypes.c_void_p(0)
+
+
+def _col_major(a, rows: int, cols: int) -> np.ndarray:
+    a = np.asarray(a, dtype=np.float64)
+    if a.ndim == 1:
+        a = a.reshape((rows, cols), order="F")
+    if a.shape != (rows, cols):
+        raise UW12LogicError(f"expected a {rows} x {cols} matrix, got {a.shape}")
+    return np.asfortranarray(a)
+
+
+class BaseIntegrals:
+    """Device-resident ``BaseIntegrals`` (src/integrals/base_integrals.hpp:46-293)."""
+
+    def __init__(self, handle: ctypes.c_void_p):
+        self._h = handle
+        n_ao, n_df, n_ri = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_size_t()
+        _check(lib().uw12c_integrals_dims(self._h, ctypes.byref(n_ao), ctypes.byref(n_df),
+                                          ctypes.byref(n_ri)))
+        self.n_ao, self.n_df, self.n_ri = n_ao.value, n_df.value, n_ri.value
+
+    def get_number_ao(self) -> int:
+        return self.n_ao
+
+    def get_number_df(self) -> int:
+        return self.n_df
+
+    def get_number_ri(self) -> int:
+        return self.n_ri
+
+    def get_df_vals(self) -> np.ndarray:
+        out = np.empty(self.n_df)
+        _check(lib().uw12c_integrals_df_vals(self._h, out.ctypes.data_as(
+            ctypes.POINTER(ctypes.c_double))))
+        return out
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().uw12c_integrals_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ABSProjectors:
+    """Device-resident ABS+ projectors (src/three_electron/ri_utils.hpp:20-29)."""
+
+    def __init__(self, handle: ctypes.c_void_p, n_ao: int, n_ri: int):
+        self._h = handle
+        self.n_ao, self.n_ri = n_ao, n_ri
+
+    @property
+    def handle(self):
+        return self._h
+
+    def blocks(self):
+        """(s_inv_ri_ri, s_inv_ri_ao, s_inv_ao_ri, s_inv_ao_ao) as host arrays."""
+        N, R = self.n_ao, self.n_ri
+        rr = np.zeros((R, R), order="F")
+        ra = np.zeros((R, N), order="F")
+        ar = np.zeros((N, R), order="F")
+        aa = np.zeros((N, N), order="F")
+        _check(lib().uw12c_abs_blocks(self._h, _fptr(rr), _fptr(ra), _fptr(ar), _fptr(aa)))
+        return rr, ra, ar, aa
+
+    def close(self):
+        if self._h:
+            lib().uw12c_abs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def setup_base_integrals(X3, X2, X3_ri=None, n_ao: Optional[int] = None,
+                         n_df: Optional[int] = None, n_ri: int = 0,
+                         device: bool = False) -> BaseIntegrals:
+    """``uw12::setup_base_integrals`` (libuw12.hpp:42-71).
+
+    With ``device=True`` the arguments are raw device pointers (ints) and the
+    sizes must be given; otherwise they are host arrays (column-major).
+    """
+    h = ctypes.c_void_p()
+    if device:
+        if n_ao is None or n_df is None:
+            raise UW12LogicError("n_ao and n_df are required for device pointers")
+        st = lib().uw12c_integrals_create(ctypes.c_void_p(X3), ctypes.c_void_p(X2),
+                                          ctypes.c_void_p(X3_ri or 0), n_ao, n_df,
+                                          n_ri if X3_ri else 0, MEM_DEVICE, ctypes.byref(h))
+        _check(st)
+        return BaseIntegrals(h)
+    X2 = np.asarray(X2, dtype=np.float64)
+    if n_df is None:
+        n_df = X2.shape[0]
+    X3 = np.asarray(X3, dtype=np.float64)
+    if n_ao is None:
+        rows = X3.shape[0] if X3.ndim == 2 else X3.size // n_df
+        n_ao = int((np.sqrt(8 * rows + 1) - 1) / 2)
+    np_ = n_ao * (n_ao + 1) // 2
+    X3 = _col_major(X3, np_, n_df)
+    X2 = _col_major(X2, n_df, n_df)
+    if X3_ri is not None:
+        X3_ri = np.asarray(X3_ri, dtype=np.float64)
+        if not n_ri:
+            rows = X3_ri.shape[0] if X3_ri.ndim == 2 else X3_ri.size // n_df
+            n_ri = rows // n_ao
+        X3_ri = _col_major(X3_ri, n_ri * n_ao, n_df)
+    st = lib().uw12c_integrals_create(_fptr(X3), _fptr(X2), _fptr(X3_ri) if X3_ri is not None
+                                      else ctypes.c_void_p(0), n_ao, n_df,
+                                      n_ri if X3_ri is not None else 0, MEM_HOST, ctypes.byref(h))
+    _check(st)
+    return BaseIntegrals(h)
+
+
+def setup_abs_projectors(S, n_ao: int, n_ri: int, device: bool = False) -> ABSProjectors:
+    """``uw12::setup_abs_projectors`` (libuw12.hpp:81)."""
+    h = ctypes.c_void_p()
+    if device:
+        st = lib().uw12c_abs_create(ctypes.c_void_p(S), n_ao, n_ri, MEM_DEVICE, ctypes.byref(h))
+    else:
+        S = _col_major(S, n_ao + n_ri, n_ao + n_ri)
+        st = lib().uw12c_abs_create(_fptr(S), n_ao, n_ri, MEM_HOST, ctypes.byref(h))
+    _check(st)
+    return ABSProjectors(h, n_ao, n_ri)
+
+
+def setup_orbitals(C, n_ao: int, n_orb: int, n_spin: int) -> List[np.ndarray]:
+    """``uw12::setup_orbitals`` (libuw12.cpp:58-77): alpha columns then beta."""
+    if n_spin not in (1, 2):
+        raise UW12RuntimeError("Number of spin channels must be 1 or 2")
+    C1 = _col_major(C, n_ao, n_orb * n_spin)
+    if n_spin == 1:
+        return [C1]
+    return [np.asfortranarray(C1[:, :n_orb]), np.asfortranarray(C1[:, n_orb:])]
+
+
+def setup_occupations(occ, n_occ_alpha: int, n_occ_beta: Optional[int] = None):
+    """``uw12::setup_occupations`` closed (n_occ) and open (n_alpha, n_beta) forms
+    (libuw12.cpp:79-112)."""
+    occ = np.asarray(occ, dtype=np.float64).reshape(-1)
+    if n_occ_beta is None:
+        return [occ[:n_occ_alpha].copy()]
+    return [occ[:n_occ_alpha].copy(), occ[n_occ_alpha:n_occ_alpha + n_occ_beta].copy()]
+
+
+def _nearly_zero(x: float) -> bool:
+    return abs(x) <= 4 * np.finfo(np.float64).eps
+
+
+def form_fock(W: BaseIntegrals, V: BaseIntegrals, WV: BaseIntegrals, abs_p: ABSProjectors,
+              orbitals: Sequence[np.ndarray], occupations: Sequence[np.ndarray],
+              n_active: Sequence[int], indirect_term: bool, calculate_fock: bool,
+              scale_opp_spin: float, scale_same_spin: float, print_level: int = 0,
+              fock_out=None) -> Tuple[float, Optional[List[np.ndarray]], Tuple[float, float, float]]:
+    """``uw12::form_fock`` (src/uw12.hpp:129-142).
+
+    Returns ``(energy, fock, (E2, E3, E4))`` with ``fock`` a list of n_ao x n_ao
+    arrays per spin (None when ``calculate_fock`` is false).  ``fock_out`` may
+    be a device pointer (int) receiving the n_ao x n_ao*n_spin Fock matrix.
+    """
+    n_spin = len(orbitals)
+    if n_spin < 1 or n_spin > 2:
+        raise UW12LogicError("invalid number of spin channels")
+    if len(occupations) != n_spin:
+        if len(occupations) < 1 or len(occupations) > 2:
+            raise UW12LogicError("invalid number of spin channels")
+        raise UW12RuntimeError("Different number of spin channels for orbitals and occupations")
+    if len(n_active) != n_spin:
+        if len(n_active) < 1 or len(n_active) > 2:
+            raise UW12LogicError("invalid number of spin channels")
+        raise UW12RuntimeError("Different number of spin channels in n_active and orbitals")
+    n_ao = W.n_ao
+    Cs = [np.asfortranarray(np.asarray(c, dtype=np.float64)) for c in orbitals]
+    for c in Cs:
+        if c.ndim != 2 or c.shape[0] != n_ao:
+            raise UW12RuntimeError("Inconsistent number of atomic orbitals")
+    occs = [np.ascontiguousarray(np.asarray(o, dtype=np.float64).reshape(-1)) for o in occupations]
+    P = ctypes.c_void_p
+    c_ptrs = (P * n_spin)(*[_fptr(c) for c in Cs])
+    ldc = (ctypes.c_size_t * n_spin)(*[max(1, c.shape[0]) for c in Cs])
+    norb = (ctypes.c_size_t * n_spin)(*[c.shape[1] for c in Cs])
+    o_ptrs = (P * n_spin)(*[_fptr(o) for o in occs])
+    nocc = (ctypes.c_size_t * n_spin)(*[o.size for o in occs])
+    nact = (ctypes.c_size_t * n_spin)(*[int(a) for a in n_active])
+    energy = ctypes.c_double()
+    terms = (ctypes.c_double * 3)()
+    fock = None
+    if fock_out is not None:
+        fptr, fmem = ctypes.c_void_p(fock_out), MEM_DEVICE
+    elif calculate_fock:
+        fock = np.zeros((n_ao, n_ao * n_spin), order="F")
+        fptr, fmem = _fptr(fock), MEM_HOST
+    else:
+        fptr, fmem = ctypes.c_void_p(0), MEM_HOST
+    st = lib().uw12c_form_fock(W.handle, V.handle, WV.handle, abs_p.handle, n_ao, n_spin, c_ptrs,
+                               ldc, norb, o_ptrs, nocc, nact, int(bool(indirect_term)),
+                               int(bool(calculate_fock)), float(scale_opp_spin),
+                               float(scale_same_spin), int(print_level), ctypes.byref(energy),
+                               terms, fptr, fmem)
+    _check(st)
+    focks = None
+    if fock is not None:
+        focks = [np.array(fock[:, s * n_ao:(s + 1) * n_ao]) for s in range(n_spin)]
+    return energy.value, focks, (terms[0], terms[1], terms[2])
+
+
+def uw12_fock(W, V, WV, abs_p, orbitals, occ, n_active, scale_opp_spin, scale_same_spin,
+              print_level: int = 0) -> Tuple[float, np.ndarray]:
+    """``uw12::uw12_fock`` (libuw12.hpp:155-167): returns (energy, fock) with
+    fock of shape n_ao x (n_ao * n_spin)."""
+    indirect = not _nearly_zero(scale_same_spin)
+    e, f, _ = form_fock(W, V, WV, abs_p, orbitals, occ, n_active, indirect, True, scale_opp_spin,
+                        scale_same_spin, print_level)
+    return e, np.concatenate(f, axis=1)
+
+
+def uw12_energy(W, V, WV, abs_p, orbitals, occ, n_active, scale_opp_spin, scale_same_spin,
+                print_level: int = 0) -> float:
+    """``uw12::uw12_energy`` (libuw12.hpp:134-144)."""
+    indirect = not _nearly_zero(scale_same_spin)
+    return form_fock(W, V, WV, abs_p, orbitals, occ, n_active, indirect, False, scale_opp_spin,
+                     scale_same_spin, print_level)[0]
+
+
+def set_stream(stream_ptr: int):
+    _check(lib().uw12c_set_stream(ctypes.c_void_p(stream_ptr)))
+
+
+def set_memory_budget(nbytes: int):
+    _check(lib().uw12c_set_memory_budget(int(nbytes)))
+
+
+def launch_count() -> int:
+    return int(lib().uw12c_launch_count())
+
+
+def profile_enable(on: bool):
+    _check(lib().uw12c_profile_enable(1 if on else 0))
+
+
+def profile_read():
+    n = ctypes.c_ulonglong()
+    ms = ctypes.c_double()
+    fl = ctypes.c_double()
+    _check(lib().uw12c_profile_read(ctypes.byref(n), ctypes.byref(ms), ctypes.byref(fl)))
+    return {"launches": n.value, "ms": ms.value, "flops": fl.value}
+
+
+def dgemm(m, n, k, alpha, A, lda, a_kcontig, B, ldb, b_ncontig, beta, C, ldc, nbo1=1, nbo2=1,
+          so=(0, 0, 0, 0, 0, 0), nbr1=1, nbr2=1, sr=(0, 0, 0, 0), split=0):
+    """The FP64 tensor-core GEMM engine on device pointers (see uw12_c.h)."""
+    LLa = ctypes.c_longlong * 6
+    LLr = ctypes.c_longlong * 4
+    _check(lib().uw12c_dgemm(m, n, k, alpha, ctypes.c_void_p(A), lda, int(a_kcontig),
+                             ctypes.c_void_p(B), ldb, int(b_ncontig), beta, ctypes.c_void_p(C),
+                             ldc, nbo1, nbo2, LLa(*so), nbr1, nbr2, LLr(*sr), int(split)))
+
+
+def synth_three_index(out_ptr: int, kind: int, n_ao: int, n_ri: int, n_df: int, seed: int,
+                      tag: int, decay: float):
+    _check(lib().uw12c_synth_three_index(ctypes.c_void_p(out_ptr), kind, n_ao, n_ri, n_df,
+                                         seed & (2**64 - 1), tag & (2**64 - 1), decay))

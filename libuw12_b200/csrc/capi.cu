@@ -1,0 +1,354 @@
+// extern "C" boundary (include/uw12_c.h): argument checks that mirror
+// libuw12's exceptions, status codes, per-thread error text and stream.
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/uw12_c.h"
+#include "engine.cuh"
+#include "gemm_f64.cuh"
+
+namespace uw12b {
+
+void synth_three_index(double* out, int kind, size_t n_ao, size_t n_ri, size_t n_df,
+                       unsigned long long seed, unsigned long long tag, double decay);
+
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+thread_local cudaStream_t g_stream = nullptr;
+std::atomic<size_t> g_budget{0};
+thread_local int g_last_status = UW12C_OK;
+thread_local std::string g_last_msg;
+}  // namespace
+
+void note_launch(const char* file, int line) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  const cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(kErrCuda, std::string("kernel launch failed: ") + cudaGetErrorString(e) + " (" +
+                              file + ":" + std::to_string(line) + ")");
+  }
+}
+unsigned long long launch_count() { return g_launches.load(); }
+cudaStream_t current_stream() { return g_stream; }
+void set_current_stream(cudaStream_t s) { g_stream = s; }
+
+}  // namespace uw12b
+
+struct uw12c_integrals {
+  std::unique_ptr<uw12b::IntegralsHandle> h;
+};
+struct uw12c_abs {
+  std::unique_ptr<uw12b::AbsHandle> h;
+};
+
+namespace {
+
+using uw12b::Error;
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    uw12b::g_last_status = UW12C_OK;
+    uw12b::g_last_msg.clear();
+    return UW12C_OK;
+  } catch (const Error& e) {
+    uw12b::g_last_status = e.code;
+    uw12b::g_last_msg = e.what();
+  } catch (const std::bad_alloc&) {
+    uw12b::g_last_status = UW12C_ERR_ALLOC;
+    uw12b::g_last_msg = "host allocation failed";
+  } catch (const std::exception& e) {
+    uw12b::g_last_status = UW12C_ERR_RUNTIME;
+    uw12b::g_last_msg = e.what();
+  } catch (...) {
+    uw12b::g_last_status = UW12C_ERR_RUNTIME;
+    uw12b::g_last_msg = "unknown error";
+  }
+  return uw12b::g_last_status;
+}
+
+void need(bool ok, const char* msg) {
+  if (!ok) throw Error(UW12C_ERR_INVALID, msg);
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    UW12_CUDA(cudaGetDevice(&prev));
+    if (prev != dev) UW12_CUDA(cudaSetDevice(dev));
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != prev && prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+bool nearly_zero(double v) { return std::fabs(v) <= 4.0 * DBL_EPSILON; }  // utils.hpp:186-189
+
+void run_form_fock(const uw12c_integrals* W, const uw12c_integrals* V, const uw12c_integrals* WV,
+                   const uw12c_abs* abs, size_t n_ao, size_t n_spin, const double* const* C,
+                   const size_t* ldc, const size_t* n_orb, const double* const* occ,
+                   const size_t* n_occ, const size_t* n_active, int indirect, int calc,
+                   double s_os, double s_ss, size_t print_level, double* energy, double* terms,
+                   double* fock, int fock_mem) {
+  need(W && V && WV && abs && W->h && V->h && WV->h && abs->h, "null handle");
+  need(C && ldc && n_orb && occ && n_occ && n_active, "null orbital/occupation argument");
+  need(fock_mem == UW12C_MEM_HOST || fock_mem == UW12C_MEM_DEVICE, "bad fock_mem_kind");
+  // form_fock / spin_channels (uw12.cpp:40-50, utils.hpp:198-205)
+  if (n_spin < 1 || n_spin > 2) uw12b::throw_logic("invalid number of spin channels");
+  uw12b::FockRequest rq;
+  rq.W = W->h.get();
+  rq.V = V->h.get();
+  rq.WV = WV->h.get();
+  rq.abs = abs->h.get();
+  rq.n_spin = static_cast<int>(n_spin);
+  rq.n_ao = n_ao;
+  for (size_t s = 0; s < n_spin; ++s) {
+    // occupation_weighted_orbitals (utils.hpp:289-310), freeze_core (:235-253)
+    for (size_t k = 0; k < n_occ[s]; ++k) {
+      need(occ[s] != nullptr, "null occupation vector");
+      if (!(occ[s][k] > 0.0)) uw12b::throw_runtime("occupations must be positive");
+    }
+    if (n_occ[s] > n_orb[s])
+      uw12b::throw_logic("Cannot have submatix with more columns than parent matrix");
+    if (n_active[s] > n_occ[s])
+      uw12b::throw_logic("Cannot have submatix with more columns than parent matrix");
+    if (n_occ[s]) need(C[s] != nullptr, "null orbital block");
+    if (ldc[s] < n_ao) uw12b::throw_logic("orbital leading dimension smaller than n_ao");
+    rq.C.push_back(C[s]);
+    rq.ldc.push_back(ldc[s]);
+    rq.n_orb.push_back(n_orb[s]);
+    rq.occ.push_back(occ[s]);
+    rq.n_occ.push_back(n_occ[s]);
+    rq.n_active.push_back(n_active[s]);
+  }
+  const auto& w = *rq.W;
+  const auto& v = *rq.V;
+  const auto& wv = *rq.WV;
+  // Integrals::number_ao_orbitals (integrals.cpp:394-402)
+  if (w.n_ao != n_ao || v.n_ao != n_ao || wv.n_ao != n_ao)
+    uw12b::throw_runtime("Inconsistent number of atomic orbitals");
+  if (w.n_ri == 0 || v.n_ri == 0) uw12b::throw_runtime("J3_ri_0 not stored");
+  // calculate_xab accumulates (M_W x M_V) components into an n_df(V)^2 matrix
+  // (direct_utils.cpp:75-79, 107-111): libuw12 only supports equal df sizes.
+  if (w.n_df != v.n_df) uw12b::throw_logic("addition: incompatible matrix dimensions");
+  if (w.n_ri != v.n_ri || rq.abs->n_ri != w.n_ri || rq.abs->n_ao != n_ao)
+    uw12b::throw_logic("ABS projectors and RI integrals are of incompatible sizes");
+  if (w.device != v.device || w.device != wv.device || w.device != rq.abs->device)
+    throw Error(UW12C_ERR_INVALID, "handles live on different devices");
+  rq.indirect = indirect != 0;
+  rq.calc_fock = calc != 0;
+  rq.s_os = s_os;
+  rq.s_ss = s_ss;
+  rq.print_level = print_level;
+  rq.energy = energy;
+  rq.terms = terms;
+  rq.fock = fock;
+  rq.fock_device = fock_mem == UW12C_MEM_DEVICE;
+  rq.mem_budget = uw12b::g_budget.load();
+  DeviceGuard dg(w.device);
+  uw12b::form_fock(rq);
+}
+
+void run_public(double* fock, const uw12c_integrals* W, const uw12c_integrals* V,
+                const uw12c_integrals* WV, const uw12c_abs* abs, const double* C, size_t n_ao,
+                size_t n_orb, size_t n_spin, const double* occ, size_t n_occ_alpha,
+                size_t n_occ_beta, const size_t* n_active, double s_os, double s_ss,
+                size_t print_level, double* energy, bool calc) {
+  // setup_orbitals / setup_occupations (libuw12.cpp:58-112)
+  if (n_spin != 1 && n_spin != 2) uw12b::throw_runtime("Number of spin channels must be 1 or 2");
+  need(n_active != nullptr, "null n_active");
+  const double* Cs[2] = {C, C ? C + n_ao * n_orb : nullptr};
+  const size_t ldc[2] = {n_ao, n_ao};
+  const size_t norb[2] = {n_orb, n_orb};
+  const double* occs[2] = {occ, occ ? occ + n_occ_alpha : nullptr};
+  const size_t nocc[2] = {n_occ_alpha, n_spin == 2 ? n_occ_beta : 0};
+  const bool indirect = !nearly_zero(s_ss);  // libuw12.cpp:138
+  run_form_fock(W, V, WV, abs, n_ao, n_spin, Cs, ldc, norb, occs, nocc, n_active,
+                indirect ? 1 : 0, calc ? 1 : 0, s_os, s_ss, print_level, energy, nullptr,
+                calc ? fock : nullptr, UW12C_MEM_HOST);
+}
+
+}  // namespace
+
+extern "C" {
+
+int uw12c_last_error(char* buf, size_t len) {
+  if (buf && len) {
+    std::strncpy(buf, uw12b::g_last_msg.c_str(), len - 1);
+    buf[len - 1] = '\0';
+  }
+  return uw12b::g_last_status;
+}
+
+const char* uw12c_version(void) { return "uw12-b200 0.1 (sm_100a, fp64 dmma)"; }
+
+int uw12c_integrals_create(const double* X3, const double* X2, const double* X3_ri, size_t n_ao,
+                           size_t n_df, size_t n_ri, int mem_kind, uw12c_integrals** out) {
+  return guarded([&] {
+    need(out != nullptr, "null output handle");
+    need(mem_kind == UW12C_MEM_HOST || mem_kind == UW12C_MEM_DEVICE, "bad mem_kind");
+    *out = nullptr;
+    auto h = std::make_unique<uw12c_integrals>();
+    h->h.reset(uw12b::integrals_create(X3, X2, X3_ri, n_ao, n_df, n_ri,
+                                       mem_kind == UW12C_MEM_DEVICE));
+    *out = h.release();
+  });
+}
+
+int uw12c_integrals_destroy(uw12c_integrals* h) {
+  return guarded([&] { delete h; });
+}
+
+int uw12c_integrals_dims(const uw12c_integrals* h, size_t* n_ao, size_t* n_df, size_t* n_ri) {
+  return guarded([&] {
+    need(h && h->h, "null handle");
+    if (n_ao) *n_ao = h->h->n_ao;
+    if (n_df) *n_df = h->h->n_df;
+    if (n_ri) *n_ri = h->h->n_ri;
+  });
+}
+
+int uw12c_integrals_df_vals(const uw12c_integrals* h, double* out) {
+  return guarded([&] {
+    need(h && h->h && out, "null argument");
+    std::memcpy(out, h->h->lam_host.data(), h->h->lam_host.size() * sizeof(double));
+  });
+}
+
+int uw12c_abs_create(const double* S, size_t n_ao, size_t n_ri, int mem_kind, uw12c_abs** out) {
+  return guarded([&] {
+    need(out != nullptr, "null output handle");
+    need(mem_kind == UW12C_MEM_HOST || mem_kind == UW12C_MEM_DEVICE, "bad mem_kind");
+    *out = nullptr;
+    auto h = std::make_unique<uw12c_abs>();
+    h->h.reset(uw12b::abs_create(S, n_ao, n_ri, mem_kind == UW12C_MEM_DEVICE));
+    *out = h.release();
+  });
+}
+
+int uw12c_abs_destroy(uw12c_abs* h) {
+  return guarded([&] { delete h; });
+}
+
+int uw12c_abs_blocks(const uw12c_abs* h, double* ri_ri, double* ri_ao, double* ao_ri,
+                     double* ao_ao) {
+  return guarded([&] {
+    need(h && h->h, "null handle");
+    const size_t N = h->h->n_ao, R = h->h->n_ri, n = N + R;
+    DeviceGuard dg(h->h->device);
+    cudaStream_t s = uw12b::current_stream();
+    auto block = [&](double* dst, size_t r0, size_t c0, size_t rows, size_t cols) {
+      if (!dst || !rows || !cols) return;
+      UW12_CUDA(cudaMemcpy2DAsync(dst, rows * sizeof(double), h->h->Sinv.get() + r0 + n * c0,
+                                  n * sizeof(double), rows * sizeof(double), cols,
+                                  cudaMemcpyDeviceToHost, s));
+    };
+    block(ri_ri, N, N, R, R);
+    block(ri_ao, N, 0, R, N);
+    block(ao_ri, 0, N, N, R);
+    block(ao_ao, 0, 0, N, N);
+    UW12_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int uw12c_form_fock(const uw12c_integrals* W, const uw12c_integrals* V,
+                    const uw12c_integrals* WV, const uw12c_abs* abs, size_t n_ao, size_t n_spin,
+                    const double* const* C, const size_t* ldc, const size_t* n_orb,
+                    const double* const* occ, const size_t* n_occ, const size_t* n_active,
+                    int indirect_term, int calculate_fock, double scale_opp_spin,
+                    double scale_same_spin, size_t print_level, double* energy, double* terms,
+                    double* fock, int fock_mem_kind) {
+  return guarded([&] {
+    run_form_fock(W, V, WV, abs, n_ao, n_spin, C, ldc, n_orb, occ, n_occ, n_active, indirect_term,
+                  calculate_fock, scale_opp_spin, scale_same_spin, print_level, energy, terms,
+                  fock, fock_mem_kind);
+  });
+}
+
+int uw12c_fock(double* fock, const uw12c_integrals* W, const uw12c_integrals* V,
+               const uw12c_integrals* WV, const uw12c_abs* abs, const double* C, size_t n_ao,
+               size_t n_orb, size_t n_spin, const double* occ, size_t n_occ_alpha,
+               size_t n_occ_beta, const size_t* n_active, double scale_opp_spin,
+               double scale_same_spin, size_t print_level, double* energy) {
+  return guarded([&] {
+    need(fock != nullptr, "null fock buffer");
+    run_public(fock, W, V, WV, abs, C, n_ao, n_orb, n_spin, occ, n_occ_alpha, n_occ_beta,
+               n_active, scale_opp_spin, scale_same_spin, print_level, energy, true);
+  });
+}
+
+int uw12c_energy(const uw12c_integrals* W, const uw12c_integrals* V, const uw12c_integrals* WV,
+                 const uw12c_abs* abs, const double* C, size_t n_ao, size_t n_orb, size_t n_spin,
+                 const double* occ, size_t n_occ_alpha, size_t n_occ_beta,
+                 const size_t* n_active, double scale_opp_spin, double scale_same_spin,
+                 size_t print_level, double* energy) {
+  return guarded([&] {
+    run_public(nullptr, W, V, WV, abs, C, n_ao, n_orb, n_spin, occ, n_occ_alpha, n_occ_beta,
+               n_active, scale_opp_spin, scale_same_spin, print_level, energy, false);
+  });
+}
+
+int uw12c_set_stream(void* stream) {
+  return guarded([&] { uw12b::set_current_stream(static_cast<cudaStream_t>(stream)); });
+}
+
+int uw12c_set_memory_budget(size_t bytes) {
+  return guarded([&] { uw12b::g_budget.store(bytes); });
+}
+
+unsigned long long uw12c_launch_count(void) { return uw12b::launch_count(); }
+
+int uw12c_profile_enable(int on) {
+  return guarded([&] {
+    if (on) uw12b::profile_reset();
+    uw12b::profile_enable(on != 0);
+  });
+}
+
+int uw12c_profile_read(unsigned long long* gemm_launches, double* gemm_ms, double* gemm_flops) {
+  return guarded([&] {
+    const uw12b::KernelStats k = uw12b::profile_read_gemm();
+    if (gemm_launches) *gemm_launches = k.launches;
+    if (gemm_ms) *gemm_ms = k.ms;
+    if (gemm_flops) *gemm_flops = k.flops;
+  });
+}
+
+int uw12c_dgemm(long long m, long long n, long long k, double alpha, const double* A,
+                long long lda, int a_kcontig, const double* B, long long ldb, int b_ncontig,
+                double beta, double* C, long long ldc, long long nbo1, long long nbo2,
+                const long long* so, long long nbr1, long long nbr2, const long long* sr,
+                int split) {
+  return guarded([&] {
+    uw12b::GemmDesc d;
+    d.m = m; d.n = n; d.k = k; d.alpha = alpha; d.beta = beta;
+    d.A = A; d.lda = lda; d.a_kcontig = a_kcontig != 0;
+    d.B = B; d.ldb = ldb; d.b_ncontig = b_ncontig != 0;
+    d.C = C; d.ldc = ldc;
+    d.nbo1 = nbo1; d.nbo2 = nbo2;
+    if (so) { d.sAo1 = so[0]; d.sAo2 = so[1]; d.sBo1 = so[2]; d.sBo2 = so[3]; d.sCo1 = so[4]; d.sCo2 = so[5]; }
+    d.nbr1 = nbr1; d.nbr2 = nbr2;
+    if (sr) { d.sAr1 = sr[0]; d.sAr2 = sr[1]; d.sBr1 = sr[2]; d.sBr2 = sr[3]; }
+    d.split = split;
+    need(m >= 0 && n >= 0 && k >= 0 && nbo1 >= 0 && nbo2 >= 0 && nbr1 >= 0 && nbr2 >= 0,
+         "negative size");
+    uw12b::gemm(d);
+  });
+}
+
+int uw12c_synth_three_index(double* out_device, int kind, size_t n_ao, size_t n_ri, size_t n_df,
+                            unsigned long long seed, unsigned long long tag, double decay) {
+  return guarded([&] {
+    need(out_device != nullptr, "null output");
+    uw12b::synth_three_index(out_device, kind, n_ao, n_ri, n_df, seed, tag, decay);
+  });
+}
+
+}  // extern "C"

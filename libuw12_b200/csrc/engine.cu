@@ -1,0 +1,771 @@
+// UW12 energy + Fock schedule on the device.
+//
+// Every contraction of libuw12's two-, three- and four-electron terms is
+// restated as a handful of large FP64 GEMMs (gemm_f64.cu); the reference's
+// per-aux-function parallel_for loops and per-orbital-pair parallel_sum_2d
+// loops become batched / reduction-batched GEMMs.  Notation: N = n_ao,
+// M = n_df, R = n_ri, R' = N + R, per spin o occupied, a active, c = o - a core.
+//
+//  T1  B1[mu + N k, A]  = sum_nu sq(J3_0[:,A])[mu,nu] Co[nu,k], then * P2
+//      (transformations.hpp:33-54, integrals.cpp:213-248)
+//  T2  Bri[nu + R i, A] = sum_mu J3ri_A[nu,mu] Ca[mu,i], then * P2
+//      (transformations.hpp:130-158, integrals.cpp:250-287)
+//  T3  B2[i + a k, A]   = sum_mu Ca[mu,i] B1[mu + N k, A]  (transformations.hpp:79-106)
+//  Wst rows p + R' j: p < N -> B1 orbital c+j, p >= N -> Bri orbital j (the
+//      AO-then-RI stacking of the ABS+ space), SV = (I_a (x) S^-1) Wst.
+//  X_AB = Wst_W^T SV_V replaces the four calculate_xab_component loops
+//      (direct_utils.cpp:31-133); t = B2_W^T B2_V, t~ = Lw t Lv
+//      (four_electron_utils.cpp:33-79).
+//  Fock pieces are accumulated unsymmetrised per spin and symmetrised once;
+//  libuw12 symmetrises the three- and four-electron terms and its
+//  two-electron pieces are symmetric by construction (utils.hpp:215-224).
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <string>
+
+#include "engine.cuh"
+#include "gemm_f64.cuh"
+#include "kernels.cuh"
+
+namespace uw12b {
+
+namespace {
+
+void solver_check(cusolverStatus_t st, const char* what) {
+  if (st != CUSOLVER_STATUS_SUCCESS)
+    throw Error(kErrCuda, std::string(what) + ": cusolver status " + std::to_string(int(st)));
+}
+
+void upload(double* dst, const double* src, size_t n, bool device_mem, cudaStream_t s) {
+  if (!n) return;
+  UW12_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double),
+                            device_mem ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+}
+
+// libuw12's linalg::is_symmetric(mat, 1e-10) (linalg.hpp:309-330), relative
+// to max(1, max|A|).
+void require_symmetric(const double* A, size_t n, const char* msg) {
+  cudaStream_t s = current_stream();
+  DevBuf st(2, s);
+  symmetry_stats(A, n, n, st.get());
+  double h[2];
+  UW12_CUDA(cudaMemcpyAsync(h, st.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+  UW12_CUDA(cudaStreamSynchronize(s));
+  if (!(h[0] <= 1e-10 * std::max(1.0, h[1]))) throw_logic(msg);
+}
+
+// Ascending eigenpairs of a symmetric n x n matrix, in place (A -> vectors).
+void eigh(double* A, size_t n, double* w) {
+  cudaStream_t s = current_stream();
+  cusolverDnHandle_t h = nullptr;
+  solver_check(cusolverDnCreate(&h), "cusolverDnCreate");
+  struct Guard { cusolverDnHandle_t h; ~Guard() { cusolverDnDestroy(h); } } guard{h};
+  solver_check(cusolverDnSetStream(h, s), "cusolverDnSetStream");
+  int lwork = 0;
+  solver_check(cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                           static_cast<int>(n), A, static_cast<int>(n), w, &lwork),
+               "cusolverDnDsyevd_bufferSize");
+  DevBuf work(static_cast<size_t>(std::max(lwork, 1)), s);
+  int* info = nullptr;
+  UW12_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&info), sizeof(int), s));
+  solver_check(cusolverDnDsyevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                static_cast<int>(n), A, static_cast<int>(n), w, work.get(), lwork,
+                                info),
+               "cusolverDnDsyevd");
+  UW12_LAUNCHED();
+  int hinfo = 0;
+  UW12_CUDA(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s));
+  UW12_CUDA(cudaFreeAsync(info, s));
+  UW12_CUDA(cudaStreamSynchronize(s));
+  if (hinfo != 0) throw_runtime("eigen-decomposition failed");
+}
+
+size_t auto_budget_doubles(size_t requested_bytes) {
+  size_t free_b = 0, total_b = 0;
+  UW12_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  size_t b = requested_bytes ? requested_bytes : static_cast<size_t>(0.45 * double(free_b));
+  b = std::max<size_t>(b, size_t(64) << 20);
+  return b / sizeof(double);
+}
+
+inline long long LL(size_t v) { return static_cast<long long>(v); }
+
+}  // namespace
+
+// --------------------------------------------------------------------------
+// handles
+// --------------------------------------------------------------------------
+IntegralsHandle* integrals_create(const double* X3, const double* X2, const double* X3_ri,
+                                  size_t n_ao, size_t n_df, size_t n_ri, bool device_mem) {
+  if (n_ao == 0) throw_runtime("Number of ao orbitals is zero");
+  if (n_df == 0) throw_runtime("Number of density-fitting basis functions is zero");
+  if (!X3 || !X2) throw Error(kErrInvalid, "null integral pointer");
+  if (X3_ri && n_ri == 0) throw_runtime("Three index ri integrals given but n_ri is zero");
+  auto h = new IntegralsHandle();
+  try {
+    UW12_CUDA(cudaGetDevice(&h->device));
+    cudaStream_t s = current_stream();
+    h->n_ao = n_ao;
+    h->n_df = n_df;
+    h->n_ri = X3_ri ? n_ri : 0;
+    const size_t np = packed_size(n_ao);
+    h->J3_0.alloc(np * n_df);
+    upload(h->J3_0.get(), X3, np * n_df, device_mem, s);
+    if (X3_ri) {
+      h->J3_ri_0.alloc(n_ri * n_ao * n_df);
+      upload(h->J3_ri_0.get(), X3_ri, n_ri * n_ao * n_df, device_mem, s);
+    }
+    h->P2.alloc(n_df * n_df);
+    upload(h->P2.get(), X2, n_df * n_df, device_mem, s);
+    require_symmetric(h->P2.get(), n_df, "matrix must be symmetric");
+    h->lam.alloc(n_df);
+    eigh(h->P2.get(), n_df, h->lam.get());
+    scale_pinv_cols(h->P2.get(), LL(n_df), h->lam.get(), 1e-10);
+    h->lam_host.resize(n_df);
+    UW12_CUDA(cudaMemcpyAsync(h->lam_host.data(), h->lam.get(), n_df * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+    UW12_CUDA(cudaStreamSynchronize(s));
+  } catch (...) {
+    delete h;
+    throw;
+  }
+  return h;
+}
+
+AbsHandle* abs_create(const double* S, size_t n_ao, size_t n_ri, bool device_mem) {
+  if (!S) throw Error(kErrInvalid, "null overlap pointer");
+  const size_t n = n_ao + n_ri;
+  if (n == 0) throw_runtime("Total number of basis functions is inconsistent");
+  auto h = new AbsHandle();
+  try {
+    UW12_CUDA(cudaGetDevice(&h->device));
+    cudaStream_t s = current_stream();
+    h->n_ao = n_ao;
+    h->n_ri = n_ri;
+    DevBuf vecs(n * n, s);
+    upload(vecs.get(), S, n * n, device_mem, s);
+    require_symmetric(vecs.get(), n, "matrix must be symmetric");
+    DevBuf vals(n, s);
+    eigh(vecs.get(), n, vals.get());
+    std::vector<double> lam(n);
+    UW12_CUDA(cudaMemcpyAsync(lam.data(), vals.get(), n * sizeof(double), cudaMemcpyDeviceToHost,
+                              s));
+    UW12_CUDA(cudaStreamSynchronize(s));
+    // eigen_decomposition(S, 1e-6, 1e-8) (linalg.hpp:1157-1197).
+    double max_eig = 0.0;
+    for (double v : lam) max_eig = std::max(max_eig, std::fabs(v));
+    const double thr = std::max(max_eig * 1e-8, 1e-6);
+    std::vector<int> keep;
+    std::vector<double> inv;
+    for (size_t i = 0; i < n; ++i)
+      if (std::fabs(lam[i]) > thr) {
+        if (!(lam[i] > 0.0)) throw_runtime("inv_sym_pd(): matrix is not positive definite");
+        keep.push_back(static_cast<int>(i));
+        inv.push_back(1.0 / lam[i]);
+      }
+    h->n_kept = keep.size();
+    h->Sinv.alloc(n * n);
+    const size_t r = keep.size();
+    if (r == 0) {
+      UW12_CUDA(cudaMemsetAsync(h->Sinv.get(), 0, n * n * sizeof(double), s));
+    } else {
+      int* d_idx = nullptr;
+      UW12_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_idx), r * sizeof(int), s));
+      DevBuf d_inv(r, s), d_one(r, s), vk(n * r, s), vks(n * r, s);
+      UW12_CUDA(cudaMemcpyAsync(d_idx, keep.data(), r * sizeof(int), cudaMemcpyHostToDevice, s));
+      UW12_CUDA(cudaMemcpyAsync(d_inv.get(), inv.data(), r * sizeof(double),
+                                cudaMemcpyHostToDevice, s));
+      std::vector<double> ones(r, 1.0);
+      UW12_CUDA(cudaMemcpyAsync(d_one.get(), ones.data(), r * sizeof(double),
+                                cudaMemcpyHostToDevice, s));
+      gather_scale_cols(vecs.get(), LL(n), d_idx, d_one.get(), LL(r), vk.get());
+      gather_scale_cols(vecs.get(), LL(n), d_idx, d_inv.get(), LL(r), vks.get());
+      GemmDesc g = gemm_nn(LL(n), LL(n), LL(r), 1.0, vks.get(), LL(n), vk.get(), LL(n), 0.0,
+                           h->Sinv.get(), LL(n));
+      g.b_ncontig = true;  // B = Vk^T
+      gemm(g);
+      UW12_CUDA(cudaFreeAsync(d_idx, s));
+    }
+    UW12_CUDA(cudaStreamSynchronize(s));
+  } catch (...) {
+    delete h;
+    throw;
+  }
+  return h;
+}
+
+// --------------------------------------------------------------------------
+// schedule helpers
+// --------------------------------------------------------------------------
+namespace {
+
+enum Slot { kE2d = 0, kE2i = 1, kE3d = 2, kE3i = 3, kE4d = 4, kE4i = 5, kSlots = 8 };
+
+double spin_factor(int ns, int s, int sp, double s_os, double s_ss) {
+  // four_electron_utils.cpp:9-30
+  if (ns == 1) return 2.0 * (s_os + s_ss);
+  return (s == sp) ? s_ss : s_os;
+}
+
+// H (N*nc x M) = [sq(J3_0[:,A]) Cm] for every A, chunked over A.
+void transform_ao(const IntegralsHandle& X, const double* Cm, size_t nc, double* H,
+                  size_t budget) {
+  const size_t N = X.n_ao, M = X.n_df, np = packed_size(N);
+  if (nc == 0) return;
+  const size_t ac = std::max<size_t>(1, std::min(M, budget / (N * N)));
+  DevBuf U(N * N * ac);
+  for (size_t a0 = 0; a0 < M; a0 += ac) {
+    const size_t na = std::min(ac, M - a0);
+    unpack_sym(X.J3_0.get() + np * a0, LL(np), LL(N), LL(na), U.get(), LL(N), LL(N * N));
+    GemmDesc g = gemm_nn(LL(N), LL(nc), LL(N), 1.0, U.get(), LL(N), Cm, LL(N), 0.0,
+                         H + N * nc * a0, LL(N));
+    g.nbo1 = LL(na);
+    g.sAo1 = LL(N * N);
+    g.sCo1 = LL(N * nc);
+    gemm(g);
+  }
+}
+
+struct SpinDims {
+  size_t o = 0, a = 0, c = 0, ooff = 0, aoff = 0;
+};
+
+}  // namespace
+
+// --------------------------------------------------------------------------
+// form_fock
+// --------------------------------------------------------------------------
+void form_fock(const FockRequest& rq) {
+  const IntegralsHandle& W = *rq.W;
+  const IntegralsHandle& V = *rq.V;
+  const IntegralsHandle& WV = *rq.WV;
+  const AbsHandle& AB = *rq.abs;
+  const int ns = rq.n_spin;
+  const size_t N = rq.n_ao;
+  const size_t np = packed_size(N);
+  const size_t MW = W.n_df, MV = V.n_df, MX = WV.n_df;
+  const size_t R = W.n_ri, Rp = N + R;
+  const double s_os = rq.s_os, s_ss = rq.s_ss;
+  const bool calc = rq.calc_fock;
+  const bool do_ind = rq.indirect && s_ss != 0.0;
+  const double half = (ns == 1) ? 0.5 : 1.0;
+  const double two = (ns == 1) ? 2.0 : 1.0;
+  const double kap4 = 2.0 * half;
+  cudaStream_t st = current_stream();
+  const size_t budget = auto_budget_doubles(rq.mem_budget);
+
+  std::vector<SpinDims> sd(ns);
+  size_t o_tot = 0, a_tot = 0;
+  for (int s = 0; s < ns; ++s) {
+    sd[s].o = rq.n_occ[s];
+    sd[s].a = rq.n_active[s];
+    sd[s].c = sd[s].o - sd[s].a;
+    sd[s].ooff = o_tot;
+    sd[s].aoff = a_tot;
+    o_tot += sd[s].o;
+    a_tot += sd[s].a;
+  }
+
+  // ---- occupation-weighted orbitals (utils.hpp:289-310), freeze_core (:235-253)
+  DevBuf Co(N * o_tot), Ca(N * a_tot), wts(o_tot);
+  {
+    std::vector<double> w(o_tot);
+    const double per = (ns == 1) ? 2.0 : 1.0;
+    for (int s = 0; s < ns; ++s)
+      for (size_t k = 0; k < sd[s].o; ++k) w[sd[s].ooff + k] = std::sqrt(rq.occ[s][k] / per);
+    if (o_tot)
+      UW12_CUDA(cudaMemcpyAsync(wts.get(), w.data(), o_tot * sizeof(double),
+                                cudaMemcpyHostToDevice, st));
+    for (int s = 0; s < ns; ++s) {
+      if (!sd[s].o) continue;
+      UW12_CUDA(cudaMemcpy2DAsync(Co.get() + N * sd[s].ooff, N * sizeof(double), rq.C[s],
+                                  rq.ldc[s] * sizeof(double), N * sizeof(double), sd[s].o,
+                                  cudaMemcpyHostToDevice, st));
+    }
+    if (o_tot) scale_rc(Co.get(), LL(N), LL(N), LL(o_tot), nullptr, wts.get(), 1.0, Co.get(), LL(N));
+    for (int s = 0; s < ns; ++s)
+      if (sd[s].a)
+        UW12_CUDA(cudaMemcpyAsync(Ca.get() + N * sd[s].aoff, Co.get() + N * (sd[s].ooff + sd[s].c),
+                                  N * sd[s].a * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
+  auto Co_s = [&](int s) { return Co.get() + N * sd[s].ooff; };
+  auto Ca_s = [&](int s) { return Ca.get() + N * sd[s].aoff; };
+
+  DevBuf acc(kSlots);
+  acc.zero();
+  std::vector<DevBuf> Fp(ns);
+  for (int s = 0; s < ns; ++s) {
+    Fp[s].alloc(N * N);
+    Fp[s].zero();
+  }
+
+  // =====================================================================
+  // two-electron term (two_electron.cpp:11-153), WV integrals, active orbitals
+  // =====================================================================
+  {
+    DevBuf dmat(np * ns), XDr(MX * ns), XD(MX * ns);
+    for (int s = 0; s < ns; ++s) pack_density(Ca_s(s), LL(N), LL(N), LL(sd[s].a), two, dmat.get() + np * s);
+    GemmDesc g = gemm_nn(LL(MX), ns, LL(np), 1.0, WV.J3_0.get(), LL(np), dmat.get(), LL(np), 0.0,
+                         XDr.get(), LL(MX));
+    g.a_kcontig = true;
+    gemm(g);
+    g = gemm_nn(LL(MX), ns, LL(MX), 0.5 * ns, WV.P2.get(), LL(MX), XDr.get(), LL(MX), 0.0,
+                XD.get(), LL(MX));
+    g.a_kcontig = true;
+    gemm(g);
+    double coef[4] = {0, 0, 0, 0};
+    for (int s = 0; s < ns; ++s)
+      for (int sp = 0; sp < ns; ++sp) {
+        const double f = spin_factor(ns, s, sp, s_os, s_ss);
+        if (f == 0.0) continue;
+        wdot(XD.get() + MX * s, LL(MX), XD.get() + MX * sp, LL(MX), LL(MX), 1, WV.lam.get(),
+             nullptr, 0.5 * f, acc.get(), kE2d);
+        coef[s * ns + sp] = 0.5 * ns * f;
+      }
+    if (calc) {
+      DevBuf vc(MX * ns), u(MX * ns), gv(np * ns);
+      combine_vecs(XD.get(), LL(MX), ns, coef, WV.lam.get(), vc.get());
+      gemm(gemm_nn(LL(MX), ns, LL(MX), 1.0, WV.P2.get(), LL(MX), vc.get(), LL(MX), 0.0, u.get(),
+                   LL(MX)));
+      gemm(gemm_nn(LL(np), ns, LL(MX), 1.0, WV.J3_0.get(), LL(np), u.get(), LL(MX), 0.0, gv.get(),
+                   LL(np)));
+      for (int s = 0; s < ns; ++s)
+        unpack_sym(gv.get() + np * s, LL(np), LL(N), 1, Fp[s].get(), LL(N), 0, 1.0, 1.0);
+    }
+    if (do_ind && a_tot > 0) {
+      DevBuf H(N * a_tot * MX);
+      transform_ao(WV, Ca.get(), a_tot, H.get(), budget / 2);
+      for (int s = 0; s < ns; ++s) {
+        const size_t a = sd[s].a;
+        if (!a) continue;
+        DevBuf B1(N * a * MX), B2(a * a * MX);
+        gemm(gemm_nn(LL(N * a), LL(MX), LL(MX), 1.0, H.get() + N * sd[s].aoff, LL(N * a_tot),
+                     WV.P2.get(), LL(MX), 0.0, B1.get(), LL(N * a)));
+        GemmDesc g3 = gemm_nn(LL(a), LL(a * MX), LL(N), 1.0, Ca_s(s), LL(N), B1.get(), LL(N), 0.0,
+                              B2.get(), LL(a));
+        g3.a_kcontig = true;
+        gemm(g3);
+        wdot(B2.get(), LL(a * a), B2.get(), LL(a * a), LL(a * a), LL(MX), nullptr, WV.lam.get(),
+             -0.5 * two, acc.get(), kE2i);
+        if (calc) {
+          DevBuf B1l(N * a * MX);
+          scale_rc(B1.get(), LL(N * a), LL(N * a), LL(MX), nullptr, WV.lam.get(), 1.0, B1l.get(),
+                   LL(N * a));
+          GemmDesc gf = gemm_nn(LL(N), LL(N), LL(a * MX), -s_ss, B1.get(), LL(N), B1l.get(),
+                                LL(N), 1.0, Fp[s].get(), LL(N));
+          gf.b_ncontig = true;
+          gemm(gf);
+        }
+      }
+    }
+  }
+
+  // =====================================================================
+  // MO transforms for W and V (integrals.cpp:184-345)
+  // =====================================================================
+  struct PerX {
+    std::vector<DevBuf> B1, B2, Wst, SV;
+  };
+  PerX XW, XV;
+  const bool need_sv_w = calc && do_ind;
+  for (int which = 0; which < 2; ++which) {
+    const IntegralsHandle& X = which == 0 ? W : V;
+    PerX& P = which == 0 ? XW : XV;
+    const size_t M = X.n_df;
+    P.B1.resize(ns);
+    P.B2.resize(ns);
+    P.Wst.resize(ns);
+    P.SV.resize(ns);
+    {
+      DevBuf H(N * o_tot * M);
+      transform_ao(X, Co.get(), o_tot, H.get(), budget / 2);
+      for (int s = 0; s < ns; ++s) {
+        const size_t o = sd[s].o;
+        if (!o) continue;
+        P.B1[s].alloc(N * o * M);
+        gemm(gemm_nn(LL(N * o), LL(M), LL(M), 1.0, H.get() + N * sd[s].ooff, LL(N * o_tot),
+                     X.P2.get(), LL(M), 0.0, P.B1[s].get(), LL(N * o)));
+      }
+    }
+    DevBuf H2(R * a_tot * M);
+    if (a_tot) {
+      GemmDesc g = gemm_nn(LL(R), LL(a_tot), LL(N), 1.0, X.J3_ri_0.get(), LL(R), Ca.get(), LL(N),
+                           0.0, H2.get(), LL(R));
+      g.nbo1 = LL(M);
+      g.sAo1 = LL(R * N);
+      g.sCo1 = LL(R * a_tot);
+      gemm(g);
+    }
+    for (int s = 0; s < ns; ++s) {
+      const size_t o = sd[s].o, a = sd[s].a, c = sd[s].c;
+      if (!a) continue;
+      P.B2[s].alloc(a * o * M);
+      GemmDesc g3 = gemm_nn(LL(a), LL(o * M), LL(N), 1.0, Ca_s(s), LL(N), P.B1[s].get(), LL(N),
+                            0.0, P.B2[s].get(), LL(a));
+      g3.a_kcontig = true;
+      gemm(g3);
+      P.Wst[s].alloc(Rp * a * M);
+      copy3d(P.B1[s].get() + N * c, LL(N), LL(N * o), P.Wst[s].get(), LL(Rp), LL(Rp * a), LL(N),
+             LL(a), LL(M));
+      GemmDesc g2 = gemm_nn(LL(R), LL(M), LL(M), 1.0, H2.get() + R * sd[s].aoff, LL(R * a_tot),
+                            X.P2.get(), LL(M), 0.0, P.Wst[s].get() + N, LL(Rp * a));
+      g2.nbo1 = LL(a);
+      g2.sAo1 = LL(R);
+      g2.sCo1 = LL(Rp);
+      gemm(g2);
+      if (which == 1 || need_sv_w) {
+        P.SV[s].alloc(Rp * a * M);
+        gemm(gemm_nn(LL(Rp), LL(a * M), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp), P.Wst[s].get(),
+                     LL(Rp), 0.0, P.SV[s].get(), LL(Rp)));
+      }
+    }
+  }
+
+  // =====================================================================
+  // X_AB, t, t~ and the direct energies (direct_utils.cpp:62-157,
+  // four_electron.cpp:80-137)
+  // =====================================================================
+  std::vector<DevBuf> Xab(ns), tab(ns), ttl(ns);
+  for (int s = 0; s < ns; ++s) {
+    const size_t o = sd[s].o, a = sd[s].a;
+    Xab[s].alloc(MW * MV);
+    tab[s].alloc(MW * MV);
+    ttl[s].alloc(MW * MV);
+    if (a == 0) {
+      Xab[s].zero();
+      tab[s].zero();
+      ttl[s].zero();
+      continue;
+    }
+    GemmDesc gx = gemm_nn(LL(MW), LL(MV), LL(Rp * a), 1.0, XW.Wst[s].get(), LL(Rp * a),
+                          XV.SV[s].get(), LL(Rp * a), 0.0, Xab[s].get(), LL(MW));
+    gx.a_kcontig = true;
+    gemm(gx);
+    GemmDesc gt = gemm_nn(LL(MW), LL(MV), LL(a * o), 1.0, XW.B2[s].get(), LL(a * o),
+                          XV.B2[s].get(), LL(a * o), 0.0, tab[s].get(), LL(MW));
+    gt.a_kcontig = true;
+    gemm(gt);
+    scale_rc(tab[s].get(), LL(MW), LL(MW), LL(MV), W.lam.get(), V.lam.get(), 1.0, ttl[s].get(),
+             LL(MW));
+  }
+  for (int s = 0; s < ns; ++s)
+    for (int sp = 0; sp < ns; ++sp) {
+      const double f = spin_factor(ns, s, sp, s_os, s_ss);
+      wdot(Xab[s].get(), LL(MW), ttl[sp].get(), LL(MW), LL(MW), LL(MV), nullptr, nullptr, -f,
+           acc.get(), kE3d);
+      if (f != 0.0)
+        wdot(ttl[sp].get(), LL(MW), tab[s].get(), LL(MW), LL(MW), LL(MV), nullptr, nullptr,
+             0.5 * f, acc.get(), kE4d);
+    }
+
+  // =====================================================================
+  // direct Fock: 4-el (four_electron.cpp:11-77) + 3-el X dt~ (direct_utils.cpp:164-204)
+  // combined as sum_k w_k (B1_W Y)_k (x) (B1_V)_k, and 3-el t~ dX
+  // (direct_utils.cpp:256-347) added to fock[sigma'] (three_electron.cpp:78)
+  // =====================================================================
+  if (calc) {
+    for (int s = 0; s < ns; ++s) {
+      const size_t o = sd[s].o, a = sd[s].a, c = sd[s].c;
+      if (!o) continue;
+      const double* Tq[2] = {ttl[0].get(), ns > 1 ? ttl[1].get() : nullptr};
+      const double* Xq[2] = {Xab[0].get(), ns > 1 ? Xab[1].get() : nullptr};
+      double cT[2] = {0, 0}, cX[2] = {0, 0};
+      for (int sp = 0; sp < ns; ++sp) {
+        const double f = spin_factor(ns, s, sp, s_os, s_ss);
+        cT[sp] = (f != 0.0) ? f * (a == 0 ? kap4 : 0.5 * kap4) : 0.0;
+        cX[sp] = half * f;
+      }
+      DevBuf Y(MW * MV), Z(N * o * MV);
+      combine_y(Y.get(), LL(MW), Tq, cT, Xq, cX, ns, W.lam.get(), V.lam.get());
+      gemm(gemm_nn(LL(N * o), LL(MV), LL(MW), 1.0, XW.B1[s].get(), LL(N * o), Y.get(), LL(MW),
+                   0.0, Z.get(), LL(N * o)));
+      if (a > 0)
+        copy3d(Z.get() + N * c, LL(N * o), 0, Z.get() + N * c, LL(N * o), 0, LL(N * a), LL(MV), 1,
+               2.0);
+      GemmDesc gf = gemm_nn(LL(N), LL(N), LL(o * MV), 1.0, Z.get(), LL(N), XV.B1[s].get(), LL(N),
+                            1.0, Fp[s].get(), LL(N));
+      gf.b_ncontig = true;
+      gemm(gf);
+    }
+    // t~ dX: F[sigma'] -= sum_ab T2[a,b] G_W[a]^T S^-1 G_V[b], T2 = P2_W Tc P2_V^T
+    for (int sp = 0; sp < ns; ++sp) {
+      const double* Tq[2] = {ttl[0].get(), ns > 1 ? ttl[1].get() : nullptr};
+      double cT[2] = {0, 0}, cX[2] = {0, 0};
+      bool any = false;
+      for (int s = 0; s < ns; ++s) {
+        cT[s] = half * spin_factor(ns, s, sp, s_os, s_ss);
+        any = any || (cT[s] != 0.0 && sd[s].a > 0);
+      }
+      if (!any) continue;
+      DevBuf Tc(MW * MV), tmp(MW * MV), T2(MW * MV);
+      combine_y(Tc.get(), LL(MW), Tq, cT, Tq, cX, ns, W.lam.get(), V.lam.get());
+      gemm(gemm_nn(LL(MW), LL(MV), LL(MW), 1.0, W.P2.get(), LL(MW), Tc.get(), LL(MW), 0.0,
+                   tmp.get(), LL(MW)));
+      GemmDesc gt2 = gemm_nn(LL(MW), LL(MV), LL(MV), 1.0, tmp.get(), LL(MW), V.P2.get(), LL(MV),
+                             0.0, T2.get(), LL(MW));
+      gt2.b_ncontig = true;
+      gemm(gt2);
+      const size_t per_a = 2 * Rp * N + N * N + np;
+      const size_t ac = std::max<size_t>(1, std::min(MW, budget / per_a));
+      DevBuf sbuf(np * ac), Hb(Rp * N * ac), Ub(Rp * N * ac), Gb(N * N * ac);
+      for (size_t a0 = 0; a0 < MW; a0 += ac) {
+        const size_t na = std::min(ac, MW - a0);
+        GemmDesc gs = gemm_nn(LL(np), LL(na), LL(MV), 1.0, V.J3_0.get(), LL(np), T2.get() + a0,
+                              LL(MW), 0.0, sbuf.get(), LL(np));
+        gs.b_ncontig = true;
+        gemm(gs);
+        unpack_sym(sbuf.get(), LL(np), LL(N), LL(na), Hb.get(), LL(Rp), LL(Rp * N));
+        GemmDesc gp = gemm_nn(LL(R), LL(na), LL(MV), 1.0, V.J3_ri_0.get(), LL(R * N),
+                              T2.get() + a0, LL(MW), 0.0, Hb.get() + N, LL(Rp * N));
+        gp.b_ncontig = true;
+        gp.nbo1 = LL(N);
+        gp.sAo1 = LL(R);
+        gp.sCo1 = LL(Rp);
+        gemm(gp);
+        gemm(gemm_nn(LL(Rp), LL(N * na), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp), Hb.get(), LL(Rp), 0.0,
+                     Ub.get(), LL(Rp)));
+        unpack_sym(W.J3_0.get() + np * a0, LL(np), LL(N), LL(na), Gb.get(), LL(N), LL(N * N));
+        GemmDesc ga = gemm_nn(LL(N), LL(N), LL(N), -1.0, Gb.get(), LL(N), Ub.get(), LL(Rp), 1.0,
+                              Fp[sp].get(), LL(N));
+        ga.nbr1 = LL(na);
+        ga.sAr1 = LL(N * N);
+        ga.sBr1 = LL(Rp * N);
+        gemm(ga);
+        GemmDesc gr = gemm_nn(LL(N), LL(N), LL(R), -1.0, W.J3_ri_0.get() + R * N * a0, LL(R),
+                              Ub.get() + N, LL(Rp), 1.0, Fp[sp].get(), LL(N));
+        gr.a_kcontig = true;
+        gr.nbr1 = LL(na);
+        gr.sAr1 = LL(R * N);
+        gr.sBr1 = LL(Rp * N);
+        gemm(gr);
+      }
+    }
+  }
+
+  // =====================================================================
+  // same-spin (indirect) terms
+  // =====================================================================
+  if (do_ind) {
+    for (int s = 0; s < ns; ++s) {
+      const size_t o = sd[s].o, a = sd[s].a, c = sd[s].c;
+      if (a == 0 || o == 0) continue;
+      const size_t ao = a * o, No = N * o;
+      DevBuf b2wl(ao * MW), b2vl(ao * MV);
+      scale_rc(XW.B2[s].get(), LL(ao), LL(ao), LL(MW), nullptr, W.lam.get(), 1.0, b2wl.get(), LL(ao));
+      scale_rc(XV.B2[s].get(), LL(ao), LL(ao), LL(MV), nullptr, V.lam.get(), 1.0, b2vl.get(), LL(ao));
+      // ---- 4-el indirect energy (four_electron.cpp:143-179)
+      {
+        DevBuf W4(ao * ao), V4(ao * ao);
+        GemmDesc g = gemm_nn(LL(ao), LL(ao), LL(MW), 1.0, b2wl.get(), LL(ao), XW.B2[s].get(),
+                             LL(ao), 0.0, W4.get(), LL(ao));
+        g.b_ncontig = true;
+        gemm(g);
+        g = gemm_nn(LL(ao), LL(ao), LL(MV), 1.0, b2vl.get(), LL(ao), XV.B2[s].get(), LL(ao), 0.0,
+                    V4.get(), LL(ao));
+        g.b_ncontig = true;
+        gemm(g);
+        permdot_4el(W4.get(), V4.get(), LL(a), LL(o), -0.5 * two, acc.get(), kE4i);
+      }
+      // ---- 3-el indirect energy (indirect_utils.cpp:101-133), chunked over k
+      {
+        const size_t per_k = 2 * Rp * a * a;
+        const size_t kc = std::max<size_t>(1, std::min(o, budget / per_k));
+        DevBuf YW(Rp * a * a * kc), ZV(Rp * a * a * kc);
+        for (size_t k0 = 0; k0 < o; k0 += kc) {
+          const size_t nk = std::min(kc, o - k0);
+          GemmDesc g = gemm_nn(LL(Rp * a), LL(a * nk), LL(MW), 1.0, XW.Wst[s].get(), LL(Rp * a),
+                               b2wl.get() + a * k0, LL(ao), 0.0, YW.get(), LL(Rp * a));
+          g.b_ncontig = true;
+          gemm(g);
+          g = gemm_nn(LL(Rp * a), LL(a * nk), LL(MV), 1.0, XV.SV[s].get(), LL(Rp * a),
+                      b2vl.get() + a * k0, LL(ao), 0.0, ZV.get(), LL(Rp * a));
+          g.b_ncontig = true;
+          gemm(g);
+          permdot_3el(YW.get(), ZV.get(), LL(Rp), LL(a), LL(nk), two, acc.get(), kE3i);
+        }
+      }
+      if (!calc) continue;
+      DevBuf b1wl(No * MW), b1vl(No * MV);
+      scale_rc(XW.B1[s].get(), LL(No), LL(No), LL(MW), nullptr, W.lam.get(), 1.0, b1wl.get(), LL(No));
+      scale_rc(XV.B1[s].get(), LL(No), LL(No), LL(MV), nullptr, V.lam.get(), 1.0, b1vl.get(), LL(No));
+      // ---- 4-el indirect Fock (four_electron.cpp:181-249)
+      {
+        DevBuf W43(No * ao), V43(No * ao);
+        GemmDesc g = gemm_nn(LL(No), LL(ao), LL(MW), 1.0, b1wl.get(), LL(No), XW.B2[s].get(),
+                             LL(ao), 0.0, W43.get(), LL(No));
+        g.b_ncontig = true;
+        gemm(g);
+        g = gemm_nn(LL(No), LL(ao), LL(MV), 1.0, b1vl.get(), LL(No), XV.B2[s].get(), LL(ao), 0.0,
+                    V43.get(), LL(No));
+        g.b_ncontig = true;
+        gemm(g);
+        GemmDesc gi = gemm_nn(LL(N), LL(N), LL(a), s_ss * (c > 0 ? -1.0 : -2.0),
+                              W43.get() + N * c, LL(No), V43.get() + N * c, LL(N), 1.0,
+                              Fp[s].get(), LL(N));
+        gi.b_ncontig = true;
+        gi.nbr1 = LL(a);
+        gi.nbr2 = LL(o);
+        gi.sAr1 = LL(N);
+        gi.sAr2 = LL(No * a);
+        gi.sBr1 = LL(No);
+        gi.sBr2 = LL(No * a);
+        gemm(gi);
+        if (c > 0) {
+          GemmDesc gf = gemm_nn(LL(N), LL(N), LL(a), -s_ss, W43.get(), LL(No), V43.get(), LL(No),
+                                1.0, Fp[s].get(), LL(N));
+          gf.b_ncontig = true;
+          gf.nbr1 = LL(o);
+          gf.nbr2 = LL(o);
+          gf.sAr1 = LL(N);
+          gf.sAr2 = LL(No * a);
+          gf.sBr1 = LL(No * a);
+          gf.sBr2 = LL(N);
+          gemm(gf);
+        }
+      }
+      // ---- 3-el indirect Fock (indirect_utils.cpp:139-345), chunked over k
+      {
+        DevBuf xhW(MW * ao), xhV(MV * ao);
+        GemmDesc g = gemm_nn(LL(MW), LL(ao), LL(MW), 1.0, W.P2.get(), LL(MW), b2wl.get(), LL(ao),
+                             0.0, xhW.get(), LL(MW));
+        g.b_ncontig = true;
+        gemm(g);
+        g = gemm_nn(LL(MV), LL(ao), LL(MV), 1.0, V.P2.get(), LL(MV), b2vl.get(), LL(ao), 0.0,
+                    xhV.get(), LL(MV));
+        g.b_ncontig = true;
+        gemm(g);
+        const size_t per_k = 3 * Rp * a * N + a * (N * N + R * N + np);
+        const size_t kc = std::max<size_t>(1, std::min(o, budget / per_k));
+        DevBuf ZYV(Rp * a * N * kc), ZYW(Rp * a * N * kc), gpk(np * a * kc), Gao(N * N * a * kc),
+            gri(R * N * a * kc), Wk(Rp * N * a * kc);
+        for (size_t k0 = 0; k0 < o; k0 += kc) {
+          const size_t nk = std::min(kc, o - k0);
+          for (int term = 0; term < 2; ++term) {
+            // term 0: fock_i(W, V) over (j, k); term 1: fock_i(V, W) over (i, k)
+            const IntegralsHandle& Xi = term == 0 ? W : V;
+            const double* xh = term == 0 ? xhW.get() : xhV.get();
+            const size_t MXi = Xi.n_df;
+            const double* SVy = term == 0 ? XV.SV[s].get() : XW.SV[s].get();
+            const double* b1yl = term == 0 ? b1vl.get() : b1wl.get();
+            const size_t MY = term == 0 ? MV : MW;
+            double* ZY = term == 0 ? ZYV.get() : ZYW.get();
+            GemmDesc gz = gemm_nn(LL(Rp * a), LL(N * nk), LL(MY), 1.0, SVy, LL(Rp * a),
+                                  b1yl + N * k0, LL(No), 0.0, ZY, LL(Rp * a));
+            gz.b_ncontig = true;
+            gemm(gz);
+            gemm(gemm_nn(LL(np), LL(a * nk), LL(MXi), 1.0, Xi.J3_0.get(), LL(np),
+                         xh + MXi * a * k0, LL(MXi), 0.0, gpk.get(), LL(np)));
+            unpack_sym(gpk.get(), LL(np), LL(N), LL(a * nk), Gao.get(), LL(N), LL(N * N));
+            gemm(gemm_nn(LL(R * N), LL(a * nk), LL(MXi), 1.0, Xi.J3_ri_0.get(), LL(R * N),
+                         xh + MXi * a * k0, LL(MXi), 0.0, gri.get(), LL(R * N)));
+            GemmDesc fa = gemm_nn(LL(N), LL(N), LL(N), s_ss, Gao.get(), LL(N), ZY, LL(Rp * a),
+                                  1.0, Fp[s].get(), LL(N));
+            fa.nbr1 = LL(a);
+            fa.nbr2 = LL(nk);
+            fa.sAr1 = LL(N * N);
+            fa.sAr2 = LL(N * N * a);
+            fa.sBr1 = LL(Rp);
+            fa.sBr2 = LL(Rp * a * N);
+            gemm(fa);
+            GemmDesc fr = gemm_nn(LL(N), LL(N), LL(R), s_ss, gri.get(), LL(R), ZY + N, LL(Rp * a),
+                                  1.0, Fp[s].get(), LL(N));
+            fr.a_kcontig = true;
+            fr.nbr1 = LL(a);
+            fr.nbr2 = LL(nk);
+            fr.sAr1 = LL(R * N);
+            fr.sAr2 = LL(R * N * a);
+            fr.sBr1 = LL(Rp);
+            fr.sBr2 = LL(Rp * a * N);
+            gemm(fr);
+          }
+          // k-term (fock_k) for active orbitals c+i inside this chunk
+          const long long i0 = std::max<long long>(0, LL(k0) - LL(c));
+          const long long i1 = LL(k0 + nk) - LL(c);
+          if (i1 > i0) {
+            const size_t ni = static_cast<size_t>(i1 - i0);
+            GemmDesc gw = gemm_nn(LL(Rp * ni), LL(N * a), LL(MW), 1.0,
+                                  XW.Wst[s].get() + Rp * i0, LL(Rp * a), b1wl.get() + N * c,
+                                  LL(No), 0.0, Wk.get(), LL(Rp * ni));
+            gw.b_ncontig = true;
+            gemm(gw);
+            GemmDesc fk = gemm_nn(LL(N), LL(N), LL(Rp), s_ss, Wk.get(), LL(Rp * ni),
+                                  ZYV.get() + Rp * a * N * (c + i0 - k0), LL(Rp * a), 1.0,
+                                  Fp[s].get(), LL(N));
+            fk.a_kcontig = true;
+            fk.nbr1 = LL(ni);
+            fk.nbr2 = LL(a);
+            fk.sAr1 = LL(Rp);
+            fk.sAr2 = LL(Rp * ni * N);
+            fk.sBr1 = LL(Rp * a * N);
+            fk.sBr2 = LL(Rp);
+            gemm(fk);
+          }
+        }
+      }
+    }
+  }
+
+  // =====================================================================
+  // energies and the symmetrised Fock matrix
+  // =====================================================================
+  double e[kSlots];
+  UW12_CUDA(cudaMemcpyAsync(e, acc.get(), sizeof(e), cudaMemcpyDeviceToHost, st));
+  if (rq.fock && calc) {
+    double* dst = rq.fock;
+    DevBuf out;
+    if (!rq.fock_device) {
+      out.alloc(N * N * ns);
+      dst = out.get();
+    }
+    for (int s = 0; s < ns; ++s) symmetrise(Fp[s].get(), LL(N), LL(N), dst + N * N * s, LL(N));
+    if (!rq.fock_device)
+      UW12_CUDA(cudaMemcpyAsync(rq.fock, dst, N * N * ns * sizeof(double), cudaMemcpyDeviceToHost,
+                                st));
+    UW12_CUDA(cudaStreamSynchronize(st));
+  } else {
+    if (rq.fock) {
+      if (rq.fock_device)
+        UW12_CUDA(cudaMemsetAsync(rq.fock, 0, N * N * ns * sizeof(double), st));
+      else
+        std::fill(rq.fock, rq.fock + N * N * ns, 0.0);
+    }
+    UW12_CUDA(cudaStreamSynchronize(st));
+  }
+  const double e2 = e[kE2d] + (do_ind ? s_ss * e[kE2i] : 0.0);
+  const double e3 = e[kE3d] + (do_ind ? s_ss * e[kE3i] : 0.0);
+  const double e4 = e[kE4d] + (do_ind ? s_ss * e[kE4i] : 0.0);
+  const double total = e2 + e3 + e4;
+  if (rq.energy) *rq.energy = total;
+  if (rq.terms) {
+    rq.terms[0] = e2;
+    rq.terms[1] = e3;
+    rq.terms[2] = e4;
+  }
+  if (rq.print_level > 0) {
+    // print.hpp:13-42 formatting
+    auto line = [](char ch) { for (int i = 0; i < 48; ++i) std::putchar(ch); std::putchar('\n'); };
+    auto res = [](const char* s, double v) {
+      std::string str(s);
+      std::printf(" %s:%*s%12.6f\n", s, int(32 - str.size()), "", v);
+    };
+    if (rq.print_level > 2) {
+      std::printf("\n");
+      line('=');
+      std::printf(" UW12 Calculation\n");
+      line('=');
+    }
+    if (rq.print_level > 1) {
+      res("Two electron energy", e2);
+      res("Three electron energy", e3);
+      res("Four electron energy", e4);
+    }
+    if (rq.print_level > 2) line('=');
+    res("Total UW12 energy", total);
+    std::fflush(stdout);
+  }
+}
+
+}  // namespace uw12b

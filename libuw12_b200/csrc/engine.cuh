@@ -1,0 +1,82 @@
+// UW12 energy + Fock engine: device-resident integral handles and the
+// pair-loop-free FP64 schedule of libuw12's form_fock (src/uw12.cpp:22-119).
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace uw12b {
+
+// Persistent device array (cudaMalloc / cudaFree, independent of streams).
+class DeviceArray {
+ public:
+  DeviceArray() = default;
+  explicit DeviceArray(size_t n) { alloc(n); }
+  DeviceArray(const DeviceArray&) = delete;
+  DeviceArray& operator=(const DeviceArray&) = delete;
+  ~DeviceArray() { if (p_) cudaFree(p_); }
+  void alloc(size_t n) {
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    n_ = n;
+    if (n_) UW12_CUDA(cudaMalloc(reinterpret_cast<void**>(&p_), n_ * sizeof(double)));
+  }
+  double* get() const { return p_; }
+  size_t size() const { return n_; }
+
+ private:
+  double* p_ = nullptr;
+  size_t n_ = 0;
+};
+
+// BaseIntegrals built from stored tensors (base_integrals.cpp:282-303):
+// J3_0 (Np x M, packed (mn|A)), J3_ri_0 ((R N) x M, row nu + R mu) and the
+// metric eigendecomposition P2 = Q pinv(Lambda), df_vals = Lambda
+// (base_integrals.cpp:155-166).
+struct IntegralsHandle {
+  int device = 0;
+  size_t n_ao = 0, n_df = 0, n_ri = 0;
+  DeviceArray J3_0, J3_ri_0, P2, lam;
+  std::vector<double> lam_host;
+};
+
+// ABS+ projectors (ri_utils.hpp:45-74) stored as one (N+R) x (N+R) matrix
+// S^-1 = V_k Lambda_k^-1 V_k^T over the kept eigenpairs, AO block first.
+struct AbsHandle {
+  int device = 0;
+  size_t n_ao = 0, n_ri = 0, n_kept = 0;
+  DeviceArray Sinv;
+};
+
+IntegralsHandle* integrals_create(const double* X3, const double* X2, const double* X3_ri,
+                                  size_t n_ao, size_t n_df, size_t n_ri, bool device_mem);
+AbsHandle* abs_create(const double* S, size_t n_ao, size_t n_ri, bool device_mem);
+
+struct FockRequest {
+  const IntegralsHandle* W = nullptr;
+  const IntegralsHandle* V = nullptr;
+  const IntegralsHandle* WV = nullptr;
+  const AbsHandle* abs = nullptr;
+  int n_spin = 0;
+  size_t n_ao = 0;
+  std::vector<const double*> C;     // per spin: n_ao x n_orb[s], column-major (host)
+  std::vector<size_t> ldc;          // leading dimension of each C block
+  std::vector<size_t> n_orb;
+  std::vector<const double*> occ;   // per spin: n_occ[s] values (host)
+  std::vector<size_t> n_occ;
+  std::vector<size_t> n_active;
+  bool indirect = false;
+  bool calc_fock = true;
+  double s_os = 1.0, s_ss = 0.0;
+  size_t print_level = 0;
+  double* energy = nullptr;         // host scalar
+  double* fock = nullptr;           // n_ao x (n_ao * n_spin); may be null
+  bool fock_device = false;         // fock points to device memory
+  double* terms = nullptr;          // host: {E2, E3, E4} or null
+  size_t mem_budget = 0;            // bytes for chunked intermediates (0 = auto)
+};
+
+void form_fock(const FockRequest& rq);
+
+}  // namespace uw12b

@@ -1,0 +1,399 @@
+// FP64 DMMA GEMM for sm_100a: 128x128x16 CTA tiles, 8 warps of 64x32,
+// 4-stage cp.async pipeline, m16n8k4 f64 tensor-core MMAs.
+#include <algorithm>
+#include <mutex>
+
+#include "gemm_f64.cuh"
+
+namespace uw12b {
+
+namespace {
+
+constexpr int BM = 128;
+constexpr int BN = 128;
+constexpr int BK = 16;
+constexpr int STAGES = 4;
+constexpr int THREADS = 256;
+constexpr int LDW = 132;  // row length of [k][m] / [k][n] tiles (doubles); 132 % 16 == 4
+constexpr int LDK = 20;   // row length of [m][k] / [n][k] tiles (doubles); 20 % 16 == 4
+constexpr int A_STAGE = (BM * LDK > BK * LDW) ? BM * LDK : BK * LDW;  // 2560
+constexpr int B_STAGE = A_STAGE;
+constexpr size_t SMEM_BYTES = size_t(STAGES) * (A_STAGE + B_STAGE) * sizeof(double);
+
+struct KParams {
+  const double* A;
+  const double* B;
+  double* C;
+  double* work;  // split > 1: partial tiles [split][nbo][m*n]
+  long long lda, ldb, ldc;
+  long long m, n, k;
+  double alpha, beta;
+  long long nbo1, nbo;
+  long long sAo1, sAo2, sBo1, sBo2, sCo1, sCo2;
+  long long nbr1;
+  long long sAr1, sAr2, sBr1, sBr2;
+  long long tiles_m, tiles_mn;
+  long long ktiles_pb, ktiles_total;
+  int split;
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+  const int bytes = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+
+template <bool AK, bool BNC>
+__global__ void __launch_bounds__(THREADS, 1) dgemm_dmma(const KParams p) {
+  extern __shared__ __align__(16) double smem[];
+  double* As = smem;
+  double* Bs = smem + STAGES * A_STAGE;
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int g = lane >> 2;  // groupID
+  const int t = lane & 3;   // thread in group
+  const int wm = (warp & 1) * 64;
+  const int wn = (warp >> 1) * 32;
+
+  long long bid = blockIdx.x;
+  const long long tile = bid % p.tiles_mn;
+  bid /= p.tiles_mn;
+  const long long bo = bid % p.nbo;
+  const int sp = static_cast<int>(bid / p.nbo);
+  const long long tm = tile % p.tiles_m;
+  const long long tn = tile / p.tiles_m;
+  const long long m0 = tm * BM;
+  const long long n0 = tn * BN;
+  const long long bo1 = bo % p.nbo1;
+  const long long bo2 = bo / p.nbo1;
+  const double* Ab = p.A + bo1 * p.sAo1 + bo2 * p.sAo2;
+  const double* Bb = p.B + bo1 * p.sBo1 + bo2 * p.sBo2;
+
+  const long long kt_begin = p.ktiles_total * sp / p.split;
+  const long long kt_end = p.ktiles_total * (sp + 1) / p.split;
+
+  // Per-thread fixed coordinates of the tile loads (8 elements per operand).
+  // A: [k][m] tile (m-contiguous global) or [m][k] tile (k-contiguous global).
+  const int a_i0 = AK ? (tid >> 4) : (tid & 127);
+  const int a_k0 = AK ? (tid & 15) : (tid >> 7);
+  const int b_j0 = BNC ? (tid & 127) : (tid >> 4);
+  const int b_k0 = BNC ? (tid >> 7) : (tid & 15);
+
+  auto load_stage = [&](int slot, long long kt) {
+    const long long br = kt / p.ktiles_pb;
+    const long long kin = (kt - br * p.ktiles_pb) * BK;
+    const long long br1 = br % p.nbr1;
+    const long long br2 = br / p.nbr1;
+    const double* Ar = Ab + br1 * p.sAr1 + br2 * p.sAr2;
+    const double* Br = Bb + br1 * p.sBr1 + br2 * p.sBr2;
+    double* as = As + slot * A_STAGE;
+    double* bs = Bs + slot * B_STAGE;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      int i, kk;
+      if (AK) { i = a_i0 + 16 * r; kk = a_k0; } else { i = a_i0; kk = a_k0 + 2 * r; }
+      const long long gi = m0 + i, gk = kin + kk;
+      const bool v = (gi < p.m) && (gk < p.k);
+      const double* src = v ? (AK ? Ar + gk + p.lda * gi : Ar + gi + p.lda * gk) : p.A;
+      double* dst = AK ? as + i * LDK + kk : as + kk * LDW + i;
+      cp_async8(dst, src, v);
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      int j, kk;
+      if (BNC) { j = b_j0; kk = b_k0 + 2 * r; } else { j = b_j0 + 16 * r; kk = b_k0; }
+      const long long gj = n0 + j, gk = kin + kk;
+      const bool v = (gj < p.n) && (gk < p.k);
+      const double* src = v ? (BNC ? Br + gj + p.ldb * gk : Br + gk + p.ldb * gj) : p.B;
+      double* dst = BNC ? bs + kk * LDW + j : bs + j * LDK + kk;
+      cp_async8(dst, src, v);
+    }
+  };
+
+  double acc[4][4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (kt_begin + s < kt_end) load_stage(s, kt_begin + s);
+    cp_async_commit();
+  }
+
+  for (long long kt = kt_begin; kt < kt_end; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    {
+      const long long nxt = kt + STAGES - 1;
+      if (nxt < kt_end) load_stage(static_cast<int>((nxt - kt_begin) % STAGES), nxt);
+      cp_async_commit();
+    }
+    const int slot = static_cast<int>((kt - kt_begin) % STAGES);
+    const double* as = As + slot * A_STAGE;
+    const double* bs = Bs + slot * B_STAGE;
+#pragma unroll
+    for (int kq = 0; kq < BK / 4; ++kq) {
+      const int kk = kq * 4 + t;
+      double af[4][2], bf[4];
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi) {
+        const int row = wm + mi * 16 + g;
+        af[mi][0] = AK ? as[row * LDK + kk] : as[kk * LDW + row];
+        af[mi][1] = AK ? as[(row + 8) * LDK + kk] : as[kk * LDW + row + 8];
+      }
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+        const int col = wn + ni * 8 + g;
+        bf[ni] = BNC ? bs[kk * LDW + col] : bs[col * LDK + kk];
+      }
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) dmma(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+    }
+  }
+  cp_async_wait<0>();
+
+  // Epilogue.
+  if (p.split == 1) {
+    double* Cb = p.C + bo1 * p.sCo1 + bo2 * p.sCo2;
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const long long r = m0 + wm + mi * 16 + g + 8 * h;
+          if (r >= p.m) continue;
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const long long c = n0 + wn + ni * 8 + 2 * t + q;
+            if (c >= p.n) continue;
+            double* dst = Cb + r + p.ldc * c;
+            const double v = p.alpha * acc[mi][ni][2 * h + q];
+            *dst = (p.beta == 0.0) ? v : v + p.beta * (*dst);
+          }
+        }
+  } else {
+    double* Wb = p.work + (static_cast<long long>(sp) * p.nbo + bo) * (p.m * p.n);
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const long long r = m0 + wm + mi * 16 + g + 8 * h;
+          if (r >= p.m) continue;
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const long long c = n0 + wn + ni * 8 + 2 * t + q;
+            if (c >= p.n) continue;
+            Wb[r + p.m * c] = acc[mi][ni][2 * h + q];
+          }
+        }
+  }
+}
+
+// C = alpha * sum_s work[s] + beta * C (fixed summation order).
+__global__ void splitk_reduce(const double* __restrict__ work, int split, long long m, long long n,
+                              long long nbo, long long nbo1, double alpha, double beta, double* C,
+                              long long ldc, long long sCo1, long long sCo2) {
+  const long long total = m * n * nbo;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long mn = m * n;
+    const long long bo = idx / mn;
+    const long long e = idx - bo * mn;
+    const long long r = e % m, c = e / m;
+    double s = 0.0;
+    for (int q = 0; q < split; ++q) s += work[(q * nbo + bo) * mn + e];
+    double* dst = C + (bo % nbo1) * sCo1 + (bo / nbo1) * sCo2 + r + ldc * c;
+    const double v = alpha * s;
+    *dst = (beta == 0.0) ? v : v + beta * (*dst);
+  }
+}
+
+// C = beta * C for an empty contraction.
+__global__ void scale_only(long long m, long long n, long long nbo, long long nbo1, double beta,
+                           double* C, long long ldc, long long sCo1, long long sCo2) {
+  const long long total = m * n * nbo;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long mn = m * n;
+    const long long bo = idx / mn;
+    const long long e = idx - bo * mn;
+    double* dst = C + (bo % nbo1) * sCo1 + (bo / nbo1) * sCo2 + (e % m) + ldc * (e / m);
+    *dst = (beta == 0.0) ? 0.0 : beta * (*dst);
+  }
+}
+
+template <bool AK, bool BNC>
+void launch_variant(const KParams& p, long long grid, cudaStream_t s) {
+  static bool attr_set[64] = {};
+  int dev = 0;
+  UW12_CUDA(cudaGetDevice(&dev));
+  static std::mutex mu;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 64 && !attr_set[dev]) {
+      UW12_CUDA(cudaFuncSetAttribute(dgemm_dmma<AK, BNC>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(SMEM_BYTES)));
+      attr_set[dev] = true;
+    }
+  }
+  dgemm_dmma<AK, BNC><<<static_cast<unsigned>(grid), THREADS, SMEM_BYTES, s>>>(p);
+  UW12_LAUNCHED();
+}
+
+// ---- profiling -------------------------------------------------------------
+struct ProfRec {
+  cudaEvent_t a, b;
+  double flops;
+};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<ProfRec> g_prof_recs;
+KernelStats g_prof_acc;
+
+void prof_collect_locked() {
+  for (auto& r : g_prof_recs) {
+    UW12_CUDA(cudaEventSynchronize(r.b));
+    float ms = 0.f;
+    UW12_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+    g_prof_acc.launches += 1;
+    g_prof_acc.ms += ms;
+    g_prof_acc.flops += r.flops;
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  g_prof_recs.clear();
+}
+
+}  // namespace
+
+void profile_enable(bool on) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof_on = on;
+}
+
+void profile_reset() {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  prof_collect_locked();
+  g_prof_acc = KernelStats{};
+}
+
+KernelStats profile_read_gemm() {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  prof_collect_locked();
+  return g_prof_acc;
+}
+
+void gemm(const GemmDesc& d) {
+  const long long nbo = d.nbo1 * d.nbo2;
+  const long long nbr = d.nbr1 * d.nbr2;
+  if (d.m <= 0 || d.n <= 0 || nbo <= 0) return;
+  cudaStream_t s = current_stream();
+  if (d.k <= 0 || nbr <= 0) {
+    if (d.beta == 1.0) return;
+    const long long total = d.m * d.n * nbo;
+    const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 16));
+    scale_only<<<blocks, 256, 0, s>>>(d.m, d.n, nbo, d.nbo1, d.beta, d.C, d.ldc, d.sCo1, d.sCo2);
+    UW12_LAUNCHED();
+    return;
+  }
+  if (!d.A || !d.B || !d.C) throw Error(kErrInvalid, "gemm: null operand");
+
+  KParams p{};
+  p.A = d.A; p.B = d.B; p.C = d.C;
+  p.lda = d.lda; p.ldb = d.ldb; p.ldc = d.ldc;
+  p.m = d.m; p.n = d.n; p.k = d.k;
+  p.alpha = d.alpha; p.beta = d.beta;
+  p.nbo1 = d.nbo1; p.nbo = nbo;
+  p.sAo1 = d.sAo1; p.sAo2 = d.sAo2; p.sBo1 = d.sBo1; p.sBo2 = d.sBo2;
+  p.sCo1 = d.sCo1; p.sCo2 = d.sCo2;
+  p.nbr1 = d.nbr1;
+  p.sAr1 = d.sAr1; p.sAr2 = d.sAr2; p.sBr1 = d.sBr1; p.sBr2 = d.sBr2;
+  p.tiles_m = (d.m + BM - 1) / BM;
+  const long long tiles_n = (d.n + BN - 1) / BN;
+  p.tiles_mn = p.tiles_m * tiles_n;
+  p.ktiles_pb = (d.k + BK - 1) / BK;
+  p.ktiles_total = p.ktiles_pb * nbr;
+
+  const long long ctas = p.tiles_mn * nbo;
+  int split = d.split;
+  if (split <= 0) {
+    constexpr long long kSMs = 148;
+    split = 1;
+    if (ctas < kSMs) {
+      long long want = (kSMs + ctas - 1) / ctas;
+      long long cap = std::max<long long>(1, p.ktiles_total / 8);  // >= 128 k per split
+      split = static_cast<int>(std::min<long long>(std::min(want, cap), 64));
+    }
+  }
+  split = static_cast<int>(std::max<long long>(1, std::min<long long>(split, p.ktiles_total)));
+  p.split = split;
+
+  DevBuf work;
+  if (split > 1) {
+    work.alloc(static_cast<size_t>(split) * nbo * d.m * d.n, s);
+    p.work = work.get();
+  }
+
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+  bool prof = false;
+  {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    prof = g_prof_on;
+  }
+  if (prof) {
+    UW12_CUDA(cudaEventCreate(&ev_a));
+    UW12_CUDA(cudaEventCreate(&ev_b));
+    UW12_CUDA(cudaEventRecord(ev_a, s));
+  }
+
+  const long long grid = ctas * split;
+  if (!d.a_kcontig && !d.b_ncontig) launch_variant<false, false>(p, grid, s);
+  else if (!d.a_kcontig && d.b_ncontig) launch_variant<false, true>(p, grid, s);
+  else if (d.a_kcontig && !d.b_ncontig) launch_variant<true, false>(p, grid, s);
+  else launch_variant<true, true>(p, grid, s);
+
+  if (split > 1) {
+    const long long total = d.m * d.n * nbo;
+    const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 16));
+    splitk_reduce<<<blocks, 256, 0, s>>>(p.work, split, d.m, d.n, nbo, d.nbo1, d.alpha, d.beta,
+                                         d.C, d.ldc, d.sCo1, d.sCo2);
+    UW12_LAUNCHED();
+  }
+  if (prof) {
+    UW12_CUDA(cudaEventRecord(ev_b, s));
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    g_prof_recs.push_back({ev_a, ev_b, 2.0 * double(d.m) * double(d.n) * double(d.k) *
+                                           double(nbo) * double(nbr)});
+  }
+}
+
+}  // namespace uw12b

@@ -1,0 +1,70 @@
+// FP64 tensor-core GEMM engine for sm_100a.
+//
+// Blackwell's tcgen05 has no FP64 kind, so FP64 contractions run on the
+// double-precision MMA path (mma.sync.aligned.m16n8k4 .f64).  One kernel
+// covers every contraction of the UW12 schedule:
+//
+//   C[bo] = alpha * sum_{r1,r2} op(A)[bo,r] * op(B)[bo,r] + beta * C[bo]
+//
+// with arbitrary m, n, k, leading dimensions and element offsets, 2-D output
+// batches (bo1, bo2) and 2-D reduction batches (r1, r2): the latter is how the
+// reference's orbital-pair loops (parallel_sum_2d over (j,k) of N x N
+// products) become a single launch.  Split-K partitions the flattened
+// (reduction batch, k-tile) space across CTAs when the output has too few
+// tiles to fill 148 SMs; partial tiles go to a workspace reduced in a fixed
+// order (deterministic).
+#pragma once
+
+#include "common.cuh"
+
+namespace uw12b {
+
+struct GemmDesc {
+  long long m = 0, n = 0, k = 0;
+  // A is m x k: element (i, kk) at A[i + lda*kk] (a_kcontig=false) or A[kk + lda*i].
+  const double* A = nullptr;
+  long long lda = 0;
+  bool a_kcontig = false;
+  // B is k x n: element (kk, j) at B[kk + ldb*j] (b_ncontig=false) or B[j + ldb*kk].
+  const double* B = nullptr;
+  long long ldb = 0;
+  bool b_ncontig = false;
+  // C is m x n column-major.
+  double* C = nullptr;
+  long long ldc = 0;
+  double alpha = 1.0, beta = 0.0;
+  // output batches
+  long long nbo1 = 1, nbo2 = 1;
+  long long sAo1 = 0, sAo2 = 0, sBo1 = 0, sBo2 = 0, sCo1 = 0, sCo2 = 0;
+  // reduction batches (summed into the same C)
+  long long nbr1 = 1, nbr2 = 1;
+  long long sAr1 = 0, sAr2 = 0, sBr1 = 0, sBr2 = 0;
+  int split = 0;  // 0: automatic
+};
+
+// Launches on current_stream().  Zero-sized problems are no-ops (k == 0 or
+// no reduction batches scales C by beta).
+void gemm(const GemmDesc& d);
+
+// Convenience wrappers in BLAS terms (column-major, 'N'/'T').
+inline GemmDesc gemm_nn(long long m, long long n, long long k, double alpha, const double* A,
+                        long long lda, const double* B, long long ldb, double beta, double* C,
+                        long long ldc) {
+  GemmDesc d;
+  d.m = m; d.n = n; d.k = k; d.alpha = alpha; d.beta = beta;
+  d.A = A; d.lda = lda; d.B = B; d.ldb = ldb; d.C = C; d.ldc = ldc;
+  return d;
+}
+
+// Per-kernel-class timing (CUDA events around every launch) for roofline
+// reporting.  Disabled by default.
+struct KernelStats {
+  unsigned long long launches = 0;
+  double ms = 0.0;
+  double flops = 0.0;  // algorithmic 2*m*n*k per launch
+};
+void profile_enable(bool on);
+KernelStats profile_read_gemm();  // synchronises the recorded events
+void profile_reset();
+
+}  // namespace uw12b

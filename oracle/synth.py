@@ -120,6 +120,40 @@ def three_index_ri(seed: int, name: str, n_ao: int, n_ri: int, n_df: int, decay:
     return out.reshape((nr, n_df), order="F")
 
 
+def fast_three_index(seed: int, name: str, n_rows: int, n_df: int, damp: np.ndarray) -> np.ndarray:
+    """Same distribution as ``three_index_ao`` / ``three_index_ri`` (value
+    g * damp[row]) from numpy's PCG64 streams, multithreaded; used only where
+    benchmark-sized host inputs are needed quickly and exact values do not
+    matter (CPU baseline timing)."""
+    out = np.empty((n_rows, n_df), order="F")
+    flat = out.reshape(-1, order="F")
+    ss = np.random.SeedSequence([seed, tag_of(name) & 0xFFFFFFFF])
+    chunk = 1 << 24
+    starts = list(range(0, flat.size, chunk))
+    children = ss.spawn(len(starts))
+
+    def work(q):
+        s = starts[q]
+        e = min(flat.size, s + chunk)
+        g = np.random.Generator(np.random.PCG64(children[q]))
+        g.standard_normal(out=flat[s:e])
+        flat[s:e] *= damp[np.arange(s, e) % n_rows]
+
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        list(ex.map(work, range(len(starts))))
+    return out
+
+
+def ao_damping(n_ao: int, decay: float) -> np.ndarray:
+    rows, cols = np.tril_indices(n_ao)
+    return np.exp(-np.abs(rows - cols).astype(np.float64) / decay)
+
+
+def ri_damping(n_ao: int, n_ri: int, decay: float) -> np.ndarray:
+    nr = n_ri * n_ao
+    return np.exp(-np.abs(np.arange(nr) % n_ri - np.arange(nr) // n_ri).astype(np.float64) / decay)
+
+
 def gaussian_matrix(seed: int, name: str, n_rows: int, n_cols: int, scale: float = 1.0) -> np.ndarray:
     key = stream_key(seed, name)
     return (normals(key, 0, n_rows * n_cols) * scale).reshape((n_rows, n_cols), order="F")

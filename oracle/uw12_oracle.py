@@ -55,13 +55,29 @@ class Sampler:
 
     ``max_iters=None`` runs every iteration.  Otherwise at most ``max_iters``
     evenly spaced iterations run and ``extra_seconds`` accumulates the
-    extrapolated time of the skipped ones (loop time * (n/k - 1)).
+    extrapolated time of the skipped ones (loop time * (n/k - 1)); large
+    products (``matmul``) likewise compute a leading block of rows and
+    extrapolate by the row count.
     """
 
-    def __init__(self, max_iters: Optional[int] = None):
+    def __init__(self, max_iters: Optional[int] = None, min_rows: int = 2048):
         self.max_iters = max_iters
+        self.min_rows = min_rows
         self.extra_seconds = 0.0
         self.loops = 0
+
+    def matmul(self, A: np.ndarray, B: np.ndarray) -> np.ndarray:
+        if self.max_iters is None:
+            return A @ B
+        n = A.shape[0]
+        k = min(n, max(self.min_rows, n // 64))
+        if k == n:
+            return A @ B
+        out = np.zeros((n, B.shape[1]))
+        t0 = time.perf_counter()
+        out[:k] = A[:k] @ B
+        self.extra_seconds += (time.perf_counter() - t0) * (n / k - 1.0)
+        return out
 
     def range(self, n: int):
         n = int(n)
@@ -393,7 +409,9 @@ class Integrals:
     def get_X3idx_one_trans(self):
         """integrals.cpp:213-248 (in-core J3_0 branch)."""
         if self._one is None:
-            self._one = [mo_transform_one_index_full(self.base.J3_0, c, self.sampler) @ self.base.P2
+            self._one = [self.sampler.matmul(mo_transform_one_index_full(self.base.J3_0, c,
+                                                                         self.sampler),
+                                             self.base.P2)
                          for c in self.occ]
         return self._one
 
@@ -402,7 +420,9 @@ class Integrals:
         if self._one_ri is None:
             if not self.base.has_J3_ri_0():
                 raise UW12RuntimeError("J3_ri_0 not stored")
-            self._one_ri = [transform_second_index(self.base.J3_ri_0, c, self.sampler) @ self.base.P2
+            self._one_ri = [self.sampler.matmul(transform_second_index(self.base.J3_ri_0, c,
+                                                                       self.sampler),
+                                                self.base.P2)
                             for c in self.act]
         return self._one_ri
 
@@ -700,13 +720,15 @@ def calculate_ttilde_dxab_incore(W: Integrals, V: Integrals, ttilde, abs_p: ABSP
     def W3_ri_fn(A):  # get_W3_ri_fn, :221-240
         return (Wb.J3_ri_0 @ Wb.P2[:, A]).reshape((n_ri, n_ao), order="F")
 
-    s = Vb.J3_0 @ Vb.P2 @ ttilde.T  # calculate_s_matrix, :242-250
+    # calculate_s_matrix (:242-250); Armadillo evaluates the triple product in
+    # the cheaper association J3_0 (P2 t~^T), as here.
+    s = sampler.matmul(Vb.J3_0, Vb.P2 @ ttilde.T)
     fock = np.zeros((n_ao, n_ao))
     for A in sampler.range(s.shape[1]):
         sA = square(s[:, A])
         fock -= square(W3_fn(A)) @ abs_p.s_inv_ao_ao @ sA
         fock -= W3_ri_fn(A).T @ abs_p.s_inv_ri_ao @ sA
-    p = Vb.J3_ri_0 @ Vb.P2 @ ttilde.T  # calculate_p_matrix, :288-296
+    p = sampler.matmul(Vb.J3_ri_0, Vb.P2 @ ttilde.T)  # calculate_p_matrix, :288-296
     for A in sampler.range(p.shape[1]):
         pA = p[:, A].reshape((n_ri, n_ao), order="F")
         fock -= square(W3_fn(A)) @ abs_p.s_inv_ao_ri @ pA

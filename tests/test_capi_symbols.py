@@ -1,0 +1,43 @@
+"""The C-ABI library loads on a machine without a GPU and exports every
+function declared in include/uw12_c.h (no compute calls)."""
+import ctypes
+import re
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "uw12_c.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(uw12c_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for must in ("uw12c_integrals_create", "uw12c_abs_create", "uw12c_fock", "uw12c_energy",
+                 "uw12c_form_fock", "uw12c_last_error"):
+        assert must in syms
+
+
+def test_library_exports_every_declared_symbol(uw12lib):
+    lib = ctypes.CDLL(str(uw12lib.library_path()))
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_version_and_error_state_without_gpu(uw12lib):
+    L = uw12lib.lib()
+    assert b"sm_100a" in L.uw12c_version()
+    buf = ctypes.create_string_buffer(64)
+    assert L.uw12c_last_error(buf, 64) == 0
+
+
+def test_invalid_arguments_are_rejected_without_touching_the_device(uw12lib):
+    L = uw12lib.lib()
+    out = ctypes.c_void_p()
+    # bad mem_kind and null output handle are argument errors (status 5)
+    assert L.uw12c_integrals_create(None, None, None, 3, 4, 0, 7, ctypes.byref(out)) == 5
+    assert L.uw12c_abs_create(None, 3, 4, 0, None) == 5
+    buf = ctypes.create_string_buffer(256)
+    assert L.uw12c_last_error(buf, 256) == 5 and buf.value
