@@ -41,6 +41,8 @@ CONFIGS = {
     # name: N, M, R, n_occ per spin, decay
     "c0": (24, 84, 116, (5,), 8.0),
     "c1": (500, 1500, 2000, (40, 38), 30.0),
+    # reduced c1 shape used for single-kernel ncu captures (inputs ~2 GB)
+    "c1s": (200, 600, 800, (16, 15), 30.0),
     "c2": (1200, 3600, 4800, (100,), 30.0),
 }
 

@@ -16,11 +16,10 @@ def pytest_configure(config):
 
 @pytest.fixture(scope="session")
 def uw12lib():
-    """The built CUDA library (builds it in-tree if missing)."""
+    """The built CUDA library (rebuilt in-tree when a source is newer)."""
     import libuw12_b200
-    if not libuw12_b200.library_path().exists():
-        from libuw12_b200 import build
-        build.build()
+    from libuw12_b200 import build
+    build.build()
     return libuw12_b200
 
 
