@@ -97,35 +97,73 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_dmma(const KParams p) {
   const int a_k0 = AK ? (tid & 15) : (tid >> 7);
   const int b_j0 = BNC ? (tid & 127) : (tid >> 4);
   const int b_k0 = BNC ? (tid >> 7) : (tid & 15);
+  // Offsets of element r = 0 within a (batch, k-tile) block, and the step per r.
+  const long long a_base = AK ? (a_k0 + p.lda * (m0 + a_i0)) : (m0 + a_i0 + p.lda * a_k0);
+  const long long a_step = AK ? 16 * p.lda : 2 * p.lda;
+  const long long a_kstep = AK ? BK : BK * p.lda;  // advance of one k-tile
+  const long long b_base = BNC ? (n0 + b_j0 + p.ldb * b_k0) : (b_k0 + p.ldb * (n0 + b_j0));
+  const long long b_step = BNC ? 2 * p.ldb : 16 * p.ldb;
+  const long long b_kstep = BNC ? BK * p.ldb : BK;
+  // Rows / columns this thread loads that lie inside the matrix (bit r).
+  unsigned a_rows_ok = 0, b_cols_ok = 0;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const long long gi = m0 + (AK ? a_i0 + 16 * r : a_i0);
+    const long long gj = n0 + (BNC ? b_j0 : b_j0 + 16 * r);
+    a_rows_ok |= (gi < p.m ? 1u : 0u) << r;
+    b_cols_ok |= (gj < p.n ? 1u : 0u) << r;
+  }
 
-  auto load_stage = [&](int slot, long long kt) {
-    const long long br = kt / p.ktiles_pb;
-    const long long kin = (kt - br * p.ktiles_pb) * BK;
-    const long long br1 = br % p.nbr1;
+  // Incremental (reduction batch, k offset) iterator of the next stage to load:
+  // no integer division inside the main loop.
+  long long it_kin, it_br1;
+  const double* itA;
+  const double* itB;
+  {
+    const long long br = kt_begin / p.ktiles_pb;
+    it_kin = (kt_begin - br * p.ktiles_pb) * BK;
+    it_br1 = br % p.nbr1;
     const long long br2 = br / p.nbr1;
-    const double* Ar = Ab + br1 * p.sAr1 + br2 * p.sAr2;
-    const double* Br = Bb + br1 * p.sBr1 + br2 * p.sBr2;
+    itA = Ab + it_br1 * p.sAr1 + br2 * p.sAr2 + (it_kin / BK) * a_kstep;
+    itB = Bb + it_br1 * p.sBr1 + br2 * p.sBr2 + (it_kin / BK) * b_kstep;
+  }
+  const long long k_pad = p.ktiles_pb * BK;
+
+  auto load_stage = [&](int slot) {
     double* as = As + slot * A_STAGE;
     double* bs = Bs + slot * B_STAGE;
+    const double* pa = itA + a_base;
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
-      int i, kk;
-      if (AK) { i = a_i0 + 16 * r; kk = a_k0; } else { i = a_i0; kk = a_k0 + 2 * r; }
-      const long long gi = m0 + i, gk = kin + kk;
-      const bool v = (gi < p.m) && (gk < p.k);
-      const double* src = v ? (AK ? Ar + gk + p.lda * gi : Ar + gi + p.lda * gk) : p.A;
+      const int i = AK ? a_i0 + 16 * r : a_i0;
+      const int kk = AK ? a_k0 : a_k0 + 2 * r;
+      const bool v = ((a_rows_ok >> r) & 1u) && (it_kin + kk < p.k);
       double* dst = AK ? as + i * LDK + kk : as + kk * LDW + i;
-      cp_async8(dst, src, v);
+      cp_async8(dst, v ? pa + r * a_step : p.A, v);
     }
+    const double* pb = itB + b_base;
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
-      int j, kk;
-      if (BNC) { j = b_j0; kk = b_k0 + 2 * r; } else { j = b_j0 + 16 * r; kk = b_k0; }
-      const long long gj = n0 + j, gk = kin + kk;
-      const bool v = (gj < p.n) && (gk < p.k);
-      const double* src = v ? (BNC ? Br + gj + p.ldb * gk : Br + gk + p.ldb * gj) : p.B;
+      const int j = BNC ? b_j0 : b_j0 + 16 * r;
+      const int kk = BNC ? b_k0 + 2 * r : b_k0;
+      const bool v = ((b_cols_ok >> r) & 1u) && (it_kin + kk < p.k);
       double* dst = BNC ? bs + kk * LDW + j : bs + j * LDK + kk;
-      cp_async8(dst, src, v);
+      cp_async8(dst, v ? pb + r * b_step : p.B, v);
+    }
+    // advance to the next k-tile / reduction batch
+    it_kin += BK;
+    itA += a_kstep;
+    itB += b_kstep;
+    if (it_kin >= k_pad) {
+      const long long back = p.ktiles_pb;
+      it_kin = 0;
+      itA += p.sAr1 - back * a_kstep;
+      itB += p.sBr1 - back * b_kstep;
+      if (++it_br1 == p.nbr1) {
+        it_br1 = 0;
+        itA += p.sAr2 - p.nbr1 * p.sAr1;
+        itB += p.sBr2 - p.nbr1 * p.sBr1;
+      }
     }
   };
 
@@ -139,7 +177,7 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_dmma(const KParams p) {
 
 #pragma unroll
   for (int s = 0; s < STAGES - 1; ++s) {
-    if (kt_begin + s < kt_end) load_stage(s, kt_begin + s);
+    if (kt_begin + s < kt_end) load_stage(s);
     cp_async_commit();
   }
 
@@ -148,7 +186,7 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_dmma(const KParams p) {
     __syncthreads();
     {
       const long long nxt = kt + STAGES - 1;
-      if (nxt < kt_end) load_stage(static_cast<int>((nxt - kt_begin) % STAGES), nxt);
+      if (nxt < kt_end) load_stage(static_cast<int>((nxt - kt_begin) % STAGES));
       cp_async_commit();
     }
     const int slot = static_cast<int>((kt - kt_begin) % STAGES);
