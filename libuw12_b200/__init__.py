@@ -204,7 +204,7 @@ class ABSProjectors:
 def setup_base_integrals(X3, X2, X3_ri=None, n_ao: Optional[int] = None,
                          n_df: Optional[int] = None, n_ri: int = 0,
                          device: bool = False) -> BaseIntegrals:
-    """``uw12::setup_base_integrals`` (libuw12.hpp:42-71).
+    """``uw12::setup_base_integrals`` (libuw12.hpp:42-70).
 
     With ``device=True`` the arguments are raw device pointers (ints) and the
     sizes must be given; otherwise they are host arrays (column-major).
@@ -242,7 +242,7 @@ def setup_base_integrals(X3, X2, X3_ri=None, n_ao: Optional[int] = None,
 
 
 def setup_abs_projectors(S, n_ao: int, n_ri: int, device: bool = False) -> ABSProjectors:
-    """``uw12::setup_abs_projectors`` (libuw12.hpp:81)."""
+    """``uw12::setup_abs_projectors`` (libuw12.hpp:80)."""
     h = ctypes.c_void_p()
     if device:
         st = lib().uw12c_abs_create(ctypes.c_void_p(S), n_ao, n_ri, MEM_DEVICE, ctypes.byref(h))
@@ -335,7 +335,7 @@ def form_fock(W: BaseIntegrals, V: BaseIntegrals, WV: BaseIntegrals, abs_p: ABSP
 
 def uw12_fock(W, V, WV, abs_p, orbitals, occ, n_active, scale_opp_spin, scale_same_spin,
               print_level: int = 0) -> Tuple[float, np.ndarray]:
-    """``uw12::uw12_fock`` (libuw12.hpp:155-167): returns (energy, fock) with
+    """``uw12::uw12_fock`` (libuw12.hpp:157-169): returns (energy, fock) with
     fock of shape n_ao x (n_ao * n_spin)."""
     indirect = not _nearly_zero(scale_same_spin)
     e, f, _ = form_fock(W, V, WV, abs_p, orbitals, occ, n_active, indirect, True, scale_opp_spin,
@@ -345,7 +345,7 @@ def uw12_fock(W, V, WV, abs_p, orbitals, occ, n_active, scale_opp_spin, scale_sa
 
 def uw12_energy(W, V, WV, abs_p, orbitals, occ, n_active, scale_opp_spin, scale_same_spin,
                 print_level: int = 0) -> float:
-    """``uw12::uw12_energy`` (libuw12.hpp:134-144)."""
+    """``uw12::uw12_energy`` (libuw12.hpp:129-140)."""
     indirect = not _nearly_zero(scale_same_spin)
     return form_fock(W, V, WV, abs_p, orbitals, occ, n_active, indirect, False, scale_opp_spin,
                      scale_same_spin, print_level)[0]
