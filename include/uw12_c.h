@@ -50,19 +50,19 @@ const char* uw12c_version(void);
 
 /* Replaces uw12::setup_base_integrals(X3, X2, X3_ri, n_ao, n_df, n_ri, copy)
  * (libuw12.hpp:42-50, libuw12.cpp:22-36) and, with X3_ri == NULL, the no-RI
- * overload (libuw12.hpp:65-71, libuw12.cpp:38-49).  The tensors are copied to
+ * overload (libuw12.hpp:64-70, libuw12.cpp:38-49).  The tensors are copied to
  * the device (mem_kind says where the caller's pointers live) and the metric
  * is diagonalised there: P2 = Q pinv(Lambda), df_vals = Lambda
  * (src/integrals/base_integrals.cpp:155-166). */
 int uw12c_integrals_create(const double* X3, const double* X2, const double* X3_ri, size_t n_ao,
                            size_t n_df, size_t n_ri, int mem_kind, uw12c_integrals** out);
 int uw12c_integrals_destroy(uw12c_integrals* h);
-/* BaseIntegrals::get_number_ao/df/ri (base_integrals.hpp:209-216). */
+/* BaseIntegrals::get_number_ao/df/ri (src/integrals/base_integrals.hpp:196-202). */
 int uw12c_integrals_dims(const uw12c_integrals* h, size_t* n_ao, size_t* n_df, size_t* n_ri);
-/* BaseIntegrals::get_df_vals (base_integrals.hpp:168-171): n_df values, host. */
+/* BaseIntegrals::get_df_vals (src/integrals/base_integrals.hpp:169): n_df values, host. */
 int uw12c_integrals_df_vals(const uw12c_integrals* h, double* out);
 
-/* Replaces uw12::setup_abs_projectors(S, n_ao, n_ri) (libuw12.hpp:81,
+/* Replaces uw12::setup_abs_projectors(S, n_ao, n_ri) (libuw12.hpp:80,
  * libuw12.cpp:51-56 -> src/three_electron/ri_utils.hpp:45-74). */
 int uw12c_abs_create(const double* S, size_t n_ao, size_t n_ri, int mem_kind, uw12c_abs** out);
 int uw12c_abs_destroy(uw12c_abs* h);
@@ -84,7 +84,7 @@ int uw12c_form_fock(const uw12c_integrals* W, const uw12c_integrals* V,
                     double scale_same_spin, size_t print_level, double* energy, double* terms,
                     double* fock, int fock_mem_kind);
 
-/* Replaces uw12::uw12_fock(double* fock, ...) (libuw12.hpp:155-167,
+/* Replaces uw12::uw12_fock(double* fock, ...) (libuw12.hpp:157-169,
  * libuw12.cpp:184-214) in its raw-pointer form: C is the setup_orbitals
  * buffer (n_ao x n_orb*n_spin), occ the setup_occupations buffer
  * (n_occ_alpha [+ n_occ_beta] values; n_occ_beta ignored for n_spin == 1),
@@ -96,7 +96,7 @@ int uw12c_fock(double* fock, const uw12c_integrals* W, const uw12c_integrals* V,
                size_t n_occ_beta, const size_t* n_active, double scale_opp_spin,
                double scale_same_spin, size_t print_level, double* energy);
 
-/* Replaces uw12::uw12_energy (libuw12.hpp:134-144, libuw12.cpp:156-182). */
+/* Replaces uw12::uw12_energy (libuw12.hpp:129-140, libuw12.cpp:156-182). */
 int uw12c_energy(const uw12c_integrals* W, const uw12c_integrals* V, const uw12c_integrals* WV,
                  const uw12c_abs* abs, const double* C, size_t n_ao, size_t n_orb, size_t n_spin,
                  const double* occ, size_t n_occ_alpha, size_t n_occ_beta,
@@ -129,6 +129,27 @@ int uw12c_dgemm(long long m, long long n, long long k, double alpha, const doubl
                 double beta, double* C, long long ldc, long long nbo1, long long nbo2,
                 const long long* so, long long nbr1, long long nbr2, const long long* sr,
                 int split);
+
+/* uw12c_dgemm for callers that cannot allocate device memory (no counterpart
+ * in libuw12).  Host programs that reserve the whole device heap for their own
+ * memory pool at start-up, and code paths where a cudaMalloc/cudaFree would
+ * fail or synchronise the device (cudaFree waits for all streams), cannot let
+ * the library allocate; this entry point allocates nothing.  The caller still
+ * passes A, B and C.  Split-K partial tiles go to one fixed device array of
+ * UW12C_NOALLOC_SCRATCH_DOUBLES doubles (16 MiB) that every device which
+ * loads the library keeps until the process exits.  An explicit split > 1
+ * whose partials (split * nbo1 * nbo2 * m * n doubles) do not fit is rejected
+ * with UW12C_ERR_INVALID; split = 0 chooses a split that fits (1 needs no
+ * scratch).  All calls share the array, so calls that overlap on the GPU
+ * race; the partial tiles are fully overwritten by each call, so nothing has
+ * to start at zero.  The first call on a device looks up the array's device
+ * address (once per device); make that first call before any stream capture. */
+#define UW12C_NOALLOC_SCRATCH_DOUBLES (1LL << 21)
+int uw12c_dgemm_noalloc(long long m, long long n, long long k, double alpha, const double* A,
+                        long long lda, int a_kcontig, const double* B, long long ldb,
+                        int b_ncontig, double beta, double* C, long long ldc, long long nbo1,
+                        long long nbo2, const long long* so, long long nbr1, long long nbr2,
+                        const long long* sr, int split);
 
 /* Deterministic synthetic three-index tensors written on the device (no
  * counterpart in libuw12; benchmark input generation).  Element e of the

@@ -343,6 +343,31 @@ int uw12c_dgemm(long long m, long long n, long long k, double alpha, const doubl
   });
 }
 
+int uw12c_dgemm_noalloc(long long m, long long n, long long k, double alpha, const double* A,
+                        long long lda, int a_kcontig, const double* B, long long ldb,
+                        int b_ncontig, double beta, double* C, long long ldc, long long nbo1,
+                        long long nbo2, const long long* so, long long nbr1, long long nbr2,
+                        const long long* sr, int split) {
+  static_assert(UW12C_NOALLOC_SCRATCH_DOUBLES == uw12b::kNoAllocScratchDoubles,
+                "scratch size of the header and the library differ");
+  return guarded([&] {
+    uw12b::GemmDesc d;
+    d.m = m; d.n = n; d.k = k; d.alpha = alpha; d.beta = beta;
+    d.A = A; d.lda = lda; d.a_kcontig = a_kcontig != 0;
+    d.B = B; d.ldb = ldb; d.b_ncontig = b_ncontig != 0;
+    d.C = C; d.ldc = ldc;
+    d.nbo1 = nbo1; d.nbo2 = nbo2;
+    if (so) { d.sAo1 = so[0]; d.sAo2 = so[1]; d.sBo1 = so[2]; d.sBo2 = so[3]; d.sCo1 = so[4]; d.sCo2 = so[5]; }
+    d.nbr1 = nbr1; d.nbr2 = nbr2;
+    if (sr) { d.sAr1 = sr[0]; d.sAr2 = sr[1]; d.sBr1 = sr[2]; d.sBr2 = sr[3]; }
+    d.split = split;
+    need(m >= 0 && n >= 0 && k >= 0 && nbo1 >= 0 && nbo2 >= 0 && nbr1 >= 0 && nbr2 >= 0 &&
+             split >= 0,
+         "negative size");
+    uw12b::gemm_noalloc(d);
+  });
+}
+
 int uw12c_synth_three_index(double* out_device, int kind, size_t n_ao, size_t n_ri, size_t n_df,
                             unsigned long long seed, unsigned long long tag, double decay) {
   return guarded([&] {

@@ -1,7 +1,9 @@
 // FP64 DMMA GEMM for sm_100a: 128x128x16 CTA tiles, 8 warps of 64x32,
 // 4-stage cp.async pipeline, m16n8k4 f64 tensor-core MMAs.
 #include <algorithm>
+#include <cmath>
 #include <mutex>
+#include <string>
 
 #include "gemm_f64.cuh"
 
@@ -432,6 +434,129 @@ void gemm(const GemmDesc& d) {
     g_prof_recs.push_back({ev_a, ev_b, 2.0 * double(d.m) * double(d.n) * double(d.k) *
                                            double(nbo) * double(nbr)});
   }
+}
+
+// ---- allocation-free variant -------------------------------------------------
+namespace {
+
+// Kernel parameters and split-K factor of an allocation-free call (the same
+// choice gemm() makes).  Returns false for an empty output; *empty_k is set
+// when the contraction is empty (C = beta C).
+bool prepare(const GemmDesc& d, KParams& p, bool* empty_k) {
+  const long long nbo = d.nbo1 * d.nbo2;
+  const long long nbr = d.nbr1 * d.nbr2;
+  *empty_k = false;
+  if (d.m <= 0 || d.n <= 0 || nbo <= 0) return false;
+  if (d.k <= 0 || nbr <= 0) {
+    *empty_k = true;
+    return true;
+  }
+  if (!d.A || !d.B || !d.C) throw Error(kErrInvalid, "gemm: null operand");
+  p = KParams{};
+  p.A = d.A; p.B = d.B; p.C = d.C;
+  p.lda = d.lda; p.ldb = d.ldb; p.ldc = d.ldc;
+  p.m = d.m; p.n = d.n; p.k = d.k;
+  p.alpha = d.alpha; p.beta = d.beta;
+  p.nbo1 = d.nbo1; p.nbo = nbo;
+  p.sAo1 = d.sAo1; p.sAo2 = d.sAo2; p.sBo1 = d.sBo1; p.sBo2 = d.sBo2;
+  p.sCo1 = d.sCo1; p.sCo2 = d.sCo2;
+  p.nbr1 = d.nbr1;
+  p.sAr1 = d.sAr1; p.sAr2 = d.sAr2; p.sBr1 = d.sBr1; p.sBr2 = d.sBr2;
+  p.tiles_m = (d.m + BM - 1) / BM;
+  const long long tiles_n = (d.n + BN - 1) / BN;
+  p.tiles_mn = p.tiles_m * tiles_n;
+  p.ktiles_pb = (d.k + BK - 1) / BK;
+  p.ktiles_total = p.ktiles_pb * nbr;
+  const long long ctas = p.tiles_mn * nbo;
+  int split = d.split;
+  if (split <= 0) {
+    constexpr long long kSMs = 148;
+    split = 1;
+    if (ctas < kSMs) {
+      long long want = (kSMs + ctas - 1) / ctas;
+      long long cap = std::max<long long>(1, p.ktiles_total / 8);  // >= 128 k per split
+      split = static_cast<int>(std::min<long long>(std::min(want, cap), 64));
+    }
+  }
+  p.split = static_cast<int>(std::max<long long>(1, std::min<long long>(split, p.ktiles_total)));
+  return true;
+}
+
+void launch_scale_only(const GemmDesc& d, cudaStream_t s) {
+  if (d.beta == 1.0) return;
+  const long long nbo = d.nbo1 * d.nbo2;
+  const long long total = d.m * d.n * nbo;
+  const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 16));
+  scale_only<<<blocks, 256, 0, s>>>(d.m, d.n, nbo, d.nbo1, d.beta, d.C, d.ldc, d.sCo1, d.sCo2);
+  UW12_LAUNCHED();
+}
+
+// Launches the GEMM (and the split-K reduction when p.split > 1, with
+// partial tiles in p.work).
+void launch(const GemmDesc& d, const KParams& p, cudaStream_t s) {
+  const long long grid = p.tiles_mn * p.nbo * p.split;
+  if (!d.a_kcontig && !d.b_ncontig) launch_variant<false, false>(p, grid, s);
+  else if (!d.a_kcontig && d.b_ncontig) launch_variant<false, true>(p, grid, s);
+  else if (d.a_kcontig && !d.b_ncontig) launch_variant<true, false>(p, grid, s);
+  else launch_variant<true, true>(p, grid, s);
+  if (p.split > 1) {
+    const long long total = d.m * d.n * p.nbo;
+    const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 16));
+    splitk_reduce<<<blocks, 256, 0, s>>>(p.work, p.split, d.m, d.n, p.nbo, d.nbo1, d.alpha,
+                                         d.beta, d.C, d.ldc, d.sCo1, d.sCo2);
+    UW12_LAUNCHED();
+  }
+}
+
+}  // namespace
+
+// Split-K partial tiles normally live in a stream-ordered allocation.  For
+// callers that must not allocate, they go into this fixed device array
+// instead: every device that loads the library keeps it (16 MiB) until the
+// process exits.  Host code cannot use the symbol itself as a pointer (it is a
+// host-side shadow), so the device address is looked up once per device.
+namespace {
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+std::mutex g_scratch_mu;
+double* g_scratch_ptr[64] = {};
+
+double* noalloc_scratch_for_current_device() {
+  int dev = 0;
+  UW12_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw Error(kErrInvalid, "gemm_noalloc: device index out of range");
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_ptr[dev]) {
+    void* ptr = nullptr;
+    UW12_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    g_scratch_ptr[dev] = static_cast<double*>(ptr);
+  }
+  return g_scratch_ptr[dev];
+}
+}  // namespace
+
+void gemm_noalloc(const GemmDesc& d) {
+  KParams p;
+  bool empty_k = false;
+  if (!prepare(d, p, &empty_k)) return;
+  cudaStream_t s = current_stream();
+  if (empty_k) {
+    launch_scale_only(d, s);
+    return;
+  }
+  const double per_split = double(p.nbo) * double(d.m) * double(d.n);
+  if (d.split > 1 && per_split * p.split > double(kNoAllocScratchDoubles))
+    throw Error(kErrInvalid,
+                "gemm_noalloc: split * batches * m * n = " +
+                    std::to_string(static_cast<long long>(per_split * p.split)) +
+                    " doubles exceeds the fixed scratch of " +
+                    std::to_string(kNoAllocScratchDoubles) + " doubles (16 MiB)");
+  if (p.split > 1 && per_split * p.split > double(kNoAllocScratchDoubles)) {
+    // automatic split: shrink it until the partial tiles fit (split 1 needs none)
+    p.split = static_cast<int>(std::max(1.0, std::floor(kNoAllocScratchDoubles / per_split)));
+  }
+  if (p.split > 1) p.work = noalloc_scratch_for_current_device();
+  launch(d, p, s);
 }
 
 }  // namespace uw12b

@@ -46,6 +46,15 @@ struct GemmDesc {
 // no reduction batches scales C by beta).
 void gemm(const GemmDesc& d);
 
+// Same contraction without any device allocation: split-K partial tiles go
+// to a fixed per-device array of kNoAllocScratchDoubles doubles (16 MiB).  An
+// explicit split > 1 whose partials (split * batches * m * n doubles) exceed it
+// is rejected; an automatic split is reduced until they fit.  The array is
+// shared by all calls: calls that overlap on the GPU race.  The first call on
+// a device looks up the array's device address (once per device).
+constexpr long long kNoAllocScratchDoubles = 1LL << 21;
+void gemm_noalloc(const GemmDesc& d);
+
 // Convenience wrappers in BLAS terms (column-major, 'N'/'T').
 inline GemmDesc gemm_nn(long long m, long long n, long long k, double alpha, const double* A,
                         long long lda, const double* B, long long ldb, double beta, double* C,
