@@ -373,6 +373,7 @@ def main():
         dist.barrier()
     launches = L.launch_count() - n0
     prof = L.profile_read()
+    phases = {k: v / args.steps for k, v in L.profile_phases().items()}
     L.profile_enable(False)
     clk = clocks.stop()
     elapsed = ev0.elapsed_time(ev1) / 1e3
@@ -470,6 +471,7 @@ def main():
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "phases_ms_per_step": phases,
             "gpu_launches": int(launches),
             "clocks": clk,
         }

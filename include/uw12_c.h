@@ -114,6 +114,9 @@ int uw12c_set_memory_budget(size_t bytes);
 unsigned long long uw12c_launch_count(void);
 int uw12c_profile_enable(int on);
 int uw12c_profile_read(unsigned long long* gemm_launches, double* gemm_ms, double* gemm_flops);
+/* Device time per phase of the evaluation accumulated while profiling is on,
+ * as "phase=milliseconds;..." (truncated to len); reading resets it. */
+int uw12c_profile_phases(char* buf, size_t len);
 
 /* The FP64 tensor-core GEMM engine on device pointers (no counterpart in
  * libuw12, which calls BLAS dgemm through Armadillo):

@@ -91,6 +91,7 @@ def lib():
     L.uw12c_launch_count.restype = ctypes.c_ulonglong
     L.uw12c_profile_enable.argtypes = [ctypes.c_int]
     L.uw12c_profile_read.argtypes = [ctypes.POINTER(ctypes.c_ulonglong), PD, PD]
+    L.uw12c_profile_phases.argtypes = [ctypes.c_char_p, c_sz]
     LL = ctypes.c_longlong
     L.uw12c_dgemm.argtypes = [LL, LL, LL, c_d, P, LL, ctypes.c_int, P, LL, ctypes.c_int, c_d, P,
                               LL, LL, LL, ctypes.POINTER(LL), LL, LL, ctypes.POINTER(LL),
@@ -383,6 +384,18 @@ def dgemm(m, n, k, alpha, A, lda, a_kcontig, B, ldb, b_ncontig, beta, C, ldc, nb
     _check(lib().uw12c_dgemm(m, n, k, alpha, ctypes.c_void_p(A), lda, int(a_kcontig),
                              ctypes.c_void_p(B), ldb, int(b_ncontig), beta, ctypes.c_void_p(C),
                              ldc, nbo1, nbo2, LLa(*so), nbr1, nbr2, LLr(*sr), int(split)))
+
+
+def profile_phases() -> dict:
+    """Device milliseconds per evaluation phase since the last read."""
+    buf = ctypes.create_string_buffer(4096)
+    _check(lib().uw12c_profile_phases(buf, 4096))
+    out = {}
+    for item in buf.value.decode().split(";"):
+        if "=" in item:
+            k, v = item.split("=", 1)
+            out[k] = float(v)
+    return out
 
 
 def synth_three_index(out_ptr: int, kind: int, n_ao: int, n_ri: int, n_df: int, seed: int,

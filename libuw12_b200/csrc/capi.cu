@@ -321,6 +321,15 @@ int uw12c_profile_read(unsigned long long* gemm_launches, double* gemm_ms, doubl
   });
 }
 
+int uw12c_profile_phases(char* buf, size_t len) {
+  return guarded([&] {
+    need(buf != nullptr && len > 0, "null buffer");
+    const std::string s = uw12b::phase_profile_read();
+    std::strncpy(buf, s.c_str(), len - 1);
+    buf[len - 1] = '\0';
+  });
+}
+
 int uw12c_dgemm(long long m, long long n, long long k, double alpha, const double* A,
                 long long lda, int a_kcontig, const double* B, long long ldb, int b_ncontig,
                 double beta, double* C, long long ldc, long long nbo1, long long nbo2,

@@ -24,6 +24,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <string>
 
 #include "engine.cuh"
@@ -202,6 +204,41 @@ AbsHandle* abs_create(const double* S, size_t n_ao, size_t n_ri, bool device_mem
 // --------------------------------------------------------------------------
 namespace {
 
+// Phase timing: events recorded at phase boundaries while profiling is on.
+std::mutex g_phase_mu;
+std::map<std::string, double> g_phase_ms;
+
+class PhaseClock {
+ public:
+  PhaseClock() : on_(profile_enabled()) {}
+  ~PhaseClock() {
+    if (!on_) return;
+    for (auto& m : marks_) cudaEventDestroy(m.second);
+  }
+  void mark(const char* name) {
+    if (!on_) return;
+    cudaEvent_t e;
+    UW12_CUDA(cudaEventCreate(&e));
+    UW12_CUDA(cudaEventRecord(e, current_stream()));
+    marks_.emplace_back(name, e);
+  }
+  // Accumulates the time from each mark to the next into its phase.
+  void finish() {
+    if (!on_ || marks_.size() < 2) return;
+    UW12_CUDA(cudaEventSynchronize(marks_.back().second));
+    std::lock_guard<std::mutex> lk(g_phase_mu);
+    for (size_t i = 0; i + 1 < marks_.size(); ++i) {
+      float ms = 0.f;
+      UW12_CUDA(cudaEventElapsedTime(&ms, marks_[i].second, marks_[i + 1].second));
+      g_phase_ms[marks_[i].first] += ms;
+    }
+  }
+
+ private:
+  bool on_;
+  std::vector<std::pair<std::string, cudaEvent_t>> marks_;
+};
+
 enum Slot { kE2d = 0, kE2i = 1, kE3d = 2, kE3i = 3, kE4d = 4, kE4i = 5, kSlots = 8 };
 
 double spin_factor(int ns, int s, int sp, double s_os, double s_ss) {
@@ -269,6 +306,8 @@ void form_fock(const FockRequest& rq) {
     a_tot += sd[s].a;
   }
 
+  PhaseClock clock;
+  clock.mark("orbitals");
   // ---- occupation-weighted orbitals (utils.hpp:289-310), freeze_core (:235-253)
   DevBuf Co(N * o_tot), Ca(N * a_tot), wts(o_tot);
   {
@@ -305,6 +344,7 @@ void form_fock(const FockRequest& rq) {
   // =====================================================================
   // two-electron term (two_electron.cpp:11-153), WV integrals, active orbitals
   // =====================================================================
+  clock.mark("two_electron");
   {
     DevBuf dmat(np * ns), XDr(MX * ns), XD(MX * ns);
     for (int s = 0; s < ns; ++s) pack_density(Ca_s(s), LL(N), LL(N), LL(sd[s].a), two, dmat.get() + np * s);
@@ -366,6 +406,7 @@ void form_fock(const FockRequest& rq) {
   // =====================================================================
   // MO transforms for W and V (integrals.cpp:184-345)
   // =====================================================================
+  clock.mark("transforms");
   struct PerX {
     std::vector<DevBuf> B1, B2, Wst, SV;
   };
@@ -428,6 +469,7 @@ void form_fock(const FockRequest& rq) {
   // X_AB, t, t~ and the direct energies (direct_utils.cpp:62-157,
   // four_electron.cpp:80-137)
   // =====================================================================
+  clock.mark("xab_t_energies");
   std::vector<DevBuf> Xab(ns), tab(ns), ttl(ns);
   for (int s = 0; s < ns; ++s) {
     const size_t o = sd[s].o, a = sd[s].a;
@@ -467,6 +509,7 @@ void form_fock(const FockRequest& rq) {
   // (direct_utils.cpp:256-347) added to fock[sigma'] (three_electron.cpp:78)
   // =====================================================================
   if (calc) {
+    clock.mark("direct_fock");
     for (int s = 0; s < ns; ++s) {
       const size_t o = sd[s].o, a = sd[s].a, c = sd[s].c;
       if (!o) continue;
@@ -491,6 +534,7 @@ void form_fock(const FockRequest& rq) {
       gemm(gf);
     }
     // t~ dX: F[sigma'] -= sum_ab T2[a,b] G_W[a]^T S^-1 G_V[b], T2 = P2_W Tc P2_V^T
+    clock.mark("tdx_fock");
     for (int sp = 0; sp < ns; ++sp) {
       const double* Tq[2] = {ttl[0].get(), ns > 1 ? ttl[1].get() : nullptr};
       double cT[2] = {0, 0}, cX[2] = {0, 0};
@@ -556,6 +600,7 @@ void form_fock(const FockRequest& rq) {
       DevBuf b2wl(ao * MW), b2vl(ao * MV);
       scale_rc(XW.B2[s].get(), LL(ao), LL(ao), LL(MW), nullptr, W.lam.get(), 1.0, b2wl.get(), LL(ao));
       scale_rc(XV.B2[s].get(), LL(ao), LL(ao), LL(MV), nullptr, V.lam.get(), 1.0, b2vl.get(), LL(ao));
+      clock.mark("ss_4el_energy");
       // ---- 4-el indirect energy (four_electron.cpp:143-179)
       {
         DevBuf W4(ao * ao), V4(ao * ao);
@@ -569,6 +614,7 @@ void form_fock(const FockRequest& rq) {
         gemm(g);
         permdot_4el(W4.get(), V4.get(), LL(a), LL(o), -0.5 * two, acc.get(), kE4i);
       }
+      clock.mark("ss_3el_energy");
       // ---- 3-el indirect energy (indirect_utils.cpp:101-133), chunked over k
       {
         const size_t per_k = 2 * Rp * a * a;
@@ -591,6 +637,7 @@ void form_fock(const FockRequest& rq) {
       DevBuf b1wl(No * MW), b1vl(No * MV);
       scale_rc(XW.B1[s].get(), LL(No), LL(No), LL(MW), nullptr, W.lam.get(), 1.0, b1wl.get(), LL(No));
       scale_rc(XV.B1[s].get(), LL(No), LL(No), LL(MV), nullptr, V.lam.get(), 1.0, b1vl.get(), LL(No));
+      clock.mark("ss_4el_fock");
       // ---- 4-el indirect Fock (four_electron.cpp:181-249)
       {
         DevBuf W43(No * ao), V43(No * ao);
@@ -626,6 +673,7 @@ void form_fock(const FockRequest& rq) {
           gemm(gf);
         }
       }
+      clock.mark("ss_3el_fock");
       // ---- 3-el indirect Fock (indirect_utils.cpp:139-345), chunked over k
       {
         DevBuf xhW(MW * ao), xhV(MV * ao);
@@ -711,6 +759,7 @@ void form_fock(const FockRequest& rq) {
   // =====================================================================
   // energies and the symmetrised Fock matrix
   // =====================================================================
+  clock.mark("finish");
   double e[kSlots];
   UW12_CUDA(cudaMemcpyAsync(e, acc.get(), sizeof(e), cudaMemcpyDeviceToHost, st));
   if (rq.fock && calc) {
@@ -734,6 +783,8 @@ void form_fock(const FockRequest& rq) {
     }
     UW12_CUDA(cudaStreamSynchronize(st));
   }
+  clock.mark("end");
+  clock.finish();
   const double e2 = e[kE2d] + (do_ind ? s_ss * e[kE2i] : 0.0);
   const double e3 = e[kE3d] + (do_ind ? s_ss * e[kE3i] : 0.0);
   const double e4 = e[kE4d] + (do_ind ? s_ss * e[kE4i] : 0.0);
@@ -766,6 +817,14 @@ void form_fock(const FockRequest& rq) {
     res("Total UW12 energy", total);
     std::fflush(stdout);
   }
+}
+
+std::string phase_profile_read() {
+  std::lock_guard<std::mutex> lk(g_phase_mu);
+  std::string out;
+  for (const auto& kv : g_phase_ms) out += kv.first + "=" + std::to_string(kv.second) + ";";
+  g_phase_ms.clear();
+  return out;
 }
 
 }  // namespace uw12b

@@ -2,6 +2,7 @@
 // pair-loop-free FP64 schedule of libuw12's form_fock (src/uw12.cpp:22-119).
 #pragma once
 
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -78,5 +79,9 @@ struct FockRequest {
 };
 
 void form_fock(const FockRequest& rq);
+
+// Device time per schedule phase accumulated while GEMM profiling is on
+// ("name=ms;..."); reading resets the accumulators.
+std::string phase_profile_read();
 
 }  // namespace uw12b

@@ -340,6 +340,11 @@ void profile_enable(bool on) {
   g_prof_on = on;
 }
 
+bool profile_enabled() {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  return g_prof_on;
+}
+
 void profile_reset() {
   std::lock_guard<std::mutex> lk(g_prof_mu);
   prof_collect_locked();

@@ -73,6 +73,7 @@ struct KernelStats {
   double flops = 0.0;  // algorithmic 2*m*n*k per launch
 };
 void profile_enable(bool on);
+bool profile_enabled();
 KernelStats profile_read_gemm();  // synchronises the recorded events
 void profile_reset();
 
