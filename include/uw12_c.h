@@ -111,6 +111,9 @@ int uw12c_energy(const uw12c_integrals* W, const uw12c_integrals* V, const uw12c
  * profiling is on). */
 int uw12c_set_stream(void* stream);
 int uw12c_set_memory_budget(size_t bytes);
+/* The library keeps device memory freed by one call reserved for the next
+ * (its own stream-ordered pool); this returns the unused part to the system. */
+int uw12c_trim_memory(void);
 unsigned long long uw12c_launch_count(void);
 int uw12c_profile_enable(int on);
 int uw12c_profile_read(unsigned long long* gemm_launches, double* gemm_ms, double* gemm_flops);

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 
 #include "../../include/uw12_c.h"
@@ -36,6 +37,37 @@ void note_launch(const char* file, int line) {
 unsigned long long launch_count() { return g_launches.load(); }
 cudaStream_t current_stream() { return g_stream; }
 void set_current_stream(cudaStream_t s) { g_stream = s; }
+
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+}  // namespace
+
+cudaMemPool_t library_pool() {
+  int dev = 0;
+  UW12_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw Error(kErrInvalid, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    UW12_CUDA(cudaMemPoolCreate(&pool, &props));
+    unsigned long long thr = ~0ULL;
+    UW12_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    g_pools[dev] = pool;
+  }
+  return g_pools[dev];
+}
+
+void trim_pools() {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  for (int d = 0; d < 64; ++d)
+    if (g_pools[d]) UW12_CUDA(cudaMemPoolTrimTo(g_pools[d], 0));
+}
 
 }  // namespace uw12b
 
@@ -297,6 +329,10 @@ int uw12c_energy(const uw12c_integrals* W, const uw12c_integrals* V, const uw12c
 
 int uw12c_set_stream(void* stream) {
   return guarded([&] { uw12b::set_current_stream(static_cast<cudaStream_t>(stream)); });
+}
+
+int uw12c_trim_memory(void) {
+  return guarded([&] { uw12b::trim_pools(); });
 }
 
 int uw12c_set_memory_budget(size_t bytes) {

@@ -50,7 +50,13 @@ unsigned long long launch_count();
 cudaStream_t current_stream();
 void set_current_stream(cudaStream_t s);
 
-// Device memory from the stream-ordered pool of the current device.
+// The library's own stream-ordered memory pool on the current device.  It
+// keeps freed memory reserved (release threshold = max) so repeated calls do
+// not map and unmap pages; trim_pools() returns it to the system.
+cudaMemPool_t library_pool();
+void trim_pools();
+
+// Device memory from the library's stream-ordered pool of the current device.
 class DevBuf {
  public:
   DevBuf() = default;
@@ -68,7 +74,9 @@ class DevBuf {
     release();
     s_ = s ? s : current_stream();
     n_ = n_doubles;
-    if (n_) UW12_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p_), n_ * sizeof(double), s_));
+    if (n_)
+      UW12_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p_), n_ * sizeof(double),
+                                        library_pool(), s_));
   }
   void zero() {
     if (n_) UW12_CUDA(cudaMemsetAsync(p_, 0, n_ * sizeof(double), s_));

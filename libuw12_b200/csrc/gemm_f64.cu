@@ -290,6 +290,30 @@ __global__ void scale_only(long long m, long long n, long long nbo, long long nb
   }
 }
 
+// Split-K factor: the CTAs of one launch run in waves of 148 (one per SM), so
+// a launch with few output tiles, or with a last wave that is mostly empty,
+// splits the contraction to fill the waves.  A split must keep >= 512 of k
+// per CTA so the partial-tile round trip stays small against the MMA work.
+int choose_split(long long ctas, long long ktiles_total) {
+  constexpr long long kSMs = 148;
+  auto eff = [&](long long c) {
+    const long long waves = (c + kSMs - 1) / kSMs;
+    return double(c) / double(waves * kSMs);
+  };
+  if (ctas >= 8 * kSMs) return 1;
+  int best = 1;
+  double best_eff = eff(ctas);
+  for (int s = 2; s <= 64; ++s) {
+    if (ktiles_total / s < 32) break;
+    const double e = eff(ctas * s);
+    if (e > best_eff + 0.05) {
+      best = s;
+      best_eff = e;
+    }
+  }
+  return best;
+}
+
 template <bool AK, bool BNC>
 void launch_variant(const KParams& p, long long grid, cudaStream_t s) {
   static bool attr_set[64] = {};
@@ -390,15 +414,7 @@ void gemm(const GemmDesc& d) {
 
   const long long ctas = p.tiles_mn * nbo;
   int split = d.split;
-  if (split <= 0) {
-    constexpr long long kSMs = 148;
-    split = 1;
-    if (ctas < kSMs) {
-      long long want = (kSMs + ctas - 1) / ctas;
-      long long cap = std::max<long long>(1, p.ktiles_total / 8);  // >= 128 k per split
-      split = static_cast<int>(std::min<long long>(std::min(want, cap), 64));
-    }
-  }
+  if (split <= 0) split = choose_split(ctas, p.ktiles_total);
   split = static_cast<int>(std::max<long long>(1, std::min<long long>(split, p.ktiles_total)));
   p.split = split;
 
