@@ -266,6 +266,28 @@ void transform_ao(const IntegralsHandle& X, const double* Cm, size_t nc, double*
   }
 }
 
+// Chunk size c <= max_chunk (in units of `unit` GEMM columns) for a loop over
+// `total` units: the chunked GEMMs have n = unit * c columns, so c is chosen
+// to fill the 128-wide column tiles over the whole loop (fewest wasted
+// columns, then the largest chunk).
+size_t tile_chunk(size_t total, size_t unit, size_t max_chunk) {
+  max_chunk = std::max<size_t>(1, std::min(max_chunk, total));
+  auto tiles = [](size_t cols) { return (cols + 127) / 128; };
+  size_t best = max_chunk;
+  double best_fill = -1.0;
+  for (size_t c = max_chunk; c >= std::max<size_t>(1, max_chunk / 2); --c) {
+    const size_t full = total / c, rem = total % c;
+    const size_t used = full * tiles(unit * c) + (rem ? tiles(unit * rem) : 0);
+    const double fill = double(total * unit) / double(used * 128);
+    if (fill > best_fill + 1e-9) {
+      best_fill = fill;
+      best = c;
+    }
+    if (c == 1) break;
+  }
+  return best;
+}
+
 struct SpinDims {
   size_t o = 0, a = 0, c = 0, ooff = 0, aoff = 0;
 };
@@ -533,8 +555,14 @@ void form_fock(const FockRequest& rq) {
       gf.b_ncontig = true;
       gemm(gf);
     }
-    // t~ dX: F[sigma'] -= sum_ab T2[a,b] G_W[a]^T S^-1 G_V[b], T2 = P2_W Tc P2_V^T
+    // t~ dX: F[sigma'] -= sum_ab T2[a,b] G_W[a]^T S^-1 G_V[b] with
+    // T2 = P2_W Tc[sigma'] P2_V^T and G_X[a] = [sq(J3_0^X[:,a]); J3ri_0^X[:,a]]
+    // (R' x N).  L[a] = S^-1 G_W[a] does not depend on sigma', so it is formed
+    // once per aux chunk and contracted with H[a] = sum_b T2[a,b] G_V[b] of
+    // every spin.
     clock.mark("tdx_fock");
+    std::vector<int> tdx_spins;
+    std::vector<DevBuf> T2s;
     for (int sp = 0; sp < ns; ++sp) {
       const double* Tq[2] = {ttl[0].get(), ns > 1 ? ttl[1].get() : nullptr};
       double cT[2] = {0, 0}, cX[2] = {0, 0};
@@ -552,39 +580,43 @@ void form_fock(const FockRequest& rq) {
                              0.0, T2.get(), LL(MW));
       gt2.b_ncontig = true;
       gemm(gt2);
-      const size_t per_a = 2 * Rp * N + N * N + np;
-      const size_t ac = std::max<size_t>(1, std::min(MW, budget / per_a));
-      DevBuf sbuf(np * ac), Hb(Rp * N * ac), Ub(Rp * N * ac), Gb(N * N * ac);
+      tdx_spins.push_back(sp);
+      T2s.push_back(std::move(T2));
+    }
+    if (!tdx_spins.empty()) {
+      const size_t per_a = 3 * Rp * N + np;
+      const size_t ac = tile_chunk(MW, 1, std::max<size_t>(1, std::min(MW, budget / per_a)));
+      DevBuf sbuf(np * ac), Gst(Rp * N * ac), Lb(Rp * N * ac), Hb(Rp * N * ac);
       for (size_t a0 = 0; a0 < MW; a0 += ac) {
         const size_t na = std::min(ac, MW - a0);
-        GemmDesc gs = gemm_nn(LL(np), LL(na), LL(MV), 1.0, V.J3_0.get(), LL(np), T2.get() + a0,
-                              LL(MW), 0.0, sbuf.get(), LL(np));
-        gs.b_ncontig = true;
-        gemm(gs);
-        unpack_sym(sbuf.get(), LL(np), LL(N), LL(na), Hb.get(), LL(Rp), LL(Rp * N));
-        GemmDesc gp = gemm_nn(LL(R), LL(na), LL(MV), 1.0, V.J3_ri_0.get(), LL(R * N),
-                              T2.get() + a0, LL(MW), 0.0, Hb.get() + N, LL(Rp * N));
-        gp.b_ncontig = true;
-        gp.nbo1 = LL(N);
-        gp.sAo1 = LL(R);
-        gp.sCo1 = LL(Rp);
-        gemm(gp);
-        gemm(gemm_nn(LL(Rp), LL(N * na), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp), Hb.get(), LL(Rp), 0.0,
-                     Ub.get(), LL(Rp)));
-        unpack_sym(W.J3_0.get() + np * a0, LL(np), LL(N), LL(na), Gb.get(), LL(N), LL(N * N));
-        GemmDesc ga = gemm_nn(LL(N), LL(N), LL(N), -1.0, Gb.get(), LL(N), Ub.get(), LL(Rp), 1.0,
-                              Fp[sp].get(), LL(N));
-        ga.nbr1 = LL(na);
-        ga.sAr1 = LL(N * N);
-        ga.sBr1 = LL(Rp * N);
-        gemm(ga);
-        GemmDesc gr = gemm_nn(LL(N), LL(N), LL(R), -1.0, W.J3_ri_0.get() + R * N * a0, LL(R),
-                              Ub.get() + N, LL(Rp), 1.0, Fp[sp].get(), LL(N));
-        gr.a_kcontig = true;
-        gr.nbr1 = LL(na);
-        gr.sAr1 = LL(R * N);
-        gr.sBr1 = LL(Rp * N);
-        gemm(gr);
+        // G_W chunk, AO rows then RI rows of each (R' x N) block
+        unpack_sym(W.J3_0.get() + np * a0, LL(np), LL(N), LL(na), Gst.get(), LL(Rp), LL(Rp * N));
+        copy3d(W.J3_ri_0.get() + R * N * a0, LL(R), LL(R * N), Gst.get() + N, LL(Rp), LL(Rp * N),
+               LL(R), LL(N), LL(na));
+        gemm(gemm_nn(LL(Rp), LL(N * na), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp), Gst.get(), LL(Rp),
+                     0.0, Lb.get(), LL(Rp)));
+        for (size_t q = 0; q < tdx_spins.size(); ++q) {
+          const double* T2 = T2s[q].get();
+          GemmDesc gs = gemm_nn(LL(np), LL(na), LL(MV), 1.0, V.J3_0.get(), LL(np), T2 + a0,
+                                LL(MW), 0.0, sbuf.get(), LL(np));
+          gs.b_ncontig = true;
+          gemm(gs);
+          unpack_sym(sbuf.get(), LL(np), LL(N), LL(na), Hb.get(), LL(Rp), LL(Rp * N));
+          GemmDesc gp = gemm_nn(LL(R), LL(na), LL(MV), 1.0, V.J3_ri_0.get(), LL(R * N), T2 + a0,
+                                LL(MW), 0.0, Hb.get() + N, LL(Rp * N));
+          gp.b_ncontig = true;
+          gp.nbo1 = LL(N);
+          gp.sAo1 = LL(R);
+          gp.sCo1 = LL(Rp);
+          gemm(gp);
+          GemmDesc gf = gemm_nn(LL(N), LL(N), LL(Rp), -1.0, Lb.get(), LL(Rp), Hb.get(), LL(Rp),
+                                1.0, Fp[tdx_spins[q]].get(), LL(N));
+          gf.a_kcontig = true;
+          gf.nbr1 = LL(na);
+          gf.sAr1 = LL(Rp * N);
+          gf.sBr1 = LL(Rp * N);
+          gemm(gf);
+        }
       }
     }
   }
@@ -618,7 +650,7 @@ void form_fock(const FockRequest& rq) {
       // ---- 3-el indirect energy (indirect_utils.cpp:101-133), chunked over k
       {
         const size_t per_k = 2 * Rp * a * a;
-        const size_t kc = std::max<size_t>(1, std::min(o, budget / per_k));
+        const size_t kc = tile_chunk(o, a, std::max<size_t>(1, std::min(o, budget / per_k)));
         DevBuf YW(Rp * a * a * kc), ZV(Rp * a * a * kc);
         for (size_t k0 = 0; k0 < o; k0 += kc) {
           const size_t nk = std::min(kc, o - k0);
@@ -686,7 +718,7 @@ void form_fock(const FockRequest& rq) {
         g.b_ncontig = true;
         gemm(g);
         const size_t per_k = 3 * Rp * a * N + a * (N * N + R * N + np);
-        const size_t kc = std::max<size_t>(1, std::min(o, budget / per_k));
+        const size_t kc = tile_chunk(o, a, std::max<size_t>(1, std::min(o, budget / per_k)));
         DevBuf ZYV(Rp * a * N * kc), ZYW(Rp * a * N * kc), gpk(np * a * kc), Gao(N * N * a * kc),
             gri(R * N * a * kc), Wk(Rp * N * a * kc);
         for (size_t k0 = 0; k0 < o; k0 += kc) {

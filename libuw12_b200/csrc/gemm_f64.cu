@@ -1,7 +1,11 @@
-// FP64 DMMA GEMM for sm_100a: 128x128x16 CTA tiles, 8 warps of 64x32,
-// 4-stage cp.async pipeline, m16n8k4 f64 tensor-core MMAs.
+// FP64 DMMA GEMM for sm_100a: 128x128x32 CTA tiles, 8 warps of 64x32,
+// 3-stage cp.async pipeline (16-byte copies when the operand allows it),
+// grouped CTA raster for L2 reuse, m16n8k4 f64 tensor-core MMAs.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 
@@ -13,14 +17,15 @@ namespace {
 
 constexpr int BM = 128;
 constexpr int BN = 128;
-constexpr int BK = 16;
-constexpr int STAGES = 4;
+constexpr int BK = 32;
+constexpr int STAGES = 3;
 constexpr int THREADS = 256;
-constexpr int LDW = 132;  // row length of [k][m] / [k][n] tiles (doubles); 132 % 16 == 4
-constexpr int LDK = 20;   // row length of [m][k] / [n][k] tiles (doubles); 20 % 16 == 4
-constexpr int A_STAGE = (BM * LDK > BK * LDW) ? BM * LDK : BK * LDW;  // 2560
-constexpr int B_STAGE = A_STAGE;
-constexpr size_t SMEM_BYTES = size_t(STAGES) * (A_STAGE + B_STAGE) * sizeof(double);
+constexpr int LDW = BM + 4;  // [k][m] / [k][n] tile rows (doubles); 132 % 16 == 4
+constexpr int LDK = BK + 4;  // [m][k] / [n][k] tile rows (doubles); 36 % 16 == 4, even
+constexpr int STAGE_ELEMS = (BM * LDK > BK * LDW) ? BM * LDK : BK * LDW;  // 4608
+constexpr size_t SMEM_BYTES = size_t(STAGES) * 2 * STAGE_ELEMS * sizeof(double);  // 216 KiB
+constexpr int GROUP_N = 8;   // CTAs that run together share A panels across 8 n-tiles
+constexpr long long kSMs = 148;
 
 struct KParams {
   const double* A;
@@ -34,7 +39,7 @@ struct KParams {
   long long sAo1, sAo2, sBo1, sBo2, sCo1, sCo2;
   long long nbr1;
   long long sAr1, sAr2, sBr1, sBr2;
-  long long tiles_m, tiles_mn;
+  long long tiles_m, tiles_n, tiles_mn;
   long long ktiles_pb, ktiles_total;
   int split;
 };
@@ -43,10 +48,16 @@ __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
 
-__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
-  const int bytes = valid ? 8 : 0;
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
-               "r"(bytes));
+// 8- or 16-byte asynchronous global -> shared copy; bytes beyond src_bytes
+// are zero-filled (src_bytes = 0 reads nothing).
+template <int BYTES>
+__device__ __forceinline__ void cp_async(double* dst, const double* src, int src_bytes) {
+  if (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)),
+                 "l"(src), "r"(src_bytes));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_u32(dst)),
+                 "l"(src), "r"(src_bytes));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
@@ -62,11 +73,61 @@ __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, doubl
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
-template <bool AK, bool BNC>
+// Loader of one operand tile (BK deep, 128 wide) into shared memory.
+//   KC  : the operand is contiguous along k in global memory ([w][k] tile,
+//         row LDK) -- otherwise along the 128-wide dimension ([k][w], row LDW);
+//   VEC : copies of two consecutive doubles (16 bytes) along the contiguous
+//         dimension; requires even leading dimension / offsets.
+// Thread mapping: the contiguous index is the fastest-varying across threads.
+template <bool KC, bool VEC>
+struct TileLoader {
+  static constexpr int W = VEC ? 2 : 1;                       // doubles per copy
+  static constexpr int CONTIG = KC ? BK : 128;                // contiguous extent
+  static constexpr int TPC = CONTIG / W;                      // threads along it
+  static constexpr int OTHER_STEP = THREADS / TPC;            // other-dim stride
+  static constexpr int OTHER = KC ? 128 : BK;                 // other extent
+  static constexpr int COPIES = OTHER / OTHER_STEP;           // copies per thread
+
+  int c0;   // contiguous index of this thread's first element
+  int o0;   // other index of this thread's first copy
+
+  __device__ __forceinline__ explicit TileLoader(int tid)
+      : c0((tid % TPC) * W), o0(tid / TPC) {}
+
+  // Element (w, kk) of the 128-wide x BK tile lives at global offset
+  // w + ld*kk (not KC) or kk + ld*w (KC).
+  __device__ __forceinline__ long long base(long long w0, long long ld) const {
+    return KC ? (c0 + ld * (w0 + o0)) : (w0 + c0 + ld * o0);
+  }
+  __device__ __forceinline__ long long step(long long ld) const { return OTHER_STEP * ld; }
+  __device__ __forceinline__ long long kstep(long long ld) const { return KC ? BK : BK * ld; }
+
+  // Copies this thread's share of a tile.  wlim = extent left along the
+  // 128-wide dimension from the tile start, klim = extent left along k.
+  __device__ __forceinline__ void load(double* s, const double* g, const double* dummy,
+                                       long long wlim, long long klim, long long ld) const {
+#pragma unroll
+    for (int r = 0; r < COPIES; ++r) {
+      const int o = o0 + r * OTHER_STEP;
+      const long long lim_c = KC ? klim : wlim;  // limit along the contiguous dim
+      const long long lim_o = KC ? wlim : klim;  // limit along the other dim
+      int bytes = 0;
+      if (o < lim_o) {
+        const long long left = lim_c - c0;
+        bytes = left >= W ? 8 * W : (left > 0 ? 8 * static_cast<int>(left) : 0);
+      }
+      double* dst = KC ? s + o * LDK + c0 : s + o * LDW + c0;
+      const double* src = bytes ? g + r * OTHER_STEP * ld : dummy;
+      cp_async<8 * W>(dst, src, bytes);
+    }
+  }
+};
+
+template <bool AK, bool BNC, bool VA, bool VB>
 __global__ void __launch_bounds__(THREADS, 1) dgemm_dmma(const KParams p) {
   extern __shared__ __align__(16) double smem[];
   double* As = smem;
-  double* Bs = smem + STAGES * A_STAGE;
+  double* Bs = smem + STAGES * STAGE_ELEMS;
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -76,13 +137,21 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_dmma(const KParams p) {
   const int wm = (warp & 1) * 64;
   const int wn = (warp >> 1) * 32;
 
+  // Block -> (tile, output batch, split).  Tiles are visited in groups of
+  // GROUP_N n-tiles, m-tile outermost inside a group, so the ~148 CTAs that
+  // run at once touch a few A panels and GROUP_N B panels.
   long long bid = blockIdx.x;
   const long long tile = bid % p.tiles_mn;
   bid /= p.tiles_mn;
   const long long bo = bid % p.nbo;
   const int sp = static_cast<int>(bid / p.nbo);
-  const long long tm = tile % p.tiles_m;
-  const long long tn = tile / p.tiles_m;
+  const long long per_group = p.tiles_m * GROUP_N;
+  const long long grp = tile / per_group;
+  const long long gn0 = grp * GROUP_N;
+  const long long gsize = (p.tiles_n - gn0) < GROUP_N ? (p.tiles_n - gn0) : GROUP_N;
+  const long long local = tile - grp * per_group;
+  const long long tn = gn0 + local % gsize;
+  const long long tm = local / gsize;
   const long long m0 = tm * BM;
   const long long n0 = tn * BN;
   const long long bo1 = bo % p.nbo1;
@@ -93,74 +162,42 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_dmma(const KParams p) {
   const long long kt_begin = p.ktiles_total * sp / p.split;
   const long long kt_end = p.ktiles_total * (sp + 1) / p.split;
 
-  // Per-thread fixed coordinates of the tile loads (8 elements per operand).
-  // A: [k][m] tile (m-contiguous global) or [m][k] tile (k-contiguous global).
-  const int a_i0 = AK ? (tid >> 4) : (tid & 127);
-  const int a_k0 = AK ? (tid & 15) : (tid >> 7);
-  const int b_j0 = BNC ? (tid & 127) : (tid >> 4);
-  const int b_k0 = BNC ? (tid >> 7) : (tid & 15);
-  // Offsets of element r = 0 within a (batch, k-tile) block, and the step per r.
-  const long long a_base = AK ? (a_k0 + p.lda * (m0 + a_i0)) : (m0 + a_i0 + p.lda * a_k0);
-  const long long a_step = AK ? 16 * p.lda : 2 * p.lda;
-  const long long a_kstep = AK ? BK : BK * p.lda;  // advance of one k-tile
-  const long long b_base = BNC ? (n0 + b_j0 + p.ldb * b_k0) : (b_k0 + p.ldb * (n0 + b_j0));
-  const long long b_step = BNC ? 2 * p.ldb : 16 * p.ldb;
-  const long long b_kstep = BNC ? BK * p.ldb : BK;
-  // Rows / columns this thread loads that lie inside the matrix (bit r).
-  unsigned a_rows_ok = 0, b_cols_ok = 0;
-#pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    const long long gi = m0 + (AK ? a_i0 + 16 * r : a_i0);
-    const long long gj = n0 + (BNC ? b_j0 : b_j0 + 16 * r);
-    a_rows_ok |= (gi < p.m ? 1u : 0u) << r;
-    b_cols_ok |= (gj < p.n ? 1u : 0u) << r;
-  }
+  const TileLoader<AK, VA> la(tid);
+  const TileLoader<!BNC, VB> lb(tid);
+  const long long a_base = la.base(m0, p.lda);
+  const long long b_base = lb.base(n0, p.ldb);
+  const long long a_kstep = la.kstep(p.lda);
+  const long long b_kstep = lb.kstep(p.ldb);
+  const long long a_wlim = p.m - m0;
+  const long long b_wlim = p.n - n0;
 
-  // Incremental (reduction batch, k offset) iterator of the next stage to load:
-  // no integer division inside the main loop.
+  // Incremental (reduction batch, k offset) iterator of the next stage to
+  // load: no integer division inside the main loop.
   long long it_kin, it_br1;
   const double* itA;
   const double* itB;
   {
     const long long br = kt_begin / p.ktiles_pb;
-    it_kin = (kt_begin - br * p.ktiles_pb) * BK;
+    const long long kt_in = kt_begin - br * p.ktiles_pb;
+    it_kin = kt_in * BK;
     it_br1 = br % p.nbr1;
     const long long br2 = br / p.nbr1;
-    itA = Ab + it_br1 * p.sAr1 + br2 * p.sAr2 + (it_kin / BK) * a_kstep;
-    itB = Bb + it_br1 * p.sBr1 + br2 * p.sBr2 + (it_kin / BK) * b_kstep;
+    itA = Ab + it_br1 * p.sAr1 + br2 * p.sAr2 + kt_in * a_kstep;
+    itB = Bb + it_br1 * p.sBr1 + br2 * p.sBr2 + kt_in * b_kstep;
   }
   const long long k_pad = p.ktiles_pb * BK;
 
   auto load_stage = [&](int slot) {
-    double* as = As + slot * A_STAGE;
-    double* bs = Bs + slot * B_STAGE;
-    const double* pa = itA + a_base;
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int i = AK ? a_i0 + 16 * r : a_i0;
-      const int kk = AK ? a_k0 : a_k0 + 2 * r;
-      const bool v = ((a_rows_ok >> r) & 1u) && (it_kin + kk < p.k);
-      double* dst = AK ? as + i * LDK + kk : as + kk * LDW + i;
-      cp_async8(dst, v ? pa + r * a_step : p.A, v);
-    }
-    const double* pb = itB + b_base;
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int j = BNC ? b_j0 : b_j0 + 16 * r;
-      const int kk = BNC ? b_k0 + 2 * r : b_k0;
-      const bool v = ((b_cols_ok >> r) & 1u) && (it_kin + kk < p.k);
-      double* dst = BNC ? bs + kk * LDW + j : bs + j * LDK + kk;
-      cp_async8(dst, v ? pb + r * b_step : p.B, v);
-    }
-    // advance to the next k-tile / reduction batch
+    const long long klim = p.k - it_kin;
+    la.load(As + slot * STAGE_ELEMS, itA + a_base, p.A, a_wlim, klim, p.lda);
+    lb.load(Bs + slot * STAGE_ELEMS, itB + b_base, p.B, b_wlim, klim, p.ldb);
     it_kin += BK;
     itA += a_kstep;
     itB += b_kstep;
     if (it_kin >= k_pad) {
-      const long long back = p.ktiles_pb;
       it_kin = 0;
-      itA += p.sAr1 - back * a_kstep;
-      itB += p.sBr1 - back * b_kstep;
+      itA += p.sAr1 - p.ktiles_pb * a_kstep;
+      itB += p.sBr1 - p.ktiles_pb * b_kstep;
       if (++it_br1 == p.nbr1) {
         it_br1 = 0;
         itA += p.sAr2 - p.nbr1 * p.sAr1;
@@ -183,17 +220,17 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_dmma(const KParams p) {
     cp_async_commit();
   }
 
+  int slot = 0;
+  int load_slot = STAGES - 1;
   for (long long kt = kt_begin; kt < kt_end; ++kt) {
     cp_async_wait<STAGES - 2>();
     __syncthreads();
-    {
-      const long long nxt = kt + STAGES - 1;
-      if (nxt < kt_end) load_stage(static_cast<int>((nxt - kt_begin) % STAGES));
-      cp_async_commit();
-    }
-    const int slot = static_cast<int>((kt - kt_begin) % STAGES);
-    const double* as = As + slot * A_STAGE;
-    const double* bs = Bs + slot * B_STAGE;
+    if (kt + STAGES - 1 < kt_end) load_stage(load_slot);
+    cp_async_commit();
+    load_slot = (load_slot + 1 == STAGES) ? 0 : load_slot + 1;
+
+    const double* as = As + slot * STAGE_ELEMS;
+    const double* bs = Bs + slot * STAGE_ELEMS;
 #pragma unroll
     for (int kq = 0; kq < BK / 4; ++kq) {
       const int kk = kq * 4 + t;
@@ -214,47 +251,35 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_dmma(const KParams p) {
 #pragma unroll
         for (int ni = 0; ni < 4; ++ni) dmma(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
     }
+    slot = (slot + 1 == STAGES) ? 0 : slot + 1;
   }
   cp_async_wait<0>();
 
-  // Epilogue.
-  if (p.split == 1) {
-    double* Cb = p.C + bo1 * p.sCo1 + bo2 * p.sCo2;
+  // Epilogue: C = alpha acc + beta C, or the raw partial tile for split-K.
+  double* Cb = p.split == 1 ? p.C + bo1 * p.sCo1 + bo2 * p.sCo2
+                            : p.work + (static_cast<long long>(sp) * p.nbo + bo) * (p.m * p.n);
+  const long long ldc = p.split == 1 ? p.ldc : p.m;
 #pragma unroll
-    for (int mi = 0; mi < 4; ++mi)
+  for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni)
+    for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const long long r = m0 + wm + mi * 16 + g + 8 * h;
-          if (r >= p.m) continue;
+      for (int h = 0; h < 2; ++h) {
+        const long long r = m0 + wm + mi * 16 + g + 8 * h;
+        if (r >= p.m) continue;
 #pragma unroll
-          for (int q = 0; q < 2; ++q) {
-            const long long c = n0 + wn + ni * 8 + 2 * t + q;
-            if (c >= p.n) continue;
-            double* dst = Cb + r + p.ldc * c;
+        for (int q = 0; q < 2; ++q) {
+          const long long c = n0 + wn + ni * 8 + 2 * t + q;
+          if (c >= p.n) continue;
+          double* dst = Cb + r + ldc * c;
+          if (p.split == 1) {
             const double v = p.alpha * acc[mi][ni][2 * h + q];
             *dst = (p.beta == 0.0) ? v : v + p.beta * (*dst);
+          } else {
+            *dst = acc[mi][ni][2 * h + q];
           }
         }
-  } else {
-    double* Wb = p.work + (static_cast<long long>(sp) * p.nbo + bo) * (p.m * p.n);
-#pragma unroll
-    for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-      for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const long long r = m0 + wm + mi * 16 + g + 8 * h;
-          if (r >= p.m) continue;
-#pragma unroll
-          for (int q = 0; q < 2; ++q) {
-            const long long c = n0 + wn + ni * 8 + 2 * t + q;
-            if (c >= p.n) continue;
-            Wb[r + p.m * c] = acc[mi][ni][2 * h + q];
-          }
-        }
-  }
+      }
 }
 
 // C = alpha * sum_s work[s] + beta * C (fixed summation order).
@@ -292,10 +317,9 @@ __global__ void scale_only(long long m, long long n, long long nbo, long long nb
 
 // Split-K factor: the CTAs of one launch run in waves of 148 (one per SM), so
 // a launch with few output tiles, or with a last wave that is mostly empty,
-// splits the contraction to fill the waves.  A split must keep >= 512 of k
-// per CTA so the partial-tile round trip stays small against the MMA work.
+// splits the contraction to fill the waves.  A split keeps >= 512 of k per
+// CTA so the partial-tile round trip stays small against the MMA work.
 int choose_split(long long ctas, long long ktiles_total) {
-  constexpr long long kSMs = 148;
   auto eff = [&](long long c) {
     const long long waves = (c + kSMs - 1) / kSMs;
     return double(c) / double(waves * kSMs);
@@ -304,7 +328,7 @@ int choose_split(long long ctas, long long ktiles_total) {
   int best = 1;
   double best_eff = eff(ctas);
   for (int s = 2; s <= 64; ++s) {
-    if (ktiles_total / s < 32) break;
+    if (ktiles_total / s < 512 / BK) break;
     const double e = eff(ctas * s);
     if (e > best_eff + 0.05) {
       best = s;
@@ -314,29 +338,108 @@ int choose_split(long long ctas, long long ktiles_total) {
   return best;
 }
 
-template <bool AK, bool BNC>
-void launch_variant(const KParams& p, long long grid, cudaStream_t s) {
+// A 16-byte copy needs the operand base, leading dimension and every batch
+// stride to be even (in doubles); tile origins are multiples of 32.
+bool vec_ok(const double* base, long long ld, long long s1, long long s2, long long s3,
+            long long s4) {
+  return (reinterpret_cast<std::uintptr_t>(base) % 16 == 0) && (ld % 2 == 0) && (s1 % 2 == 0) &&
+         (s2 % 2 == 0) && (s3 % 2 == 0) && (s4 % 2 == 0);
+}
+
+template <bool AK, bool BNC, bool VA, bool VB>
+void launch_kernel(const KParams& p, long long grid, cudaStream_t s) {
   static bool attr_set[64] = {};
+  static std::mutex mu;
   int dev = 0;
   UW12_CUDA(cudaGetDevice(&dev));
-  static std::mutex mu;
   {
     std::lock_guard<std::mutex> lk(mu);
     if (dev < 64 && !attr_set[dev]) {
-      UW12_CUDA(cudaFuncSetAttribute(dgemm_dmma<AK, BNC>,
+      UW12_CUDA(cudaFuncSetAttribute(dgemm_dmma<AK, BNC, VA, VB>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(SMEM_BYTES)));
       attr_set[dev] = true;
     }
   }
-  dgemm_dmma<AK, BNC><<<static_cast<unsigned>(grid), THREADS, SMEM_BYTES, s>>>(p);
+  dgemm_dmma<AK, BNC, VA, VB><<<static_cast<unsigned>(grid), THREADS, SMEM_BYTES, s>>>(p);
   UW12_LAUNCHED();
+}
+
+template <bool AK, bool BNC>
+void launch_layout(const KParams& p, bool va, bool vb, long long grid, cudaStream_t s) {
+  if (va && vb) launch_kernel<AK, BNC, true, true>(p, grid, s);
+  else if (va) launch_kernel<AK, BNC, true, false>(p, grid, s);
+  else if (vb) launch_kernel<AK, BNC, false, true>(p, grid, s);
+  else launch_kernel<AK, BNC, false, false>(p, grid, s);
+}
+
+// Fills the kernel parameters and chooses the split-K factor.  Returns false
+// for an empty output; *empty_k is set when the contraction is empty
+// (C = beta C).
+bool prepare(const GemmDesc& d, KParams& p, bool* empty_k) {
+  const long long nbo = d.nbo1 * d.nbo2;
+  const long long nbr = d.nbr1 * d.nbr2;
+  *empty_k = false;
+  if (d.m <= 0 || d.n <= 0 || nbo <= 0) return false;
+  if (d.k <= 0 || nbr <= 0) {
+    *empty_k = true;
+    return true;
+  }
+  if (!d.A || !d.B || !d.C) throw Error(kErrInvalid, "gemm: null operand");
+  p = KParams{};
+  p.A = d.A; p.B = d.B; p.C = d.C;
+  p.lda = d.lda; p.ldb = d.ldb; p.ldc = d.ldc;
+  p.m = d.m; p.n = d.n; p.k = d.k;
+  p.alpha = d.alpha; p.beta = d.beta;
+  p.nbo1 = d.nbo1; p.nbo = nbo;
+  p.sAo1 = d.sAo1; p.sAo2 = d.sAo2; p.sBo1 = d.sBo1; p.sBo2 = d.sBo2;
+  p.sCo1 = d.sCo1; p.sCo2 = d.sCo2;
+  p.nbr1 = d.nbr1;
+  p.sAr1 = d.sAr1; p.sAr2 = d.sAr2; p.sBr1 = d.sBr1; p.sBr2 = d.sBr2;
+  p.tiles_m = (d.m + BM - 1) / BM;
+  p.tiles_n = (d.n + BN - 1) / BN;
+  p.tiles_mn = p.tiles_m * p.tiles_n;
+  p.ktiles_pb = (d.k + BK - 1) / BK;
+  p.ktiles_total = p.ktiles_pb * nbr;
+  int split = d.split;
+  if (split <= 0) split = choose_split(p.tiles_mn * nbo, p.ktiles_total);
+  p.split = static_cast<int>(std::max<long long>(1, std::min<long long>(split, p.ktiles_total)));
+  return true;
+}
+
+void launch_scale_only(const GemmDesc& d, cudaStream_t s) {
+  if (d.beta == 1.0) return;
+  const long long nbo = d.nbo1 * d.nbo2;
+  const long long total = d.m * d.n * nbo;
+  const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, kSMs * 16));
+  scale_only<<<blocks, 256, 0, s>>>(d.m, d.n, nbo, d.nbo1, d.beta, d.C, d.ldc, d.sCo1, d.sCo2);
+  UW12_LAUNCHED();
+}
+
+// Launches the GEMM (and the split-K reduction when p.split > 1, with
+// partial tiles in p.work).
+void launch(const GemmDesc& d, const KParams& p, cudaStream_t s) {
+  const long long grid = p.tiles_mn * p.nbo * p.split;
+  const bool va = vec_ok(d.A, d.lda, d.sAo1, d.sAo2, d.sAr1, d.sAr2);
+  const bool vb = vec_ok(d.B, d.ldb, d.sBo1, d.sBo2, d.sBr1, d.sBr2);
+  if (!d.a_kcontig && !d.b_ncontig) launch_layout<false, false>(p, va, vb, grid, s);
+  else if (!d.a_kcontig && d.b_ncontig) launch_layout<false, true>(p, va, vb, grid, s);
+  else if (d.a_kcontig && !d.b_ncontig) launch_layout<true, false>(p, va, vb, grid, s);
+  else launch_layout<true, true>(p, va, vb, grid, s);
+  if (p.split > 1) {
+    const long long total = d.m * d.n * p.nbo;
+    const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, kSMs * 16));
+    splitk_reduce<<<blocks, 256, 0, s>>>(p.work, p.split, d.m, d.n, p.nbo, d.nbo1, d.alpha,
+                                         d.beta, d.C, d.ldc, d.sCo1, d.sCo2);
+    UW12_LAUNCHED();
+  }
 }
 
 // ---- profiling -------------------------------------------------------------
 struct ProfRec {
   cudaEvent_t a, b;
   double flops;
+  std::string shape;  // "m n k nbo nbr split layout vec" for the per-launch log
 };
 std::mutex g_prof_mu;
 bool g_prof_on = false;
@@ -351,6 +454,12 @@ void prof_collect_locked() {
     g_prof_acc.launches += 1;
     g_prof_acc.ms += ms;
     g_prof_acc.flops += r.flops;
+    if (const char* path = std::getenv("UW12_PROFILE_LOG")) {
+      if (FILE* f = std::fopen(path, "a")) {
+        std::fprintf(f, "%.4f %s\n", ms, r.shape.c_str());
+        std::fclose(f);
+      }
+    }
     cudaEventDestroy(r.a);
     cudaEventDestroy(r.b);
   }
@@ -382,155 +491,43 @@ KernelStats profile_read_gemm() {
 }
 
 void gemm(const GemmDesc& d) {
-  const long long nbo = d.nbo1 * d.nbo2;
-  const long long nbr = d.nbr1 * d.nbr2;
-  if (d.m <= 0 || d.n <= 0 || nbo <= 0) return;
+  KParams p;
+  bool empty_k = false;
+  if (!prepare(d, p, &empty_k)) return;
   cudaStream_t s = current_stream();
-  if (d.k <= 0 || nbr <= 0) {
-    if (d.beta == 1.0) return;
-    const long long total = d.m * d.n * nbo;
-    const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 16));
-    scale_only<<<blocks, 256, 0, s>>>(d.m, d.n, nbo, d.nbo1, d.beta, d.C, d.ldc, d.sCo1, d.sCo2);
-    UW12_LAUNCHED();
+  if (empty_k) {
+    launch_scale_only(d, s);
     return;
   }
-  if (!d.A || !d.B || !d.C) throw Error(kErrInvalid, "gemm: null operand");
-
-  KParams p{};
-  p.A = d.A; p.B = d.B; p.C = d.C;
-  p.lda = d.lda; p.ldb = d.ldb; p.ldc = d.ldc;
-  p.m = d.m; p.n = d.n; p.k = d.k;
-  p.alpha = d.alpha; p.beta = d.beta;
-  p.nbo1 = d.nbo1; p.nbo = nbo;
-  p.sAo1 = d.sAo1; p.sAo2 = d.sAo2; p.sBo1 = d.sBo1; p.sBo2 = d.sBo2;
-  p.sCo1 = d.sCo1; p.sCo2 = d.sCo2;
-  p.nbr1 = d.nbr1;
-  p.sAr1 = d.sAr1; p.sAr2 = d.sAr2; p.sBr1 = d.sBr1; p.sBr2 = d.sBr2;
-  p.tiles_m = (d.m + BM - 1) / BM;
-  const long long tiles_n = (d.n + BN - 1) / BN;
-  p.tiles_mn = p.tiles_m * tiles_n;
-  p.ktiles_pb = (d.k + BK - 1) / BK;
-  p.ktiles_total = p.ktiles_pb * nbr;
-
-  const long long ctas = p.tiles_mn * nbo;
-  int split = d.split;
-  if (split <= 0) split = choose_split(ctas, p.ktiles_total);
-  split = static_cast<int>(std::max<long long>(1, std::min<long long>(split, p.ktiles_total)));
-  p.split = split;
-
   DevBuf work;
-  if (split > 1) {
-    work.alloc(static_cast<size_t>(split) * nbo * d.m * d.n, s);
+  if (p.split > 1) {
+    work.alloc(static_cast<size_t>(p.split) * p.nbo * d.m * d.n, s);
     p.work = work.get();
   }
-
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;
-  bool prof = false;
-  {
-    std::lock_guard<std::mutex> lk(g_prof_mu);
-    prof = g_prof_on;
-  }
+  const bool prof = profile_enabled();
   if (prof) {
     UW12_CUDA(cudaEventCreate(&ev_a));
     UW12_CUDA(cudaEventCreate(&ev_b));
     UW12_CUDA(cudaEventRecord(ev_a, s));
   }
-
-  const long long grid = ctas * split;
-  if (!d.a_kcontig && !d.b_ncontig) launch_variant<false, false>(p, grid, s);
-  else if (!d.a_kcontig && d.b_ncontig) launch_variant<false, true>(p, grid, s);
-  else if (d.a_kcontig && !d.b_ncontig) launch_variant<true, false>(p, grid, s);
-  else launch_variant<true, true>(p, grid, s);
-
-  if (split > 1) {
-    const long long total = d.m * d.n * nbo;
-    const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 16));
-    splitk_reduce<<<blocks, 256, 0, s>>>(p.work, split, d.m, d.n, nbo, d.nbo1, d.alpha, d.beta,
-                                         d.C, d.ldc, d.sCo1, d.sCo2);
-    UW12_LAUNCHED();
-  }
+  launch(d, p, s);
   if (prof) {
     UW12_CUDA(cudaEventRecord(ev_b, s));
     std::lock_guard<std::mutex> lk(g_prof_mu);
+    char shape[256];
+    std::snprintf(shape, sizeof(shape), "%lld %lld %lld %lld %lld %d %d%d %d%d", d.m, d.n, d.k,
+                  p.nbo, d.nbr1 * d.nbr2, p.split, int(d.a_kcontig), int(d.b_ncontig),
+                  int(vec_ok(d.A, d.lda, d.sAo1, d.sAo2, d.sAr1, d.sAr2)),
+                  int(vec_ok(d.B, d.ldb, d.sBo1, d.sBo2, d.sBr1, d.sBr2)));
     g_prof_recs.push_back({ev_a, ev_b, 2.0 * double(d.m) * double(d.n) * double(d.k) *
-                                           double(nbo) * double(nbr)});
+                                           double(p.nbo) * double(d.nbr1 * d.nbr2),
+                           shape});
   }
 }
 
 // ---- allocation-free variant -------------------------------------------------
-namespace {
-
-// Kernel parameters and split-K factor of an allocation-free call (the same
-// choice gemm() makes).  Returns false for an empty output; *empty_k is set
-// when the contraction is empty (C = beta C).
-bool prepare(const GemmDesc& d, KParams& p, bool* empty_k) {
-  const long long nbo = d.nbo1 * d.nbo2;
-  const long long nbr = d.nbr1 * d.nbr2;
-  *empty_k = false;
-  if (d.m <= 0 || d.n <= 0 || nbo <= 0) return false;
-  if (d.k <= 0 || nbr <= 0) {
-    *empty_k = true;
-    return true;
-  }
-  if (!d.A || !d.B || !d.C) throw Error(kErrInvalid, "gemm: null operand");
-  p = KParams{};
-  p.A = d.A; p.B = d.B; p.C = d.C;
-  p.lda = d.lda; p.ldb = d.ldb; p.ldc = d.ldc;
-  p.m = d.m; p.n = d.n; p.k = d.k;
-  p.alpha = d.alpha; p.beta = d.beta;
-  p.nbo1 = d.nbo1; p.nbo = nbo;
-  p.sAo1 = d.sAo1; p.sAo2 = d.sAo2; p.sBo1 = d.sBo1; p.sBo2 = d.sBo2;
-  p.sCo1 = d.sCo1; p.sCo2 = d.sCo2;
-  p.nbr1 = d.nbr1;
-  p.sAr1 = d.sAr1; p.sAr2 = d.sAr2; p.sBr1 = d.sBr1; p.sBr2 = d.sBr2;
-  p.tiles_m = (d.m + BM - 1) / BM;
-  const long long tiles_n = (d.n + BN - 1) / BN;
-  p.tiles_mn = p.tiles_m * tiles_n;
-  p.ktiles_pb = (d.k + BK - 1) / BK;
-  p.ktiles_total = p.ktiles_pb * nbr;
-  const long long ctas = p.tiles_mn * nbo;
-  int split = d.split;
-  if (split <= 0) {
-    constexpr long long kSMs = 148;
-    split = 1;
-    if (ctas < kSMs) {
-      long long want = (kSMs + ctas - 1) / ctas;
-      long long cap = std::max<long long>(1, p.ktiles_total / 8);  // >= 128 k per split
-      split = static_cast<int>(std::min<long long>(std::min(want, cap), 64));
-    }
-  }
-  p.split = static_cast<int>(std::max<long long>(1, std::min<long long>(split, p.ktiles_total)));
-  return true;
-}
-
-void launch_scale_only(const GemmDesc& d, cudaStream_t s) {
-  if (d.beta == 1.0) return;
-  const long long nbo = d.nbo1 * d.nbo2;
-  const long long total = d.m * d.n * nbo;
-  const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 16));
-  scale_only<<<blocks, 256, 0, s>>>(d.m, d.n, nbo, d.nbo1, d.beta, d.C, d.ldc, d.sCo1, d.sCo2);
-  UW12_LAUNCHED();
-}
-
-// Launches the GEMM (and the split-K reduction when p.split > 1, with
-// partial tiles in p.work).
-void launch(const GemmDesc& d, const KParams& p, cudaStream_t s) {
-  const long long grid = p.tiles_mn * p.nbo * p.split;
-  if (!d.a_kcontig && !d.b_ncontig) launch_variant<false, false>(p, grid, s);
-  else if (!d.a_kcontig && d.b_ncontig) launch_variant<false, true>(p, grid, s);
-  else if (d.a_kcontig && !d.b_ncontig) launch_variant<true, false>(p, grid, s);
-  else launch_variant<true, true>(p, grid, s);
-  if (p.split > 1) {
-    const long long total = d.m * d.n * p.nbo;
-    const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 16));
-    splitk_reduce<<<blocks, 256, 0, s>>>(p.work, p.split, d.m, d.n, p.nbo, d.nbo1, d.alpha,
-                                         d.beta, d.C, d.ldc, d.sCo1, d.sCo2);
-    UW12_LAUNCHED();
-  }
-}
-
-}  // namespace
-
+//
 // Split-K partial tiles normally live in a stream-ordered allocation.  For
 // callers that must not allocate, they go into this fixed device array
 // instead: every device that loads the library keeps it (16 MiB) until the

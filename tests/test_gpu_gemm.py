@@ -42,6 +42,32 @@ def test_single(uw12lib, cuda_device, a_k, b_n, m, n, k):
                           C.reshape((ldc, n), order="F")[m:, :])
 
 
+@pytest.mark.parametrize("a_k,b_n", [(False, False), (False, True), (True, False), (True, True)])
+@pytest.mark.parametrize("m,n,k", [(129, 131, 33), (255, 97, 1001), (64, 300, 65)])
+def test_sixteen_byte_copies(uw12lib, cuda_device, a_k, b_n, m, n, k):
+    """Even leading dimensions select the 16-byte copy path; odd extents make
+    the last copy of a row partial (8 bytes copied, 8 zero-filled)."""
+    import torch
+    rng = np.random.default_rng(m + 7 * n + 11 * k)
+    lda = (k if a_k else m) + 1
+    lda += lda % 2
+    ldb = (n if b_n else k) + 1
+    ldb += ldb % 2
+    A = rng.standard_normal(lda * (m if a_k else k))
+    B = rng.standard_normal(ldb * (k if b_n else n))
+    Am = A.reshape((lda, m if a_k else k), order="F")
+    Am = Am[:k, :m].T if a_k else Am[:m, :k]
+    Bm = B.reshape((ldb, k if b_n else n), order="F")
+    Bm = Bm[:n, :k].T if b_n else Bm[:k, :n]
+    dA, dB = _dev(torch, A), _dev(torch, B)
+    dC = torch.zeros(m * n, dtype=torch.float64, device=cuda_device)
+    uw12lib.dgemm(m, n, k, 1.0, dA.data_ptr(), lda, a_k, dB.data_ptr(), ldb, b_n, 0.0,
+                  dC.data_ptr(), m)
+    torch.cuda.synchronize()
+    out = dC.cpu().numpy().reshape((m, n), order="F")
+    assert np.all(np.abs(out - Am @ Bm) <= 1e-13 * (np.abs(Am) @ np.abs(Bm)) + 1e-300)
+
+
 @pytest.mark.parametrize("split", [0, 1, 3, 7])
 def test_batched_and_reduction(uw12lib, cuda_device, split):
     import torch
