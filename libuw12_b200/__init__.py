@@ -26,7 +26,7 @@ __all__ = [
 ]
 
 _HERE = Path(__file__).resolve().parent
-_LIB_PATH = _HERE / "_lib" / "libuw12_b200.so"
+_LIB_PATH = Path(os.environ.get("UW12_LIB_PATH", _HERE / "_lib" / "libuw12_b200.so"))
 _lib = None
 
 OK, ERR_RUNTIME, ERR_LOGIC, ERR_CUDA, ERR_ALLOC, ERR_INVALID = range(6)

@@ -73,6 +73,15 @@ __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, doubl
       : "d"(a0), "d"(a1), "d"(b0));
 }
 
+__device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+      "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+        "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
 // Loader of one operand tile (BK deep, 128 wide) into shared memory.
 //   KC  : the operand is contiguous along k in global memory ([w][k] tile,
 //         row LDK) -- otherwise along the 128-wide dimension ([k][w], row LDW);
@@ -231,6 +240,35 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_dmma(const KParams p) {
 
     const double* as = As + slot * STAGE_ELEMS;
     const double* bs = Bs + slot * STAGE_ELEMS;
+#if UW12_DMMA_K16
+    // m16n8k16: A fragment element q sits at row g + 8 (q & 1), k = t + 4 (q >> 1);
+    // B fragment element q at k = t + 4 q, column g.
+#pragma unroll
+    for (int kh = 0; kh < BK / 16; ++kh) {
+      double bf[4][4];
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+        const int col = wn + ni * 8 + g;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int kk = kh * 16 + t + 4 * q;
+          bf[ni][q] = BNC ? bs[kk * LDW + col] : bs[col * LDK + kk];
+        }
+      }
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi) {
+        double af[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int row = wm + mi * 16 + g + 8 * (q & 1);
+          const int kk = kh * 16 + t + 4 * (q >> 1);
+          af[q] = AK ? as[row * LDK + kk] : as[kk * LDW + row];
+        }
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) dmma16(acc[mi][ni], af, bf[ni]);
+      }
+    }
+#else
 #pragma unroll
     for (int kq = 0; kq < BK / 4; ++kq) {
       const int kk = kq * 4 + t;
@@ -251,6 +289,7 @@ __global__ void __launch_bounds__(THREADS, 1) dgemm_dmma(const KParams p) {
 #pragma unroll
         for (int ni = 0; ni < 4; ++ni) dmma(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
     }
+#endif
     slot = (slot + 1 == STAGES) ? 0 : slot + 1;
   }
   cp_async_wait<0>();
