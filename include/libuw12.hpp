@@ -1,0 +1,414 @@
+// libuw12.hpp -- C++ drop-in for libuw12's public API on the B200 library.
+//
+// Same namespace, types and function signatures as libuw12's libuw12.hpp
+// (setup_base_integrals, setup_abs_projectors, setup_orbitals,
+// setup_occupations, uw12_energy, uw12_fock) plus form_fock (src/uw12.hpp)
+// and the BaseIntegrals constructors of src/integrals/base_integrals.hpp,
+// implemented header-only over the C-ABI in uw12_c.h.  Armadillo's arma::mat
+// is replaced by uw12::linalg::Mat, a column-major matrix owning its storage.
+// Failures throw std::runtime_error / std::logic_error as libuw12 does.
+#ifndef UW12_B200_LIBUW12_HPP
+#define UW12_B200_LIBUW12_HPP
+
+#include <cfloat>
+#include <cmath>
+#include <cstddef>
+#include <functional>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "uw12_c.h"
+
+namespace uw12 {
+
+namespace linalg {
+
+/// Column-major dense matrix (the role of arma::mat in libuw12).
+class Mat {
+ public:
+  Mat() = default;
+  Mat(size_t rows, size_t cols) : r_(rows), c_(cols), d_(rows * cols, 0.0) {}
+  Mat(const double* data, size_t rows, size_t cols)
+      : r_(rows), c_(cols), d_(data, data + rows * cols) {}
+  size_t n_rows() const { return r_; }
+  size_t n_cols() const { return c_; }
+  size_t n_elem() const { return d_.size(); }
+  double& operator()(size_t i, size_t j) { return d_[i + r_ * j]; }
+  double operator()(size_t i, size_t j) const { return d_[i + r_ * j]; }
+  double& operator[](size_t i) { return d_[i]; }
+  double operator[](size_t i) const { return d_[i]; }
+  double* memptr() { return d_.data(); }
+  const double* memptr() const { return d_.data(); }
+
+ private:
+  size_t r_ = 0, c_ = 0;
+  std::vector<double> d_;
+};
+
+/// Column vector (the role of arma::vec).
+class Vec : public Mat {
+ public:
+  Vec() = default;
+  explicit Vec(size_t n) : Mat(n, 1) {}
+  Vec(size_t rows, size_t cols) : Mat(rows, cols) {}
+  Vec(const double* data, size_t n) : Mat(data, n, 1) {}
+  Vec(const double* data, size_t rows, size_t cols) : Mat(data, rows, cols) {}
+};
+
+inline size_t n_rows(const Mat& m) { return m.n_rows(); }
+inline size_t n_cols(const Mat& m) { return m.n_cols(); }
+inline size_t n_elem(const Mat& m) { return m.n_elem(); }
+
+}  // namespace linalg
+
+namespace detail {
+
+inline std::string last_error() {
+  char buf[1024];
+  uw12c_last_error(buf, sizeof(buf));
+  return std::string(buf);
+}
+
+inline void check(int status) {
+  if (status == UW12C_OK) return;
+  if (status == UW12C_ERR_LOGIC) throw std::logic_error(last_error());
+  throw std::runtime_error(last_error());
+}
+
+}  // namespace detail
+
+namespace integrals {
+
+/// Returns the two-index integrals (A|w|B), n_df x n_df (integral_functions.hpp:17).
+using TwoIndexFn = std::function<linalg::Mat()>;
+/// Returns the three-index integrals of one df shell A: n_ao(n_ao+1)/2 x n_A
+/// (AO) or n_ri*n_ao x n_A (RI) (integral_functions.hpp:20).
+using ThreeIndexFn = std::function<linalg::Mat(size_t)>;
+
+/// Device-resident density-fitting integrals (base_integrals.hpp:46-293).
+class BaseIntegrals {
+ public:
+  BaseIntegrals() = default;
+
+  /// Stored integrals with RI (base_integrals.hpp:94-96).
+  BaseIntegrals(const linalg::Mat& J3_0, const linalg::Mat& J2, const linalg::Mat& J3_ri_0) {
+    const size_t n_ao = n_ao_from_packed(J3_0.n_rows());
+    create(J3_0.memptr(), J2.memptr(), J3_ri_0.memptr(), n_ao, J2.n_rows(),
+           n_ao ? J3_ri_0.n_rows() / n_ao : 0, J3_0.n_cols(), J3_ri_0.n_cols());
+  }
+
+  /// Stored integrals without RI (base_integrals.hpp:99).
+  BaseIntegrals(const linalg::Mat& J3_0, const linalg::Mat& J2) {
+    create(J3_0.memptr(), J2.memptr(), nullptr, n_ao_from_packed(J3_0.n_rows()), J2.n_rows(), 0,
+           J3_0.n_cols(), 0);
+  }
+
+  /// Integrals already in the metric eigenbasis, J3 = J3_0 P2, with their
+  /// eigenvalues (base_integrals.hpp:104); cannot be used for RI.
+  BaseIntegrals(const linalg::Mat& J3, const linalg::Vec& df_vals) {
+    const size_t n_ao = n_ao_from_packed(J3.n_rows());
+    if (J3.n_cols() != df_vals.n_elem())
+      throw std::runtime_error("Number of density-fitting basis functions inconsistent");
+    uw12c_integrals* h = nullptr;
+    detail::check(uw12c_integrals_create_eigenbasis(J3.memptr(), df_vals.memptr(), n_ao,
+                                                    df_vals.n_elem(), UW12C_MEM_HOST, &h));
+    h_.reset(h, uw12c_integrals_destroy);
+  }
+
+  /// Integrals from callbacks, one df shell per three-index call
+  /// (base_integrals.hpp:52-62).  The shells are assembled on the host and
+  /// uploaded once.
+  BaseIntegrals(const TwoIndexFn& two_index_fn, const ThreeIndexFn& three_index_fn,
+                const ThreeIndexFn& three_index_ri_fn, const std::vector<size_t>& df_sizes,
+                size_t n_ao, size_t n_df, size_t n_ri, bool /*store_ao_integrals*/ = true,
+                bool /*store_ri_integrals*/ = true) {
+    check_shells(df_sizes, n_ao, n_df);
+    if (n_ri == 0)
+      throw std::runtime_error(
+          "Three index ri integrals requested but number of ri basis functions is zero");
+    const linalg::Mat J2 = two_index_fn();
+    const linalg::Mat J3 = assemble(three_index_fn, df_sizes, n_ao * (n_ao + 1) / 2, n_df);
+    const linalg::Mat J3r = assemble(three_index_ri_fn, df_sizes, n_ao * n_ri, n_df);
+    create(J3.memptr(), J2.memptr(), J3r.memptr(), n_ao, n_df, n_ri, n_df, n_df);
+  }
+
+  /// Callback integrals without RI (base_integrals.hpp:65-72).
+  BaseIntegrals(const TwoIndexFn& two_index_fn, const ThreeIndexFn& three_index_fn,
+                const std::vector<size_t>& df_sizes, size_t n_ao, size_t n_df,
+                bool /*store_ao_integrals*/ = true) {
+    check_shells(df_sizes, n_ao, n_df);
+    const linalg::Mat J2 = two_index_fn();
+    const linalg::Mat J3 = assemble(three_index_fn, df_sizes, n_ao * (n_ao + 1) / 2, n_df);
+    create(J3.memptr(), J2.memptr(), nullptr, n_ao, n_df, 0, n_df, 0);
+  }
+
+  /// Stored AO integrals with RI integrals from a callback (base_integrals.hpp:78-88).
+  BaseIntegrals(const linalg::Mat& J3_0, const linalg::Mat& J2,
+                const ThreeIndexFn& three_index_ri, const std::vector<size_t>& df_sizes,
+                bool use_ri, size_t n_ao, size_t n_df, size_t n_ri,
+                bool /*store_ri_integrals*/ = false) {
+    if (!use_ri) {
+      create(J3_0.memptr(), J2.memptr(), nullptr, n_ao_from_packed(J3_0.n_rows()), J2.n_rows(),
+             0, J3_0.n_cols(), 0);
+      return;
+    }
+    check_shells(df_sizes, n_ao, n_df);
+    const linalg::Mat J3r = assemble(three_index_ri, df_sizes, n_ao * n_ri, n_df);
+    create(J3_0.memptr(), J2.memptr(), J3r.memptr(), n_ao, n_df, n_ri, J3_0.n_cols(), n_df);
+  }
+
+  /// From raw pointers in host or device memory (uw12c_integrals_create).
+  static BaseIntegrals from_pointers(const double* X3, const double* X2, const double* X3_ri,
+                                     size_t n_ao, size_t n_df, size_t n_ri, int mem_kind) {
+    BaseIntegrals b;
+    uw12c_integrals* h = nullptr;
+    detail::check(uw12c_integrals_create(X3, X2, X3_ri, n_ao, n_df, n_ri, mem_kind, &h));
+    b.h_.reset(h, uw12c_integrals_destroy);
+    return b;
+  }
+
+  size_t get_number_ao() const { return dims(0); }
+  size_t get_number_df() const { return dims(1); }
+  size_t get_number_ri() const { return dims(2); }
+
+  linalg::Vec get_df_vals() const {
+    linalg::Vec v(get_number_df(), 1);
+    detail::check(uw12c_integrals_df_vals(handle(), v.memptr()));
+    return v;
+  }
+
+  const uw12c_integrals* handle() const {
+    if (!h_) throw std::runtime_error("BaseIntegrals not initialised");
+    return h_.get();
+  }
+
+ private:
+  static size_t n_ao_from_packed(size_t n) {
+    if (n == 0) throw std::runtime_error("Number of ao orbitals is zero");
+    const auto n_ao = static_cast<size_t>(std::sqrt(8.0 * double(n) - 1.0) / 2.0);
+    if (n_ao * (n_ao + 1) / 2 != n) throw std::logic_error("vector must be of length n(n+1)/2");
+    return n_ao;
+  }
+
+  static void check_shells(const std::vector<size_t>& df_sizes, size_t n_ao, size_t n_df) {
+    if (df_sizes.empty())
+      throw std::runtime_error("no df_sizes provided, cannot calculate three index integrals");
+    if (n_df == 0 || n_ao == 0)
+      throw std::runtime_error(
+          "Number of basis functions is zero, cannot calculate basis functions");
+    if (df_sizes.size() > n_df)
+      throw std::runtime_error("More shells than basis functions in df basis");
+    size_t total = 0;
+    for (size_t s : df_sizes) total += s;
+    if (total != n_df)
+      throw std::runtime_error("total df basis functions inconsistent with number in shells");
+  }
+
+  // coulomb_3idx (integral_functions.hpp:33-55): shell A fills columns
+  // offset(A) .. offset(A) + n_A.
+  static linalg::Mat assemble(const ThreeIndexFn& fn, const std::vector<size_t>& df_sizes,
+                              size_t rows, size_t n_df) {
+    linalg::Mat out(rows, n_df);
+    size_t off = 0;
+    for (size_t A = 0; A < df_sizes.size(); ++A) {
+      const linalg::Mat shell = fn(A);
+      if (shell.n_rows() != rows || shell.n_cols() != df_sizes[A])
+        throw std::logic_error("three-index shell of unexpected size");
+      for (size_t j = 0; j < shell.n_cols(); ++j)
+        for (size_t i = 0; i < rows; ++i) out(i, off + j) = shell(i, j);
+      off += df_sizes[A];
+    }
+    return out;
+  }
+
+  void create(const double* X3, const double* X2, const double* X3_ri, size_t n_ao, size_t n_df,
+              size_t n_ri, size_t cols3, size_t cols3_ri) {
+    if (cols3 != n_df || (X3_ri && cols3_ri != n_df))
+      throw std::runtime_error("Number of density-fitting basis functions inconsistent");
+    uw12c_integrals* h = nullptr;
+    detail::check(uw12c_integrals_create(X3, X2, X3_ri, n_ao, n_df, X3_ri ? n_ri : 0,
+                                         UW12C_MEM_HOST, &h));
+    h_.reset(h, uw12c_integrals_destroy);
+  }
+
+  size_t dims(int which) const {
+    size_t d[3] = {0, 0, 0};
+    detail::check(uw12c_integrals_dims(handle(), &d[0], &d[1], &d[2]));
+    return d[which];
+  }
+
+  std::shared_ptr<uw12c_integrals> h_;
+};
+
+}  // namespace integrals
+
+namespace three_el::ri {
+
+/// ABS+ projectors (ri_utils.hpp:20-29), device resident.
+class ABSProjectors {
+ public:
+  ABSProjectors() = default;
+  ABSProjectors(const double* S, size_t n_ao, size_t n_ri, int mem_kind = UW12C_MEM_HOST)
+      : n_ao_(n_ao), n_ri_(n_ri) {
+    uw12c_abs* h = nullptr;
+    detail::check(uw12c_abs_create(S, n_ao, n_ri, mem_kind, &h));
+    h_.reset(h, uw12c_abs_destroy);
+  }
+  /// The four blocks s_inv_ri_ri, s_inv_ri_ao, s_inv_ao_ri, s_inv_ao_ao.
+  std::vector<linalg::Mat> blocks() const {
+    std::vector<linalg::Mat> b{linalg::Mat(n_ri_, n_ri_), linalg::Mat(n_ri_, n_ao_),
+                               linalg::Mat(n_ao_, n_ri_), linalg::Mat(n_ao_, n_ao_)};
+    detail::check(uw12c_abs_blocks(handle(), b[0].memptr(), b[1].memptr(), b[2].memptr(),
+                                   b[3].memptr()));
+    return b;
+  }
+  const uw12c_abs* handle() const {
+    if (!h_) throw std::runtime_error("ABSProjectors not initialised");
+    return h_.get();
+  }
+
+ private:
+  size_t n_ao_ = 0, n_ri_ = 0;
+  std::shared_ptr<uw12c_abs> h_;
+};
+
+/// calculate_abs_projectors (ri_utils.hpp:45-74) for a combined AO+RI overlap.
+inline ABSProjectors calculate_abs_projectors(const linalg::Mat& S, size_t n_ao, size_t n_ri) {
+  if (S.n_rows() != n_ao + n_ri || S.n_cols() != n_ao + n_ri)
+    throw std::runtime_error("Total number of basis functions is inconsistent");
+  return ABSProjectors(S.memptr(), n_ao, n_ri);
+}
+
+}  // namespace three_el::ri
+
+namespace utils {
+using Orbitals = std::vector<linalg::Mat>;
+using Occupations = std::vector<linalg::Vec>;
+using FockMatrix = std::vector<linalg::Mat>;
+/// utils.hpp:142-146.
+struct FockMatrixAndEnergy {
+  FockMatrix fock;
+  double energy = 0.0;
+};
+}  // namespace utils
+
+using integrals::BaseIntegrals;
+using three_el::ri::ABSProjectors;
+using utils::Occupations;
+using utils::Orbitals;
+
+/// uw12::form_fock (src/uw12.hpp:129-142).
+inline utils::FockMatrixAndEnergy form_fock(const BaseIntegrals& W, const BaseIntegrals& V,
+                                            const BaseIntegrals& WV,
+                                            const ABSProjectors& abs_projectors,
+                                            const Orbitals& orbitals,
+                                            const Occupations& occupations,
+                                            const std::vector<size_t>& n_active,
+                                            bool indirect_term, bool calculate_fock,
+                                            double scale_opp_spin, double scale_same_spin,
+                                            size_t print_level = 0) {
+  const size_t n_spin = orbitals.size();
+  if (n_spin < 1 || n_spin > 2) throw std::logic_error("invalid number of spin channels");
+  if (occupations.size() < 1 || occupations.size() > 2)
+    throw std::logic_error("invalid number of spin channels");
+  if (occupations.size() != n_spin)
+    throw std::runtime_error("Different number of spin channels for orbitals and occupations");
+  if (n_active.size() < 1 || n_active.size() > 2)
+    throw std::logic_error("invalid number of spin channels");
+  if (n_active.size() != n_spin)
+    throw std::runtime_error("Different number of spin channels in n_active and orbitals");
+  const size_t n_ao = orbitals[0].n_rows();
+  std::vector<const double*> C, occ;
+  std::vector<size_t> ldc, n_orb, n_occ;
+  for (size_t s = 0; s < n_spin; ++s) {
+    if (orbitals[s].n_rows() != n_ao)
+      throw std::runtime_error("Inconsistent number of atomic orbitals");
+    C.push_back(orbitals[s].memptr());
+    ldc.push_back(n_ao);
+    n_orb.push_back(orbitals[s].n_cols());
+    occ.push_back(occupations[s].memptr());
+    n_occ.push_back(occupations[s].n_elem());
+  }
+  utils::FockMatrixAndEnergy out;
+  linalg::Mat fock(n_ao, n_ao * n_spin);
+  double terms[3];
+  detail::check(uw12c_form_fock(W.handle(), V.handle(), WV.handle(), abs_projectors.handle(),
+                                n_ao, n_spin, C.data(), ldc.data(), n_orb.data(), occ.data(),
+                                n_occ.data(), n_active.data(), indirect_term ? 1 : 0,
+                                calculate_fock ? 1 : 0, scale_opp_spin, scale_same_spin,
+                                print_level, &out.energy, terms,
+                                calculate_fock ? fock.memptr() : nullptr, UW12C_MEM_HOST));
+  for (size_t s = 0; s < n_spin; ++s)
+    out.fock.emplace_back(fock.memptr() + s * n_ao * n_ao, n_ao, n_ao);
+  return out;
+}
+
+/// libuw12.hpp:42-50.
+inline BaseIntegrals setup_base_integrals(const double* X3, const double* X2, const double* X3_ri,
+                                          size_t n_ao, size_t n_df, size_t n_ri,
+                                          bool /*copy_data*/ = false) {
+  return BaseIntegrals::from_pointers(X3, X2, X3_ri, n_ao, n_df, n_ri, UW12C_MEM_HOST);
+}
+
+/// libuw12.hpp:64-70.
+inline BaseIntegrals setup_base_integrals(const double* X3, const double* X2, size_t n_ao,
+                                          size_t n_df, bool /*copy_data*/ = false) {
+  return BaseIntegrals::from_pointers(X3, X2, nullptr, n_ao, n_df, 0, UW12C_MEM_HOST);
+}
+
+/// libuw12.hpp:80.
+inline ABSProjectors setup_abs_projectors(const double* S, size_t n_ao, size_t n_ri) {
+  return ABSProjectors(S, n_ao, n_ri);
+}
+
+/// libuw12.hpp:90-92 / libuw12.cpp:58-77: alpha columns then beta.
+inline Orbitals setup_orbitals(const double* C, size_t n_ao, size_t n_orb, size_t n_spin) {
+  if (n_spin != 1 && n_spin != 2)
+    throw std::runtime_error("Number of spin channels must be 1 or 2");
+  Orbitals out;
+  for (size_t s = 0; s < n_spin; ++s) out.emplace_back(C + s * n_ao * n_orb, n_ao, n_orb);
+  return out;
+}
+
+/// libuw12.hpp:101 (closed shell).
+inline Occupations setup_occupations(const double* occ, size_t n_occ) {
+  return {linalg::Vec(occ, n_occ, 1)};
+}
+
+/// libuw12.hpp:111-113 (open shell).
+inline Occupations setup_occupations(const double* occ, size_t n_occ_alpha, size_t n_occ_beta) {
+  return {linalg::Vec(occ, n_occ_alpha, 1), linalg::Vec(occ + n_occ_alpha, n_occ_beta, 1)};
+}
+
+/// libuw12.hpp:129-140.
+inline double uw12_energy(const BaseIntegrals& W, const BaseIntegrals& V, const BaseIntegrals& WV,
+                          const ABSProjectors& abs_projectors, const Orbitals& orbitals,
+                          const Occupations& occ, const std::vector<size_t>& n_active,
+                          double scale_opp_spin, double scale_same_spin,
+                          size_t print_level = 0) {
+  const bool indirect = !(std::fabs(scale_same_spin) <= 4 * DBL_EPSILON);
+  return form_fock(W, V, WV, abs_projectors, orbitals, occ, n_active, indirect, false,
+                   scale_opp_spin, scale_same_spin, print_level)
+      .energy;
+}
+
+/// libuw12.hpp:157-169: fock receives n_ao x (n_ao * n_spin), spin blocks side by side.
+inline double uw12_fock(double* fock, const BaseIntegrals& W, const BaseIntegrals& V,
+                        const BaseIntegrals& WV, const ABSProjectors& abs_projectors,
+                        const Orbitals& orbitals, const Occupations& occ,
+                        const std::vector<size_t>& n_active, double scale_opp_spin,
+                        double scale_same_spin, size_t print_level = 0) {
+  const bool indirect = !(std::fabs(scale_same_spin) <= 4 * DBL_EPSILON);
+  const auto res = form_fock(W, V, WV, abs_projectors, orbitals, occ, n_active, indirect, true,
+                             scale_opp_spin, scale_same_spin, print_level);
+  const size_t n_ao = orbitals[0].n_rows();
+  for (size_t s = 0; s < res.fock.size(); ++s)
+    for (size_t e = 0; e < n_ao * n_ao; ++e) fock[s * n_ao * n_ao + e] = res.fock[s][e];
+  return res.energy;
+}
+
+}  // namespace uw12
+
+#endif  // UW12_B200_LIBUW12_HPP

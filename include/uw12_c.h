@@ -56,6 +56,12 @@ const char* uw12c_version(void);
  * (src/integrals/base_integrals.cpp:155-166). */
 int uw12c_integrals_create(const double* X3, const double* X2, const double* X3_ri, size_t n_ao,
                            size_t n_df, size_t n_ri, int mem_kind, uw12c_integrals** out);
+/* Replaces the BaseIntegrals(J3, df_vals) constructor
+ * (src/integrals/base_integrals.hpp:104, base_integrals.cpp:308-326):
+ * three-index integrals already in the metric eigenbasis (J3 = J3_0 P2,
+ * n_ao(n_ao+1)/2 x n_df) and their eigenvalues; no RI. */
+int uw12c_integrals_create_eigenbasis(const double* J3, const double* df_vals, size_t n_ao,
+                                      size_t n_df, int mem_kind, uw12c_integrals** out);
 int uw12c_integrals_destroy(uw12c_integrals* h);
 /* BaseIntegrals::get_number_ao/df/ri (src/integrals/base_integrals.hpp:196-202). */
 int uw12c_integrals_dims(const uw12c_integrals* h, size_t* n_ao, size_t* n_df, size_t* n_ri);

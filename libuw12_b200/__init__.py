@@ -73,6 +73,8 @@ def lib():
     L.uw12c_version.restype = ctypes.c_char_p
     L.uw12c_integrals_create.argtypes = [P, P, P, c_sz, c_sz, c_sz, ctypes.c_int,
                                          ctypes.POINTER(P)]
+    L.uw12c_integrals_create_eigenbasis.argtypes = [P, P, c_sz, c_sz, ctypes.c_int,
+                                                    ctypes.POINTER(P)]
     L.uw12c_integrals_destroy.argtypes = [P]
     L.uw12c_integrals_dims.argtypes = [P, PSZ, PSZ, PSZ]
     L.uw12c_integrals_df_vals.argtypes = [P, PD]
@@ -239,6 +241,21 @@ def setup_base_integrals(X3, X2, X3_ri=None, n_ao: Optional[int] = None,
                                       else ctypes.c_void_p(0), n_ao, n_df,
                                       n_ri if X3_ri is not None else 0, MEM_HOST, ctypes.byref(h))
     _check(st)
+    return BaseIntegrals(h)
+
+
+def base_integrals_eigenbasis(J3, df_vals) -> BaseIntegrals:
+    """``BaseIntegrals(J3, df_vals)`` (src/integrals/base_integrals.hpp:104): three-index
+    integrals already in the metric eigenbasis (J3 = J3_0 P2) and the eigenvalues; no RI."""
+    df_vals = np.ascontiguousarray(np.asarray(df_vals, dtype=np.float64).reshape(-1))
+    n_df = df_vals.size
+    J3 = np.asarray(J3, dtype=np.float64)
+    rows = J3.shape[0] if J3.ndim == 2 else J3.size // n_df
+    n_ao = int((np.sqrt(8 * rows + 1) - 1) / 2)
+    J3 = _col_major(J3, n_ao * (n_ao + 1) // 2, n_df)
+    h = ctypes.c_void_p()
+    _check(lib().uw12c_integrals_create_eigenbasis(_fptr(J3), _fptr(df_vals), n_ao, n_df,
+                                                   MEM_HOST, ctypes.byref(h)))
     return BaseIntegrals(h)
 
 

@@ -234,6 +234,19 @@ int uw12c_integrals_create(const double* X3, const double* X2, const double* X3_
   });
 }
 
+int uw12c_integrals_create_eigenbasis(const double* J3, const double* df_vals, size_t n_ao,
+                                      size_t n_df, int mem_kind, uw12c_integrals** out) {
+  return guarded([&] {
+    need(out != nullptr, "null output handle");
+    need(mem_kind == UW12C_MEM_HOST || mem_kind == UW12C_MEM_DEVICE, "bad mem_kind");
+    *out = nullptr;
+    auto h = std::make_unique<uw12c_integrals>();
+    h->h.reset(uw12b::integrals_create_eigenbasis(J3, df_vals, n_ao, n_df,
+                                                  mem_kind == UW12C_MEM_DEVICE));
+    *out = h.release();
+  });
+}
+
 int uw12c_integrals_destroy(uw12c_integrals* h) {
   return guarded([&] { delete h; });
 }

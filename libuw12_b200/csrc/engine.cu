@@ -137,6 +137,35 @@ IntegralsHandle* integrals_create(const double* X3, const double* X2, const doub
   return h;
 }
 
+IntegralsHandle* integrals_create_eigenbasis(const double* J3, const double* df_vals, size_t n_ao,
+                                             size_t n_df, bool device_mem) {
+  if (n_ao == 0) throw_runtime("Number of ao orbitals is zero");
+  if (n_df == 0) throw_runtime("Number of density-fitting basis functions is zero");
+  if (!J3 || !df_vals) throw Error(kErrInvalid, "null integral pointer");
+  auto h = new IntegralsHandle();
+  try {
+    UW12_CUDA(cudaGetDevice(&h->device));
+    cudaStream_t s = current_stream();
+    h->n_ao = n_ao;
+    h->n_df = n_df;
+    const size_t np = packed_size(n_ao);
+    h->J3_0.alloc(np * n_df);
+    upload(h->J3_0.get(), J3, np * n_df, device_mem, s);
+    h->P2.alloc(n_df * n_df);
+    set_identity(h->P2.get(), LL(n_df));
+    h->lam.alloc(n_df);
+    upload(h->lam.get(), df_vals, n_df, device_mem, s);
+    h->lam_host.resize(n_df);
+    UW12_CUDA(cudaMemcpyAsync(h->lam_host.data(), h->lam.get(), n_df * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+    UW12_CUDA(cudaStreamSynchronize(s));
+  } catch (...) {
+    delete h;
+    throw;
+  }
+  return h;
+}
+
 AbsHandle* abs_create(const double* S, size_t n_ao, size_t n_ri, bool device_mem) {
   if (!S) throw Error(kErrInvalid, "null overlap pointer");
   const size_t n = n_ao + n_ri;

@@ -52,6 +52,10 @@ struct AbsHandle {
 
 IntegralsHandle* integrals_create(const double* X3, const double* X2, const double* X3_ri,
                                   size_t n_ao, size_t n_df, size_t n_ri, bool device_mem);
+// BaseIntegrals(J3, df_vals) (base_integrals.cpp:308-326): three-index
+// integrals already in the metric eigenbasis; P2 = I, Lambda = df_vals, no RI.
+IntegralsHandle* integrals_create_eigenbasis(const double* J3, const double* df_vals, size_t n_ao,
+                                             size_t n_df, bool device_mem);
 AbsHandle* abs_create(const double* S, size_t n_ao, size_t n_ri, bool device_mem);
 
 struct FockRequest {

@@ -249,6 +249,13 @@ __global__ void k_scale_pinv_cols(double* Q, long long n, const double* __restri
   }
 }
 
+__global__ void k_set_identity(double* A, long long n) {
+  const long long total = n * n;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x)
+    A[idx] = (idx % n == idx / n) ? 1.0 : 0.0;
+}
+
 __global__ void k_gather_scale_cols(const double* __restrict__ src, long long rows,
                                     const int* __restrict__ idxv, const double* __restrict__ s,
                                     long long nq, double* dst) {
@@ -383,6 +390,12 @@ void combine_vecs(const double* U, long long m, int ns, const double* coef, cons
 void scale_pinv_cols(double* Q, long long n, const double* lambda, double tol) {
   if (n <= 0) return;
   k_scale_pinv_cols<<<grid_for(n * n), kT, 0, current_stream()>>>(Q, n, lambda, tol);
+  UW12_LAUNCHED();
+}
+
+void set_identity(double* A, long long n) {
+  if (n <= 0) return;
+  k_set_identity<<<grid_for(n * n), kT, 0, current_stream()>>>(A, n);
   UW12_LAUNCHED();
 }
 

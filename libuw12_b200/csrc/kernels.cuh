@@ -61,6 +61,9 @@ void combine_vecs(const double* U, long long m, int ns, const double* coef, cons
 // P2 = Q * diag(pinv(lambda)) with |lambda| <= tol -> 0; in place on Q (n x n).
 void scale_pinv_cols(double* Q, long long n, const double* lambda, double tol);
 
+// A = I (n x n, column-major).
+void set_identity(double* A, long long n);
+
 // Gather columns: dst[:, q] = src[:, idx[q]] * s[q] (idx, s on device).
 void gather_scale_cols(const double* src, long long rows, const int* idx, const double* s,
                        long long nq, double* dst);

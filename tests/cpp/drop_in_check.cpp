@@ -1,0 +1,106 @@
+// Drives the C++ drop-in header (include/libuw12.hpp) the way a libuw12 caller
+// does (compare example/example.cpp of libuw12): raw-pointer setup calls,
+// uw12_fock / uw12_energy, the callback BaseIntegrals constructor and the
+// error behaviour.  Input and output are flat binary files written and read by
+// tests/test_gpu_cpp_drop_in.py.
+#include <cstdint>
+#include <cstdio>
+#include <fstream>
+#include <iostream>
+#include <stdexcept>
+#include <vector>
+
+#include "libuw12.hpp"
+
+namespace {
+
+std::vector<double> read_doubles(std::ifstream& f, size_t n) {
+  std::vector<double> v(n);
+  f.read(reinterpret_cast<char*>(v.data()), static_cast<std::streamsize>(n * sizeof(double)));
+  if (!f) throw std::runtime_error("short input file");
+  return v;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc != 3) {
+    std::cerr << "usage: drop_in_check <input> <output>\n";
+    return 2;
+  }
+  std::ifstream in(argv[1], std::ios::binary);
+  int64_t hdr[9];
+  in.read(reinterpret_cast<char*>(hdr), sizeof(hdr));
+  const size_t n_ao = hdr[0], n_df = hdr[1], n_ri = hdr[2], n_spin = hdr[3], n_orb = hdr[4];
+  const size_t n_occ_a = hdr[5], n_occ_b = hdr[6];
+  const std::vector<size_t> n_active = n_spin == 1 ? std::vector<size_t>{size_t(hdr[7])}
+                                                    : std::vector<size_t>{size_t(hdr[7]),
+                                                                          size_t(hdr[8])};
+  const size_t np = n_ao * (n_ao + 1) / 2;
+  const auto W3 = read_doubles(in, np * n_df), W2 = read_doubles(in, n_df * n_df),
+             W3r = read_doubles(in, n_ri * n_ao * n_df);
+  const auto V3 = read_doubles(in, np * n_df), V2 = read_doubles(in, n_df * n_df),
+             V3r = read_doubles(in, n_ri * n_ao * n_df);
+  const auto WV3 = read_doubles(in, np * n_df), WV2 = read_doubles(in, n_df * n_df);
+  const auto S = read_doubles(in, (n_ao + n_ri) * (n_ao + n_ri));
+  const auto C = read_doubles(in, n_ao * n_orb * n_spin);
+  const auto occ = read_doubles(in, n_occ_a + n_occ_b);
+  const auto scales = read_doubles(in, 2);
+
+  // libuw12's public API, raw pointers in (libuw12.hpp:42-169)
+  const auto W = uw12::setup_base_integrals(W3.data(), W2.data(), W3r.data(), n_ao, n_df, n_ri);
+  const auto V = uw12::setup_base_integrals(V3.data(), V2.data(), V3r.data(), n_ao, n_df, n_ri);
+  const auto WV = uw12::setup_base_integrals(WV3.data(), WV2.data(), n_ao, n_df);
+  const auto abs = uw12::setup_abs_projectors(S.data(), n_ao, n_ri);
+  const auto orbitals = uw12::setup_orbitals(C.data(), n_ao, n_orb, n_spin);
+  const auto occupations = n_spin == 1 ? uw12::setup_occupations(occ.data(), n_occ_a)
+                                       : uw12::setup_occupations(occ.data(), n_occ_a, n_occ_b);
+  std::vector<double> fock(n_ao * n_ao * n_spin);
+  const double e_fock = uw12::uw12_fock(fock.data(), W, V, WV, abs, orbitals, occupations,
+                                        n_active, scales[0], scales[1]);
+  const double e_only = uw12::uw12_energy(W, V, WV, abs, orbitals, occupations, n_active,
+                                          scales[0], scales[1]);
+
+  // The callback constructor with df shells of sizes 1, 3, 5, 7, ...
+  std::vector<size_t> shells, offsets;
+  for (size_t off = 0, s = 1; off < n_df; s += 2) {
+    const size_t w = std::min(s, n_df - off);
+    shells.push_back(w);
+    offsets.push_back(off);
+    off += w;
+  }
+  const uw12::integrals::TwoIndexFn two = [&] { return uw12::linalg::Mat(W2.data(), n_df, n_df); };
+  const uw12::integrals::ThreeIndexFn three = [&](size_t A) {
+    return uw12::linalg::Mat(W3.data() + np * offsets[A], np, shells[A]);
+  };
+  const uw12::integrals::ThreeIndexFn three_ri = [&](size_t A) {
+    return uw12::linalg::Mat(W3r.data() + n_ri * n_ao * offsets[A], n_ri * n_ao, shells[A]);
+  };
+  const uw12::BaseIntegrals W_cb(two, three, three_ri, shells, n_ao, n_df, n_ri);
+  const double e_cb = uw12::uw12_energy(W_cb, V, WV, abs, orbitals, occupations, n_active,
+                                        scales[0], scales[1]);
+
+  // Error behaviour (libuw12.cpp:61-63, utils.hpp:235-253)
+  double errors = 0;
+  try {
+    uw12::setup_orbitals(C.data(), n_ao, n_orb, 3);
+  } catch (const std::runtime_error&) {
+    errors += 1;
+  }
+  try {
+    std::vector<size_t> too_many = n_active;
+    too_many[0] = n_orb + 1;
+    uw12::uw12_energy(W, V, WV, abs, orbitals, occupations, too_many, scales[0], scales[1]);
+  } catch (const std::logic_error&) {
+    errors += 1;
+  }
+
+  std::ofstream out(argv[2], std::ios::binary);
+  const double head[4] = {e_fock, e_only, e_cb, errors};
+  out.write(reinterpret_cast<const char*>(head), sizeof(head));
+  out.write(reinterpret_cast<const char*>(fock.data()),
+            static_cast<std::streamsize>(fock.size() * sizeof(double)));
+  std::printf("drop_in_check: E=%.15e (energy-only %.15e, callback integrals %.15e)\n", e_fock,
+              e_only, e_cb);
+  return 0;
+}

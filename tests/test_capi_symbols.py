@@ -33,6 +33,17 @@ def test_version_and_error_state_without_gpu(uw12lib):
     assert L.uw12c_last_error(buf, 64) == 0
 
 
+def test_cpp_drop_in_header_compiles(uw12lib, tmp_path):
+    """include/libuw12.hpp (libuw12's C++ API over the C-ABI) compiles and links."""
+    import subprocess
+    lib_dir = uw12lib.library_path().parent
+    out = tmp_path / "drop_in_check"
+    r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", f"-I{ROOT / 'include'}",
+                        str(ROOT / "tests" / "cpp" / "drop_in_check.cpp"), "-o", str(out),
+                        f"-L{lib_dir}", "-luw12_b200"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
 def test_invalid_arguments_are_rejected_without_touching_the_device(uw12lib):
     L = uw12lib.lib()
     out = ctypes.c_void_p()

@@ -146,6 +146,24 @@ def test_unequal_df_sizes_rejected(uw12lib, cuda_device):
         uw12lib.form_fock(W, V, WV, A, c1.orbitals, c1.occ, [3], True, True, 1.0, 0.5)
 
 
+def test_eigenbasis_integrals_constructor(uw12lib, cuda_device):
+    """BaseIntegrals(J3, df_vals) (base_integrals.hpp:104) with J3 = J3_0 P2 gives the
+    same result as BaseIntegrals(J3_0, J2) (the metric enters only through P2 Λ P2^T)."""
+    from oracle import uw12_oracle as O
+    case = CASES[2]
+    d = make_case(case)
+    W, V, WV, A = _gpu_objects(uw12lib, d)
+    ob = O.BaseIntegrals(d.WV3, d.WV2)
+    WV_eig = uw12lib.base_integrals_eigenbasis(d.WV3 @ ob.P2, ob.df_vals)
+    e1, f1, _ = uw12lib.form_fock(W, V, WV, A, d.orbitals, d.occ, case.n_active, True, True,
+                                  1.0, 0.5)
+    e2, f2, _ = uw12lib.form_fock(W, V, WV_eig, A, d.orbitals, d.occ, case.n_active, True, True,
+                                  1.0, 0.5)
+    assert abs(e1 - e2) <= 1e-9 * abs(e1)
+    for s in range(2):
+        assert np.max(np.abs(f1[s] - f2[s])) <= 1e-8 * np.max(np.abs(f1[s]))
+
+
 def test_abs_projectors_match_oracle(uw12lib, cuda_device):
     from oracle import uw12_oracle as O
     d = make_case(CASES[0])
