@@ -6,11 +6,15 @@ synthetic inputs (three-index N(0,1) exp(-|m-n|/30), metrics B B^T + 1e-6 I,
 S-orthonormal orbitals), FP64 throughout.  One step = one energy + Fock
 evaluation (uw12 form_fock with the integrals resident in HBM).
 
-``value`` is seconds per evaluation for the whole job (max-over-ranks device
-time / evaluations of all ranks); ranks evaluate independent molecules
-(weak scaling, no collective on the data path).  ``e2e`` is the same metric
+``value`` is seconds per evaluation (max-over-ranks device time / steps).
+With N > 1 ranks one evaluation is split over the ranks (strong scaling):
+each rank holds the full integrals, evaluates its shard (a contiguous part of
+the aux functions of the t~ dX Fock term and of the occupied orbitals of the
+same-spin three-electron terms; the rest on rank 0) and one NCCL all-reduce
+sums the partial Fock matrices and energies.  ``e2e`` is the same metric
 through the C-ABI from pinned host buffers: integral upload, on-device metric
-and overlap eigensolves, evaluation and Fock read-back per step.
+and overlap eigensolves, evaluation (and all-reduce) and Fock read-back per
+step.
 
 ``--impl reference`` times the CPU restatement of libuw12's algorithm (the
 oracle; libuw12 itself cannot be built here) on the host cores for the same
@@ -273,7 +277,7 @@ def run_reference(args, rank, world):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s/eval",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3,
-        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded, numpy PCG64 streams)",
         "config": config_dict(args),
         "cpu_baseline": {"value": value, "unit": "s/eval", "cores": cores, "kind": "port",
@@ -335,7 +339,7 @@ def main():
     cfg = CONFIGS[args.config]
     N, M, R, occ, _ = cfg
     act = list(occ)
-    t, orbs, occs = make_device_inputs(cfg, 11 + rank, device)
+    t, orbs, occs = make_device_inputs(cfg, 11, device)
     peak = fp64_peak_tflops(device)
 
     W = L.setup_base_integrals(t["W3"].data_ptr(), t["W2"].data_ptr(), t["W3_ri"].data_ptr(),
@@ -348,9 +352,17 @@ def main():
     fock_dev = torch.empty(N * N * len(occ), dtype=torch.float64, device=device)
     indirect = abs(args.s_ss) > 4 * np.finfo(float).eps
 
+    from libuw12_b200.distributed import form_fock_sharded
+
+    def evaluate(Wh, Vh, WVh, Ah, fock):
+        if world > 1:
+            return form_fock_sharded(Wh, Vh, WVh, Ah, orbs, occs, act, indirect, True, args.s_os,
+                                     args.s_ss, fock)[0]
+        return L.form_fock(Wh, Vh, WVh, Ah, orbs, occs, act, indirect, True, args.s_os,
+                           args.s_ss, fock_out=fock.data_ptr())[0]
+
     def step():
-        return L.form_fock(W, V, WV, A, orbs, occs, act, indirect, True, args.s_os, args.s_ss,
-                           fock_out=fock_dev.data_ptr())[0]
+        return evaluate(W, V, WV, A, fock_dev)
 
     for _ in range(args.warmup):
         energy = step()
@@ -381,7 +393,7 @@ def main():
         tt = torch.tensor([elapsed], dtype=torch.float64, device=device)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         elapsed = float(tt.item())
-    s_per_eval = elapsed / (args.steps * world)
+    s_per_eval = elapsed / args.steps
 
     # ---- end to end through the C-ABI from pinned host buffers
     e2e = None
@@ -413,7 +425,12 @@ def main():
             WVe = L.setup_base_integrals(hp["WV3"].reshape((np_, M), order="F"),
                                          hp["WV2"].reshape((M, M)))
             Ae = L.setup_abs_projectors(hp["S"].reshape((N + R, N + R)), N, R)
-            e_e2e, fock_host = L.uw12_fock(We, Ve, WVe, Ae, orbs, occs, act, args.s_os, args.s_ss)
+            if world > 1:
+                e_e2e = evaluate(We, Ve, WVe, Ae, fock_dev)
+                fock_host = fock_dev.cpu()
+            else:
+                e_e2e, fock_host = L.uw12_fock(We, Ve, WVe, Ae, orbs, occs, act, args.s_os,
+                                               args.s_ss)
             for h in (We, Ve, WVe, Ae):
                 h.close()
         torch.cuda.synchronize(device)
@@ -422,7 +439,7 @@ def main():
             tt = torch.tensor([te], dtype=torch.float64, device=device)
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             te = float(tt.item())
-        e2e = {"value": te / (args.e2e_steps * world), "unit": "s/eval",
+        e2e = {"value": te / args.e2e_steps, "unit": "s/eval",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "includes": "H2D of all integrals from pinned host memory, metric/overlap "
                            "eigensolves, evaluation, Fock D2H",
@@ -462,9 +479,11 @@ def main():
         line = {
             "metric": METRIC, "value": s_per_eval, "unit": "s/eval", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3,
-            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generators; integrals generated on device)",
-            "config": config_dict(args),
+            "config": dict(config_dict(args), parallelism=(
+                "single GPU" if world == 1 else
+                f"{world}-way sharded evaluation + NCCL all-reduce of Fock and energy")),
             "tflops_canonical": flops / s_per_eval / 1e12,
             "canonical_flops_per_eval": flops,
             "energy": energy,

@@ -117,6 +117,16 @@ int uw12c_energy(const uw12c_integrals* W, const uw12c_integrals* V, const uw12c
  * profiling is on). */
 int uw12c_set_stream(void* stream);
 int uw12c_set_memory_budget(size_t bytes);
+/* Splits the following evaluations of this host thread into n_shards parts
+ * and computes part `shard` only (no counterpart in libuw12): the loops of
+ * the t~ dX Fock term (over aux functions) and of the same-spin
+ * three-electron energy and Fock (over occupied orbitals k) run over a
+ * contiguous, balanced part of their range; every other contribution is
+ * computed by shard 0.  Energies and
+ * Fock matrices of the n_shards parts sum to the full result (one GPU per
+ * shard, summed with an all-reduce).  uw12c_set_shard(0, 1) restores full
+ * evaluations. */
+int uw12c_set_shard(size_t shard, size_t n_shards);
 /* The library keeps device memory freed by one call reserved for the next
  * (its own stream-ordered pool); this returns the unused part to the system. */
 int uw12c_trim_memory(void);

@@ -90,6 +90,7 @@ def lib():
                                c_sz, PD]
     L.uw12c_set_stream.argtypes = [P]
     L.uw12c_set_memory_budget.argtypes = [c_sz]
+    L.uw12c_set_shard.argtypes = [c_sz, c_sz]
     L.uw12c_launch_count.restype = ctypes.c_ulonglong
     L.uw12c_profile_enable.argtypes = [ctypes.c_int]
     L.uw12c_profile_read.argtypes = [ctypes.POINTER(ctypes.c_ulonglong), PD, PD]
@@ -371,6 +372,12 @@ def uw12_energy(W, V, WV, abs_p, orbitals, occ, n_active, scale_opp_spin, scale_
 
 def set_stream(stream_ptr: int):
     _check(lib().uw12c_set_stream(ctypes.c_void_p(stream_ptr)))
+
+
+def set_shard(shard: int, n_shards: int):
+    """Evaluate only part `shard` of `n_shards` in subsequent calls on this thread
+    (partial energies and Fock matrices sum to the full result)."""
+    _check(lib().uw12c_set_shard(int(shard), int(n_shards)))
 
 
 def set_memory_budget(nbytes: int):

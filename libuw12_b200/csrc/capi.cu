@@ -21,6 +21,7 @@ namespace {
 std::atomic<unsigned long long> g_launches{0};
 thread_local cudaStream_t g_stream = nullptr;
 std::atomic<size_t> g_budget{0};
+thread_local size_t g_shard = 0, g_n_shards = 1;
 thread_local int g_last_status = UW12C_OK;
 thread_local std::string g_last_msg;
 }  // namespace
@@ -184,6 +185,8 @@ void run_form_fock(const uw12c_integrals* W, const uw12c_integrals* V, const uw1
   rq.fock = fock;
   rq.fock_device = fock_mem == UW12C_MEM_DEVICE;
   rq.mem_budget = uw12b::g_budget.load();
+  rq.shard = uw12b::g_shard;
+  rq.n_shards = uw12b::g_n_shards;
   DeviceGuard dg(w.device);
   uw12b::form_fock(rq);
 }
@@ -342,6 +345,14 @@ int uw12c_energy(const uw12c_integrals* W, const uw12c_integrals* V, const uw12c
 
 int uw12c_set_stream(void* stream) {
   return guarded([&] { uw12b::set_current_stream(static_cast<cudaStream_t>(stream)); });
+}
+
+int uw12c_set_shard(size_t shard, size_t n_shards) {
+  return guarded([&] {
+    need(n_shards >= 1 && shard < n_shards, "shard must be < n_shards, n_shards >= 1");
+    uw12b::g_shard = shard;
+    uw12b::g_n_shards = n_shards;
+  });
 }
 
 int uw12c_trim_memory(void) {

@@ -89,7 +89,9 @@ size_t auto_budget_doubles(size_t requested_bytes) {
   size_t free_b = 0, total_b = 0;
   UW12_CUDA(cudaMemGetInfo(&free_b, &total_b));
   size_t b = requested_bytes ? requested_bytes : static_cast<size_t>(0.45 * double(free_b));
-  b = std::max<size_t>(b, size_t(64) << 20);
+  // an explicit budget may be small (many small chunks); the automatic one
+  // never drops below 64 MiB
+  b = std::max<size_t>(b, requested_bytes ? size_t(64) << 10 : size_t(64) << 20);
   return b / sizeof(double);
 }
 
@@ -344,6 +346,16 @@ void form_fock(const FockRequest& rq) {
   const double kap4 = 2.0 * half;
   cudaStream_t st = current_stream();
   const size_t budget = auto_budget_doubles(rq.mem_budget);
+  // Sharding: the chunk loops (t~ dX over aux functions, same-spin 3-el
+  // energy and Fock over occupied k) run over a contiguous, balanced part of
+  // their index range per shard; all other contributions come from shard 0
+  // only.  The caller sums the partial energies and Fock matrices over shards.
+  const size_t n_shards = std::max<size_t>(1, rq.n_shards);
+  const size_t shard = rq.shard;
+  const bool lead = shard == 0;
+  auto part = [&](size_t total) {
+    return std::make_pair(total * shard / n_shards, total * (shard + 1) / n_shards);
+  };
 
   std::vector<SpinDims> sd(ns);
   size_t o_tot = 0, a_tot = 0;
@@ -396,7 +408,7 @@ void form_fock(const FockRequest& rq) {
   // two-electron term (two_electron.cpp:11-153), WV integrals, active orbitals
   // =====================================================================
   clock.mark("two_electron");
-  {
+  if (lead) {
     DevBuf dmat(np * ns), XDr(MX * ns), XD(MX * ns);
     for (int s = 0; s < ns; ++s) pack_density(Ca_s(s), LL(N), LL(N), LL(sd[s].a), two, dmat.get() + np * s);
     GemmDesc g = gemm_nn(LL(MX), ns, LL(np), 1.0, WV.J3_0.get(), LL(np), dmat.get(), LL(np), 0.0,
@@ -544,7 +556,7 @@ void form_fock(const FockRequest& rq) {
     scale_rc(tab[s].get(), LL(MW), LL(MW), LL(MV), W.lam.get(), V.lam.get(), 1.0, ttl[s].get(),
              LL(MW));
   }
-  for (int s = 0; s < ns; ++s)
+  for (int s = 0; s < ns && lead; ++s)
     for (int sp = 0; sp < ns; ++sp) {
       const double f = spin_factor(ns, s, sp, s_os, s_ss);
       wdot(Xab[s].get(), LL(MW), ttl[sp].get(), LL(MW), LL(MW), LL(MV), nullptr, nullptr, -f,
@@ -561,7 +573,7 @@ void form_fock(const FockRequest& rq) {
   // =====================================================================
   if (calc) {
     clock.mark("direct_fock");
-    for (int s = 0; s < ns; ++s) {
+    for (int s = 0; s < ns && lead; ++s) {
       const size_t o = sd[s].o, a = sd[s].a, c = sd[s].c;
       if (!o) continue;
       const double* Tq[2] = {ttl[0].get(), ns > 1 ? ttl[1].get() : nullptr};
@@ -614,10 +626,12 @@ void form_fock(const FockRequest& rq) {
     }
     if (!tdx_spins.empty()) {
       const size_t per_a = 3 * Rp * N + np;
-      const size_t ac = tile_chunk(MW, 1, std::max<size_t>(1, std::min(MW, budget / per_a)));
+      const auto [alo, ahi] = part(MW);
+      const size_t ac = tile_chunk(ahi - alo, 1,
+                                   std::max<size_t>(1, std::min(ahi - alo, budget / per_a)));
       DevBuf sbuf(np * ac), Gst(Rp * N * ac), Lb(Rp * N * ac), Hb(Rp * N * ac);
-      for (size_t a0 = 0; a0 < MW; a0 += ac) {
-        const size_t na = std::min(ac, MW - a0);
+      for (size_t a0 = alo; a0 < ahi; a0 += ac) {
+        const size_t na = std::min(ac, ahi - a0);
         // G_W chunk, AO rows then RI rows of each (R' x N) block
         unpack_sym(W.J3_0.get() + np * a0, LL(np), LL(N), LL(na), Gst.get(), LL(Rp), LL(Rp * N));
         copy3d(W.J3_ri_0.get() + R * N * a0, LL(R), LL(R * N), Gst.get() + N, LL(Rp), LL(Rp * N),
@@ -663,7 +677,7 @@ void form_fock(const FockRequest& rq) {
       scale_rc(XV.B2[s].get(), LL(ao), LL(ao), LL(MV), nullptr, V.lam.get(), 1.0, b2vl.get(), LL(ao));
       clock.mark("ss_4el_energy");
       // ---- 4-el indirect energy (four_electron.cpp:143-179)
-      {
+      if (lead) {
         DevBuf W4(ao * ao), V4(ao * ao);
         GemmDesc g = gemm_nn(LL(ao), LL(ao), LL(MW), 1.0, b2wl.get(), LL(ao), XW.B2[s].get(),
                              LL(ao), 0.0, W4.get(), LL(ao));
@@ -679,10 +693,12 @@ void form_fock(const FockRequest& rq) {
       // ---- 3-el indirect energy (indirect_utils.cpp:101-133), chunked over k
       {
         const size_t per_k = 2 * Rp * a * a;
-        const size_t kc = tile_chunk(o, a, std::max<size_t>(1, std::min(o, budget / per_k)));
+        const auto [klo, khi] = part(o);
+        const size_t kc = tile_chunk(khi - klo, a,
+                                     std::max<size_t>(1, std::min(khi - klo, budget / per_k)));
         DevBuf YW(Rp * a * a * kc), ZV(Rp * a * a * kc);
-        for (size_t k0 = 0; k0 < o; k0 += kc) {
-          const size_t nk = std::min(kc, o - k0);
+        for (size_t k0 = klo; k0 < khi; k0 += kc) {
+          const size_t nk = std::min(kc, khi - k0);
           GemmDesc g = gemm_nn(LL(Rp * a), LL(a * nk), LL(MW), 1.0, XW.Wst[s].get(), LL(Rp * a),
                                b2wl.get() + a * k0, LL(ao), 0.0, YW.get(), LL(Rp * a));
           g.b_ncontig = true;
@@ -700,7 +716,7 @@ void form_fock(const FockRequest& rq) {
       scale_rc(XV.B1[s].get(), LL(No), LL(No), LL(MV), nullptr, V.lam.get(), 1.0, b1vl.get(), LL(No));
       clock.mark("ss_4el_fock");
       // ---- 4-el indirect Fock (four_electron.cpp:181-249)
-      {
+      if (lead) {
         DevBuf W43(No * ao), V43(No * ao);
         GemmDesc g = gemm_nn(LL(No), LL(ao), LL(MW), 1.0, b1wl.get(), LL(No), XW.B2[s].get(),
                              LL(ao), 0.0, W43.get(), LL(No));
@@ -747,11 +763,13 @@ void form_fock(const FockRequest& rq) {
         g.b_ncontig = true;
         gemm(g);
         const size_t per_k = 3 * Rp * a * N + a * (N * N + R * N + np);
-        const size_t kc = tile_chunk(o, a, std::max<size_t>(1, std::min(o, budget / per_k)));
+        const auto [klo, khi] = part(o);
+        const size_t kc = tile_chunk(khi - klo, a,
+                                     std::max<size_t>(1, std::min(khi - klo, budget / per_k)));
         DevBuf ZYV(Rp * a * N * kc), ZYW(Rp * a * N * kc), gpk(np * a * kc), Gao(N * N * a * kc),
             gri(R * N * a * kc), Wk(Rp * N * a * kc);
-        for (size_t k0 = 0; k0 < o; k0 += kc) {
-          const size_t nk = std::min(kc, o - k0);
+        for (size_t k0 = klo; k0 < khi; k0 += kc) {
+          const size_t nk = std::min(kc, khi - k0);
           for (int term = 0; term < 2; ++term) {
             // term 0: fock_i(W, V) over (j, k); term 1: fock_i(V, W) over (i, k)
             const IntegralsHandle& Xi = term == 0 ? W : V;

@@ -80,6 +80,7 @@ struct FockRequest {
   bool fock_device = false;         // fock points to device memory
   double* terms = nullptr;          // host: {E2, E3, E4} or null
   size_t mem_budget = 0;            // bytes for chunked intermediates (0 = auto)
+  size_t shard = 0, n_shards = 1;   // partial evaluation: this shard's share only
 };
 
 void form_fock(const FockRequest& rq);

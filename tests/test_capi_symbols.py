@@ -2,6 +2,8 @@
 function declared in include/uw12_c.h (no compute calls)."""
 import ctypes
 import re
+
+import pytest
 from pathlib import Path
 
 ROOT = Path(__file__).resolve().parents[1]
@@ -52,3 +54,13 @@ def test_invalid_arguments_are_rejected_without_touching_the_device(uw12lib):
     assert L.uw12c_abs_create(None, 3, 4, 0, None) == 5
     buf = ctypes.create_string_buffer(256)
     assert L.uw12c_last_error(buf, 256) == 5 and buf.value
+
+
+def test_shard_arguments_are_validated_without_touching_the_device(uw12lib):
+    L = uw12lib.lib()
+    assert L.uw12c_set_shard(2, 2) == 5
+    assert L.uw12c_set_shard(0, 0) == 5
+    with pytest.raises(uw12lib.UW12Error):
+        uw12lib.set_shard(3, 2)
+    assert L.uw12c_set_shard(1, 2) == 0
+    assert L.uw12c_set_shard(0, 1) == 0
