@@ -173,6 +173,35 @@ int uw12c_dgemm_noalloc(long long m, long long n, long long k, double alpha, con
                         long long nbo2, const long long* so, long long nbr1, long long nbr2,
                         const long long* sr, int split);
 
+/* Split precision (no counterpart in libuw12, which computes in FP64 only).
+ * uw12c_set_precision(L) makes the following evaluations of this host thread
+ * run every GEMM of at least 2e9 FLOPs as a split-precision GEMM with L
+ * moduli (1..16; 0 = FP64 DMMA GEMMs, the default): each FP64 row of A and
+ * column of B is scaled by a power of two and rounded to an integer of beta
+ * bits, its residues modulo L coprime moduli <= 256 are multiplied exactly as
+ * int8 matrices on the tensor cores (int32 accumulation), and the Chinese
+ * remainder theorem rebuilds the FP64 product.  The error of one GEMM is at
+ * most 2^-beta (max|a_i.| sum_k |b_kj| + max|b_.j| sum_k |a_ik|) per element;
+ * uw12c_split_bits gives beta for L moduli and a contraction of k_total terms
+ * (48 bits for L = 14, k_total = 1500).  The metric and overlap
+ * eigensolves, energy reductions and Fock symmetrisation stay FP64. */
+int uw12c_set_precision(int n_moduli);
+/* GEMMs below min_flops stay FP64 in split-precision mode (default 2e9;
+ * 0 routes every GEMM through the split-precision path). */
+int uw12c_set_split_threshold(double min_flops);
+int uw12c_split_bits(int n_moduli, long long k_total, int* bits);
+/* uw12c_dgemm computed by the split-precision GEMM with n_moduli moduli. */
+int uw12c_dgemm_split(long long m, long long n, long long k, double alpha, const double* A,
+                      long long lda, int a_kcontig, const double* B, long long ldb, int b_ncontig,
+                      double beta, double* C, long long ldc, long long nbo1, long long nbo2,
+                      const long long* so, long long nbr1, long long nbr2, const long long* sr,
+                      int n_moduli);
+/* Timing of a kernel class while profiling is on: 0 FP64 DMMA GEMM (work =
+ * FLOPs), 1 whole split-precision GEMMs (FP64-equivalent FLOPs), 2 their int8
+ * tensor-core kernel (int8 operations), 3 their operand preparation and 4
+ * their CRT reconstruction (bytes read + written). */
+int uw12c_profile_read_kind(int kind, unsigned long long* launches, double* ms, double* work);
+
 /* Deterministic synthetic three-index tensors written on the device (no
  * counterpart in libuw12; benchmark input generation).  Element e of the
  * stream (seed, tag) is the Box-Muller normal of two SplitMix64 draws, times

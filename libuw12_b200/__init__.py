@@ -101,6 +101,12 @@ def lib():
                               ctypes.c_int]
     L.uw12c_synth_three_index.argtypes = [P, ctypes.c_int, c_sz, c_sz, c_sz, ctypes.c_ulonglong,
                                           ctypes.c_ulonglong, c_d]
+    L.uw12c_dgemm_split.argtypes = L.uw12c_dgemm.argtypes
+    L.uw12c_set_precision.argtypes = [ctypes.c_int]
+    L.uw12c_set_split_threshold.argtypes = [c_d]
+    L.uw12c_split_bits.argtypes = [ctypes.c_int, LL, ctypes.POINTER(ctypes.c_int)]
+    L.uw12c_profile_read_kind.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong),
+                                          ctypes.POINTER(c_d), ctypes.POINTER(c_d)]
     _lib = L
     return L
 
@@ -408,6 +414,46 @@ def dgemm(m, n, k, alpha, A, lda, a_kcontig, B, ldb, b_ncontig, beta, C, ldc, nb
     _check(lib().uw12c_dgemm(m, n, k, alpha, ctypes.c_void_p(A), lda, int(a_kcontig),
                              ctypes.c_void_p(B), ldb, int(b_ncontig), beta, ctypes.c_void_p(C),
                              ldc, nbo1, nbo2, LLa(*so), nbr1, nbr2, LLr(*sr), int(split)))
+
+
+def dgemm_split(m, n, k, alpha, A, lda, a_kcontig, B, ldb, b_ncontig, beta, C, ldc, nbo1=1,
+                nbo2=1, so=(0, 0, 0, 0, 0, 0), nbr1=1, nbr2=1, sr=(0, 0, 0, 0), n_moduli=14):
+    """``dgemm`` computed by the split-precision (int8 tensor-core, CRT) GEMM."""
+    LLa = ctypes.c_longlong * 6
+    LLr = ctypes.c_longlong * 4
+    _check(lib().uw12c_dgemm_split(m, n, k, alpha, ctypes.c_void_p(A), lda, int(a_kcontig),
+                                   ctypes.c_void_p(B), ldb, int(b_ncontig), beta,
+                                   ctypes.c_void_p(C), ldc, nbo1, nbo2, LLa(*so), nbr1, nbr2,
+                                   LLr(*sr), int(n_moduli)))
+
+
+def set_precision(n_moduli: int):
+    """Split-precision GEMMs with ``n_moduli`` moduli in subsequent evaluations on
+    this thread (0 = FP64)."""
+    _check(lib().uw12c_set_precision(int(n_moduli)))
+
+
+def set_split_threshold(min_flops: float):
+    """GEMMs below ``min_flops`` stay FP64 in split-precision mode (default 2e9)."""
+    _check(lib().uw12c_set_split_threshold(float(min_flops)))
+
+
+def split_bits(n_moduli: int, k_total: int) -> int:
+    """Bits kept per operand element by a split-precision GEMM."""
+    b = ctypes.c_int()
+    _check(lib().uw12c_split_bits(int(n_moduli), int(k_total), ctypes.byref(b)))
+    return b.value
+
+
+PROFILE_KINDS = ("dgemm", "split_gemm", "i8_mma", "split_prep", "split_crt")
+
+
+def profile_read_kind(kind: str) -> dict:
+    """Launches, milliseconds and work (FLOPs, int8 ops or bytes) of a kernel class."""
+    n, ms, w = ctypes.c_ulonglong(), ctypes.c_double(), ctypes.c_double()
+    _check(lib().uw12c_profile_read_kind(PROFILE_KINDS.index(kind), ctypes.byref(n),
+                                         ctypes.byref(ms), ctypes.byref(w)))
+    return {"launches": n.value, "ms": ms.value, "work": w.value}
 
 
 def profile_phases() -> dict:

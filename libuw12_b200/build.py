@@ -16,7 +16,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 OUT_DIR = HERE / "_lib"
 LIB = OUT_DIR / "libuw12_b200.so"
-SOURCES = ["gemm_f64.cu", "kernels.cu", "engine.cu", "synth.cu", "capi.cu"]
+SOURCES = ["gemm_f64.cu", "ozaki.cu", "kernels.cu", "engine.cu", "synth.cu", "capi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -11,6 +11,7 @@
 #include "../../include/uw12_c.h"
 #include "engine.cuh"
 #include "gemm_f64.cuh"
+#include "ozaki.cuh"
 
 namespace uw12b {
 
@@ -124,6 +125,14 @@ struct DeviceGuard {
 
 bool nearly_zero(double v) { return std::fabs(v) <= 4.0 * DBL_EPSILON; }  // utils.hpp:186-189
 
+// A split-precision GEMM kernel whose pipeline wait timed out leaves a device
+// flag; its results are not trusted.
+void check_split_pipeline() {
+  if (uw12b::split_moduli() > 0 && uw12b::ozaki_error_read_and_clear())
+    throw uw12b::Error(uw12b::kErrCuda,
+                       "split-precision GEMM: a tensor-core pipeline wait timed out");
+}
+
 void run_form_fock(const uw12c_integrals* W, const uw12c_integrals* V, const uw12c_integrals* WV,
                    const uw12c_abs* abs, size_t n_ao, size_t n_spin, const double* const* C,
                    const size_t* ldc, const size_t* n_orb, const double* const* occ,
@@ -189,6 +198,7 @@ void run_form_fock(const uw12c_integrals* W, const uw12c_integrals* V, const uw1
   rq.n_shards = uw12b::g_n_shards;
   DeviceGuard dg(w.device);
   uw12b::form_fock(rq);
+  check_split_pipeline();
 }
 
 void run_public(double* fock, const uw12c_integrals* W, const uw12c_integrals* V,
@@ -409,6 +419,58 @@ int uw12c_dgemm(long long m, long long n, long long k, double alpha, const doubl
     need(m >= 0 && n >= 0 && k >= 0 && nbo1 >= 0 && nbo2 >= 0 && nbr1 >= 0 && nbr2 >= 0,
          "negative size");
     uw12b::gemm(d);
+  });
+}
+
+int uw12c_set_precision(int n_moduli) {
+  return guarded([&] { uw12b::set_split_moduli(n_moduli); });
+}
+
+int uw12c_dgemm_split(long long m, long long n, long long k, double alpha, const double* A,
+                      long long lda, int a_kcontig, const double* B, long long ldb, int b_ncontig,
+                      double beta, double* C, long long ldc, long long nbo1, long long nbo2,
+                      const long long* so, long long nbr1, long long nbr2, const long long* sr,
+                      int n_moduli) {
+  return guarded([&] {
+    uw12b::GemmDesc d;
+    d.m = m; d.n = n; d.k = k; d.alpha = alpha; d.beta = beta;
+    d.A = A; d.lda = lda; d.a_kcontig = a_kcontig != 0;
+    d.B = B; d.ldb = ldb; d.b_ncontig = b_ncontig != 0;
+    d.C = C; d.ldc = ldc;
+    d.nbo1 = nbo1; d.nbo2 = nbo2;
+    if (so) { d.sAo1 = so[0]; d.sAo2 = so[1]; d.sBo1 = so[2]; d.sBo2 = so[3]; d.sCo1 = so[4]; d.sCo2 = so[5]; }
+    d.nbr1 = nbr1; d.nbr2 = nbr2;
+    if (sr) { d.sAr1 = sr[0]; d.sAr2 = sr[1]; d.sBr1 = sr[2]; d.sBr2 = sr[3]; }
+    need(m >= 0 && n >= 0 && k >= 0 && nbo1 >= 0 && nbo2 >= 0 && nbr1 >= 0 && nbr2 >= 0,
+         "negative size");
+    need(n_moduli >= 1 && n_moduli <= uw12b::kOzakiMaxModuli, "n_moduli must be 1..16");
+    need(uw12b::ozaki_supported(d), "shape too large for the split-precision GEMM");
+    uw12b::gemm_ozaki(d, n_moduli);
+    if (uw12b::ozaki_error_read_and_clear())
+      throw uw12b::Error(uw12b::kErrCuda,
+                         "split-precision GEMM: a tensor-core pipeline wait timed out");
+  });
+}
+
+int uw12c_set_split_threshold(double min_flops) {
+  return guarded([&] { uw12b::set_split_min_flops(min_flops); });
+}
+
+int uw12c_split_bits(int n_moduli, long long k_total, int* bits) {
+  return guarded([&] {
+    need(n_moduli >= 1 && n_moduli <= uw12b::kOzakiMaxModuli && k_total >= 1 && bits,
+         "n_moduli must be 1..16, k_total >= 1");
+    *bits = uw12b::ozaki_bits(n_moduli, k_total);
+  });
+}
+
+int uw12c_profile_read_kind(int kind, unsigned long long* launches, double* ms, double* work) {
+  return guarded([&] {
+    need(kind >= 0 && kind < uw12b::kProfKinds, "unknown kernel class");
+    const uw12b::KernelStats k = uw12b::profile_read_kind(kind);
+    if (launches) *launches = k.launches;
+    if (ms) *ms = k.ms;
+    if (work) *work = k.flops;
   });
 }
 

@@ -10,6 +10,7 @@
 #include <string>
 
 #include "gemm_f64.cuh"
+#include "ozaki.cuh"
 
 namespace uw12b {
 
@@ -479,20 +480,22 @@ struct ProfRec {
   cudaEvent_t a, b;
   double flops;
   std::string shape;  // "m n k nbo nbr split layout vec" for the per-launch log
+  int kind;
 };
 std::mutex g_prof_mu;
 bool g_prof_on = false;
 std::vector<ProfRec> g_prof_recs;
-KernelStats g_prof_acc;
+KernelStats g_prof_acc[kProfKinds];
 
 void prof_collect_locked() {
   for (auto& r : g_prof_recs) {
     UW12_CUDA(cudaEventSynchronize(r.b));
     float ms = 0.f;
     UW12_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
-    g_prof_acc.launches += 1;
-    g_prof_acc.ms += ms;
-    g_prof_acc.flops += r.flops;
+    KernelStats& acc = g_prof_acc[r.kind];
+    acc.launches += 1;
+    acc.ms += ms;
+    acc.flops += r.flops;
     if (const char* path = std::getenv("UW12_PROFILE_LOG")) {
       if (FILE* f = std::fopen(path, "a")) {
         std::fprintf(f, "%.4f %s\n", ms, r.shape.c_str());
@@ -520,16 +523,36 @@ bool profile_enabled() {
 void profile_reset() {
   std::lock_guard<std::mutex> lk(g_prof_mu);
   prof_collect_locked();
-  g_prof_acc = KernelStats{};
+  for (auto& a : g_prof_acc) a = KernelStats{};
 }
 
-KernelStats profile_read_gemm() {
+KernelStats profile_read_gemm() { return profile_read_kind(kProfDgemm); }
+
+KernelStats profile_read_kind(int kind) {
   std::lock_guard<std::mutex> lk(g_prof_mu);
   prof_collect_locked();
-  return g_prof_acc;
+  return g_prof_acc[kind];
+}
+
+void profile_record(int kind, cudaEvent_t a, cudaEvent_t b, double work, std::string shape) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof_recs.push_back({a, b, work, std::move(shape), kind});
 }
 
 void gemm(const GemmDesc& d) {
+  const int L = split_moduli();
+  if (L > 0) {
+    const double flops = 2.0 * double(d.m) * double(d.n) * double(d.k) * double(d.nbo1) *
+                         double(d.nbo2) * double(d.nbr1) * double(d.nbr2);
+    if (flops >= split_min_flops() && ozaki_supported(d)) {
+      gemm_ozaki(d, L);
+      return;
+    }
+  }
+  gemm_dmma(d);
+}
+
+void gemm_dmma(const GemmDesc& d) {
   KParams p;
   bool empty_k = false;
   if (!prepare(d, p, &empty_k)) return;
@@ -561,7 +584,7 @@ void gemm(const GemmDesc& d) {
                   int(vec_ok(d.B, d.ldb, d.sBo1, d.sBo2, d.sBr1, d.sBr2)));
     g_prof_recs.push_back({ev_a, ev_b, 2.0 * double(d.m) * double(d.n) * double(d.k) *
                                            double(p.nbo) * double(d.nbr1 * d.nbr2),
-                           shape});
+                           shape, kProfDgemm});
   }
 }
 

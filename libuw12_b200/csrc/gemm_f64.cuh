@@ -16,6 +16,7 @@
 #pragma once
 
 #include "common.cuh"
+#include <string>
 
 namespace uw12b {
 
@@ -43,8 +44,12 @@ struct GemmDesc {
 };
 
 // Launches on current_stream().  Zero-sized problems are no-ops (k == 0 or
-// no reduction batches scales C by beta).
+// no reduction batches scales C by beta).  While split precision is selected
+// on this host thread (set_split_moduli), GEMMs of at least kOzakiMinFlops
+// run as split-precision int8 tensor-core GEMMs (ozaki.cuh); gemm_dmma always
+// runs the FP64 DMMA kernel.
 void gemm(const GemmDesc& d);
+void gemm_dmma(const GemmDesc& d);
 
 // Same contraction without any device allocation: split-K partial tiles go
 // to a fixed per-device array of kNoAllocScratchDoubles doubles (16 MiB).  An
@@ -76,5 +81,13 @@ void profile_enable(bool on);
 bool profile_enabled();
 KernelStats profile_read_gemm();  // synchronises the recorded events
 void profile_reset();
+// Kernel classes: the FP64 DMMA GEMM; whole split-precision GEMMs (work =
+// FP64-equivalent 2mnk FLOPs); their int8 tcgen05 product kernel (work = int8
+// operations 2 m n K per modulus); their operand preparation and CRT
+// reconstruction kernels (work = algorithmic bytes read + written).
+enum { kProfDgemm = 0, kProfSplitGemm, kProfI8Mma, kProfSplitPrep, kProfSplitCrt, kProfKinds };
+KernelStats profile_read_kind(int kind);
+// Adds one timed launch (the events are destroyed once read).
+void profile_record(int kind, cudaEvent_t a, cudaEvent_t b, double work, std::string shape);
 
 }  // namespace uw12b

@@ -1,0 +1,976 @@
+// Split-precision FP64 GEMM: int8 residue products on the tcgen05 tensor
+// cores, recombined by the Chinese remainder theorem (see ozaki.cuh).
+//
+// Kernels per GEMM (slab):
+//   k_row_exponent per row of A / column of B: the binary exponent of its
+//                 largest element; rows are scaled by 2^(beta - exponent) so
+//                 that every element is below 2^beta in magnitude;
+//   k_residues    FP64 -> rint(x 2^shift) -> L int8 residue planes, K-major
+//                 (row r of plane (l, p) is K_pad contiguous bytes);
+//   k_i8_mma      one CTA = one 128 x 256 output tile of one modulus and one
+//                 K chunk: TMA (128-byte swizzled boxes) -> shared memory ->
+//                 tcgen05.mma.kind::i8 with the int32 accumulator in TMEM ->
+//                 tcgen05.ld -> residue mod p -> uint8 plane in HBM.
+//                 Warp roles: 0 TMA producer, 1 TMEM owner + MMA issuer,
+//                 2..5 epilogue (TMEM lane quarter = warp % 4);
+//   k_crt         per output element: sum the K-chunk residues mod p, CRT on
+//                 36-bit chunks in FP64 (exact integer arithmetic; the value is
+//                 rounded only when the chunks are joined, <= 2^-52 relative),
+//                 scale by 2^-(sa+sb), apply alpha / beta, store FP64.
+// The MMA's M side (TMEM lanes) runs over the output column j (B's n index)
+// and its N side over the output row i (A's m index), so that one thread of
+// the epilogue owns 256 consecutive i of one column j and the residue planes
+// and C are both i-contiguous.
+#include <cuda.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+#include "ozaki.cuh"
+
+namespace uw12b {
+
+namespace {
+
+// Pairwise-coprime moduli <= 256 (residues fit int8: [-128, 127]).
+constexpr uint32_t kModuli[kOzakiMaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233,
+                                               229, 227, 223, 217, 211, 199, 197, 193};
+constexpr int kChunkBits = 36;  // CRT weight chunks: r_l * chunk < 2^44, sums < 2^49
+constexpr int kMaxChunks = 4;   // 144 bits >= log2(M) for 16 moduli (~125.3)
+constexpr long long kMaxKChunk = 65536;  // |acc| <= 65536 * 128^2 = 2^30 per split
+
+struct Consts {
+  int L = 0, nch = 0, beta = 0;
+  uint32_t p[kOzakiMaxModuli];
+  uint32_t barrett[kOzakiMaxModuli];  // floor(2^32 / p)
+  uint32_t off[kOzakiMaxModuli];      // multiple of p, >= 2^30
+  double pd[kOzakiMaxModuli], inv_p[kOzakiMaxModuli];
+  double w[kOzakiMaxModuli][kMaxChunks];  // chunks of (M/p_l) * ((M/p_l)^-1 mod p_l) mod M
+  double mc[kMaxChunks];                  // chunks of M
+  double inv_m;
+  double log2_m;
+};
+
+using u128 = unsigned __int128;
+
+long long inv_mod(long long a, long long p) {
+  long long t = 0, nt = 1, r = p, nr = a % p;
+  while (nr) {
+    const long long q = r / nr;
+    std::swap(t, nt); nt -= q * t;
+    std::swap(r, nr); nr -= q * r;
+  }
+  if (r != 1) throw Error(kErrInvalid, "split-precision moduli are not coprime");
+  return t < 0 ? t + p : t;
+}
+
+Consts make_consts(int L) {
+  Consts c;
+  c.L = L;
+  u128 M = 1;
+  c.log2_m = 0.0;
+  for (int l = 0; l < L; ++l) {
+    const uint32_t p = kModuli[l];
+    M *= p;
+    c.log2_m += std::log2(double(p));
+    c.p[l] = p;
+    c.barrett[l] = static_cast<uint32_t>((1ULL << 32) / p);
+    c.off[l] = static_cast<uint32_t>(((1ULL << 30) + p - 1) / p * p);
+    c.pd[l] = double(p);
+    c.inv_p[l] = 1.0 / double(p);
+  }
+  int bits = 0;
+  for (u128 t = M; t; t >>= 1) ++bits;
+  c.nch = (bits + kChunkBits - 1) / kChunkBits;
+  const u128 mask = (u128(1) << kChunkBits) - 1;
+  for (int l = 0; l < L; ++l) {
+    const u128 Ml = M / kModuli[l];
+    const long long y = inv_mod(static_cast<long long>(Ml % kModuli[l]), kModuli[l]);
+    const u128 w = Ml * u128(y);  // < M: Ml * y < Ml * p_l
+    for (int ch = 0; ch < kMaxChunks; ++ch)
+      c.w[l][ch] = ch < c.nch ? double(static_cast<uint64_t>((w >> (kChunkBits * ch)) & mask))
+                              : 0.0;
+  }
+  for (int ch = 0; ch < kMaxChunks; ++ch)
+    c.mc[ch] = ch < c.nch ? double(static_cast<uint64_t>((M >> (kChunkBits * ch)) & mask)) : 0.0;
+  c.inv_m = 1.0 / static_cast<double>(M);
+  return c;
+}
+
+const Consts& consts_for(int L) {
+  static std::once_flag once[kOzakiMaxModuli + 1];
+  static Consts table[kOzakiMaxModuli + 1];
+  std::call_once(once[L], [&] { table[L] = make_consts(L); });
+  return table[L];
+}
+
+thread_local int g_split_moduli = 0;
+thread_local double g_split_min_flops = kOzakiMinFlops;
+
+// device error flag (pipeline wait timed out), one per device
+std::mutex g_err_mu;
+int* g_err_ptr[64] = {};
+
+int* err_flag() {
+  int dev = 0;
+  UW12_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  if (!g_err_ptr[dev]) {
+    UW12_CUDA(cudaMalloc(reinterpret_cast<void**>(&g_err_ptr[dev]), sizeof(int)));
+    UW12_CUDA(cudaMemset(g_err_ptr[dev], 0, sizeof(int)));
+  }
+  return g_err_ptr[dev];
+}
+
+// ---------------------------------------------------------------------------
+// operand preparation
+// ---------------------------------------------------------------------------
+// Operand rows: element (row, kt) of plane (p1, p2), kt = kk + k * (r1 + nbr1 r2),
+// lives at base + p1*po1 + p2*po2 + row*rs + kk*ks + r1*sr1 + r2*sr2.
+struct OperandView {
+  const double* base;
+  long long rows, k, k_total;
+  long long rs, ks, sr1, sr2, nbr1;
+  long long po1, po2;
+  int np1, np2;
+};
+
+// Offsets (kk*ks + r1*sr1 + r2*sr2) of the 128 k of the tile starting at k0
+// (-1 beyond k_total), one division per k.
+__device__ __forceinline__ void tile_k_offsets(const OperandView& v, long long k0,
+                                               long long* koff) {
+  if (threadIdx.x < 128) {
+    const long long kt = k0 + threadIdx.x;
+    long long off = -1;
+    if (kt < v.k_total) {
+      const long long r = kt / v.k, kk = kt - r * v.k;
+      off = kk * v.ks + (r % v.nbr1) * v.sr1 + (r / v.nbr1) * v.sr2;
+    }
+    koff[threadIdx.x] = off;
+  }
+}
+
+// Loads the 32 x 128 tile (rows row0.., k k0..) of one plane, zeros outside,
+// reading along whichever of rows / k is contiguous in memory.
+template <bool KCONTIG>
+__device__ __forceinline__ void load_tile(const OperandView& v, int plane, long long row0,
+                                          const long long* koff, double (*tile)[129]) {
+  const double* pb = v.base + (plane % v.np1) * v.po1 + (plane / v.np1) * v.po2;
+  for (int e = threadIdx.x; e < 32 * 128; e += 256) {
+    const int r = KCONTIG ? (e >> 7) : (e & 31);
+    const int c = KCONTIG ? (e & 127) : (e >> 5);
+    const long long row = row0 + r;
+    const long long ko = koff[c];
+    tile[r][c] = (row < v.rows && ko >= 0) ? pb[row * v.rs + ko] : 0.0;
+  }
+}
+
+// Per row: exponent e of its largest element (2^(e-1) <= max|x| < 2^e),
+// stored as e + 2048 through atomicMax (0 = all zeros).  Grid: (row tiles,
+// k tiles, planes).
+template <bool KCONTIG>
+__global__ void __launch_bounds__(256) k_row_exponent(OperandView v,
+                                                      unsigned* __restrict__ eplus) {
+  __shared__ double tile[32][129];
+  __shared__ long long koff[128];
+  const int plane = blockIdx.z;
+  const long long row0 = static_cast<long long>(blockIdx.x) * 32;
+  tile_k_offsets(v, static_cast<long long>(blockIdx.y) * 128, koff);
+  __syncthreads();
+  load_tile<KCONTIG>(v, plane, row0, koff, tile);
+  __syncthreads();
+  // 8 warps x 4 rows: each warp reduces its rows across the 32 lanes
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  for (int rr = 0; rr < 4; ++rr) {
+    const int r = warp * 4 + rr;
+    double mx = fmax(fmax(fabs(tile[r][lane]), fabs(tile[r][lane + 32])),
+                     fmax(fabs(tile[r][lane + 64]), fabs(tile[r][lane + 96])));
+    for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const long long row = row0 + r;
+    if (lane == 0 && row < v.rows && mx > 0.0) {
+      int e = 0;
+      frexp(mx, &e);
+      atomicMax(&eplus[plane * v.rows + row], static_cast<unsigned>(e + 2048));
+    }
+  }
+}
+
+// shift = beta - e (0 for an all-zero row).
+__global__ void k_exponent_to_shift(const unsigned* __restrict__ eplus, long long n, int beta,
+                                    int* __restrict__ shift) {
+  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t < n) shift[t] = eplus[t] ? beta - (static_cast<int>(eplus[t]) - 2048) : 0;
+}
+
+struct ResidueMods {
+  int L;
+  double pd[kOzakiMaxModuli], inv_p[kOzakiMaxModuli];
+};
+
+__device__ __forceinline__ uint32_t residue_byte(double v, double p, double inv_p) {
+  const double q = rint(v * inv_p);
+  double r = fma(-q, p, v);  // exact: an integer of magnitude <= p/2 + 1
+  if (r > 127.0) r -= p;
+  if (r < -128.0) r += p;
+  return static_cast<uint32_t>(static_cast<int>(r)) & 0xffu;
+}
+
+// Tile of 32 rows x 128 k of one plane -> L residue planes.
+// out[((l * planes + plane) * rows_pad + row) * k_pad + kt], zeros in padding.
+// Grid: (row tiles, k tiles, planes).
+template <bool KCONTIG>
+__global__ void __launch_bounds__(256) k_residues(OperandView v, const int* __restrict__ shift,
+                                                  ResidueMods mods, int planes,
+                                                  long long rows_pad, long long k_pad,
+                                                  uint8_t* __restrict__ out) {
+  __shared__ double tile[32][129];
+  __shared__ long long koff[128];
+  const int plane = blockIdx.z;
+  const long long row0 = static_cast<long long>(blockIdx.x) * 32;
+  const long long k0 = static_cast<long long>(blockIdx.y) * 128;
+  tile_k_offsets(v, k0, koff);
+  __syncthreads();
+  load_tile<KCONTIG>(v, plane, row0, koff, tile);
+  __syncthreads();
+  const int tid = threadIdx.x;
+  const int c4 = (tid & 31) * 4;
+  for (int it = 0; it < 4; ++it) {
+    const int r = it * 8 + tid / 32;
+    const long long row = row0 + r;
+    const int sh = row < v.rows ? shift[plane * v.rows + row] : 0;
+    const double x0 = rint(ldexp(tile[r][c4], sh)), x1 = rint(ldexp(tile[r][c4 + 1], sh)),
+                 x2 = rint(ldexp(tile[r][c4 + 2], sh)), x3 = rint(ldexp(tile[r][c4 + 3], sh));
+    for (int l = 0; l < mods.L; ++l) {
+      const double p = mods.pd[l], ip = mods.inv_p[l];
+      const uint32_t word = residue_byte(x0, p, ip) | (residue_byte(x1, p, ip) << 8) |
+                            (residue_byte(x2, p, ip) << 16) | (residue_byte(x3, p, ip) << 24);
+      uint8_t* dst =
+          out + ((static_cast<long long>(l) * planes + plane) * rows_pad + row) * k_pad + k0 + c4;
+      *reinterpret_cast<uint32_t*>(dst) = word;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tcgen05 int8 product kernel
+// ---------------------------------------------------------------------------
+constexpr int kTileJ = 128;  // MMA M (TMEM lanes): output columns j
+constexpr int kTileI = 256;  // MMA N (TMEM columns): output rows i
+constexpr int kTileK = 128;  // bytes of K per pipeline stage (one 128-byte swizzle row)
+constexpr int kBytesJ = kTileJ * kTileK;  // 16 KiB
+constexpr int kBytesI = kTileI * kTileK;  // 32 KiB
+constexpr int kMmaK = 32;                 // K of one kind::i8 MMA
+constexpr int kThreads = 192;
+constexpr unsigned long long kWaitLimitNs = 4000000000ULL;  // 4 s
+
+struct MmaArgs {
+  int tiles_j, L, splits, nbatch, nbo1;
+  int a_var1, a_var2, b_var1, b_var2;  // operand planes vary with bo1 / bo2
+  int planes_a, planes_b;
+  long long m_pad, n_pad;
+  int kb_per_split, kb_total;
+  uint32_t p[kOzakiMaxModuli], barrett[kOzakiMaxModuli], off[kOzakiMaxModuli];
+  uint8_t* R;
+  int* err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the phase of the given parity to complete.  Gives up
+// (returns false, sets the CTA's abort flag and the device error flag) after
+// kWaitLimitNs, or when another role of the CTA has aborted.
+__device__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err,
+                          int code) {
+  if (mbar_test(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (unsigned it = 1;; ++it) {
+    if (mbar_test(bar, parity)) return true;
+    if ((it & 255u) == 0) {
+      if (*abort_flag) return false;
+      if (global_ns() - t0 > kWaitLimitNs) {
+        *abort_flag = 1;
+        atomicExch(err, code);
+        return false;
+      }
+    }
+  }
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                            uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row core
+// groups 1024 bytes apart (stride byte offset), version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+  return static_cast<uint64_t>((addr >> 4) & 0x3fffu) | (1ull << 16) |
+         (static_cast<uint64_t>(1024 >> 4) << 32) | (1ull << 46) | (2ull << 61);
+}
+// Instruction descriptor of kind::i8: s32 accumulator, signed int8 A and B,
+// both K-major, N = kTileI, M = kTileJ.
+constexpr uint32_t kIdesc = (2u << 4) | (1u << 7) | (1u << 10) |
+                            (static_cast<uint32_t>(kTileI >> 3) << 17) |
+                            (static_cast<uint32_t>(kTileJ >> 4) << 24);
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(
+          tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   bar)
+               : "memory");
+}
+
+#define UW12_TMEM_LD32(taddr, v)                                                               \
+  asm volatile(                                                                                \
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "  \
+      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "  \
+      "%28, %29, %30, %31}, [%32];"                                                            \
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),    \
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),             \
+        "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),          \
+        "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),          \
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),          \
+        "=r"(v[31])                                                                            \
+      : "r"(taddr))
+
+__device__ __forceinline__ uint32_t mod_u32(uint32_t u, uint32_t p, uint32_t barrett) {
+  uint32_t r = u - __umulhi(u, barrett) * p;
+  return r >= p ? r - p : r;
+}
+
+template <int STAGES>
+__global__ void __launch_bounds__(kThreads, 2)
+    k_i8_mma(const __grid_constant__ CUtensorMap tm_j, const __grid_constant__ CUtensorMap tm_i,
+             const MmaArgs a) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                             ~static_cast<uintptr_t>(1023));
+  uint8_t* sj = base;                            // STAGES x 16 KiB
+  uint8_t* si = base + STAGES * kBytesJ;         // STAGES x 32 KiB
+  uint64_t* bars = reinterpret_cast<uint64_t*>(si + STAGES * kBytesI);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + STAGES;
+  uint64_t* acc_full = bars + 2 * STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int tj = blockIdx.x % a.tiles_j, ti = blockIdx.x / a.tiles_j;
+  const int l = blockIdx.y;
+  const int split = blockIdx.z % a.splits, b = blockIdx.z / a.splits;
+  const int b1 = b % a.nbo1, b2 = b / a.nbo1;
+  const int pa = (a.a_var1 ? b1 : 0) + (a.a_var1 ? a.nbo1 : 1) * (a.a_var2 ? b2 : 0);
+  const int pb = (a.b_var1 ? b1 : 0) + (a.b_var1 ? a.nbo1 : 1) * (a.b_var2 ? b2 : 0);
+  const int kb0 = split * a.kb_per_split;
+  const int nkb = min(a.kb_per_split, a.kb_total - kb0);
+  const int yj = static_cast<int>((static_cast<long long>(l) * a.planes_b + pb) * a.n_pad +
+                                  static_cast<long long>(tj) * kTileJ);
+  const int yi = static_cast<int>((static_cast<long long>(l) * a.planes_a + pa) * a.m_pad +
+                                  static_cast<long long>(ti) * kTileI);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&empty[s]), 1);
+    }
+    mbar_init(smem_u32(acc_full), 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(static_cast<uint32_t>(kTileI))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer
+    int issued = 0;
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int s = kb % STAGES;
+      const uint32_t ph = (kb / STAGES) & 1;
+      if (!mbar_wait(smem_u32(&empty[s]), ph ^ 1, abort_flag, a.err, 1)) break;
+      const uint32_t fb = smem_u32(&full[s]);
+      mbar_expect_tx(fb, kBytesJ + kBytesI);
+      const int x = (kb0 + kb) * kTileK;
+      tma_load_2d(smem_u32(sj + s * kBytesJ), &tm_j, x, yj, fb);
+      tma_load_2d(smem_u32(si + s * kBytesI), &tm_i, x, yi, fb);
+      ++issued;
+    }
+    if (*abort_flag) {
+      // let the copies already issued land before the CTA exits
+      for (int kb = max(0, issued - STAGES); kb < issued; ++kb)
+        (void)mbar_wait(smem_u32(&full[kb % STAGES]), (kb / STAGES) & 1, abort_flag, a.err, 1);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int s = kb % STAGES;
+      const uint32_t ph = (kb / STAGES) & 1;
+      if (!mbar_wait(smem_u32(&full[s]), ph, abort_flag, a.err, 2)) break;
+      tc_fence_after();
+      const uint64_t dj = sw128_desc(smem_u32(sj + s * kBytesJ));
+      const uint64_t di = sw128_desc(smem_u32(si + s * kBytesI));
+#pragma unroll
+      for (int kk = 0; kk < kTileK / kMmaK; ++kk) {
+        // advance along K inside the swizzle row: +32 bytes = +2 in the
+        // 16-byte address field
+        mma_i8(tmem, dj + 2 * kk, di + 2 * kk, (kb | kk) != 0);
+      }
+      mma_commit(smem_u32(&empty[s]));
+    }
+    mma_commit(smem_u32(acc_full));
+  } else if (warp >= 2) {
+    // ---- epilogue: TMEM -> residues mod p -> uint8 plane
+    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    // warp-uniform, so that the .sync.aligned TMEM loads below are convergent
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(acc_full), 0, abort_flag, a.err, 3));
+    tc_fence_after();
+    if (ok && nkb > 0) {
+      const uint32_t p = a.p[l], bm = a.barrett[l], off = a.off[l];
+      const long long j = static_cast<long long>(tj) * kTileJ + q * 32 + lane;
+      uint8_t* rowp =
+          a.R + ((static_cast<long long>(split) * a.L + l) * a.nbatch + b) * a.n_pad * a.m_pad +
+          j * a.m_pad + static_cast<long long>(ti) * kTileI;
+#pragma unroll 1
+      for (int c = 0; c < kTileI / 32; ++c) {
+        uint32_t v[32];
+        UW12_TMEM_LD32(tmem + (static_cast<uint32_t>(q * 32) << 16) + c * 32, v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        uint32_t w[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          uint32_t word = 0;
+#pragma unroll
+          for (int t = 0; t < 4; ++t)
+            word |= mod_u32(v[4 * e + t] + off, p, bm) << (8 * t);
+          w[e] = word;
+        }
+        uint4* dst = reinterpret_cast<uint4*>(rowp + c * 32);
+        dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+        dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+      }
+    } else if (nkb == 0) {
+      // empty K chunk: residue 0
+      const long long j = static_cast<long long>(tj) * kTileJ + q * 32 + lane;
+      uint4* dst = reinterpret_cast<uint4*>(
+          a.R + ((static_cast<long long>(split) * a.L + l) * a.nbatch + b) * a.n_pad * a.m_pad +
+          j * a.m_pad + static_cast<long long>(ti) * kTileI);
+      for (int c = 0; c < kTileI / 16; ++c) dst[c] = make_uint4(0, 0, 0, 0);
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    if (lane == 0) {
+      // all MMAs of this CTA have completed before TMEM is released
+      (void)mbar_wait(smem_u32(acc_full), 0, abort_flag, a.err, 4);
+    }
+    __syncwarp();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(static_cast<uint32_t>(kTileI))
+                 : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CRT reconstruction
+// ---------------------------------------------------------------------------
+struct CrtArgs {
+  const uint8_t* R;
+  long long m, n, m_pad, n_pad;
+  int splits, L, nch, nbatch, nbo1;
+  const int* shift_a;
+  const int* shift_b;
+  int a_var1, a_var2, b_var1, b_var2;
+  long long rows_a, rows_b;  // rows per shift plane (m, n)
+  double* C;
+  long long ldc, sCo1, sCo2;
+  double alpha, beta;
+  uint32_t p[kOzakiMaxModuli], barrett[kOzakiMaxModuli];
+  double w[kOzakiMaxModuli][kMaxChunks];
+  double mc[kMaxChunks];
+  double inv_m;
+};
+
+// One thread = 4 consecutive rows i of one column j of one batch.
+__global__ void __launch_bounds__(256) k_crt(const CrtArgs a, long long i4_count) {
+  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const long long per_b = i4_count * a.n;
+  if (t >= per_b * a.nbatch) return;
+  const int b = static_cast<int>(t / per_b);
+  const long long rem = t - b * per_b;
+  const long long j = rem / i4_count;
+  const long long i0 = (rem - j * i4_count) * 4;
+  const int b1 = b % a.nbo1, b2 = b / a.nbo1;
+  const int pa = (a.a_var1 ? b1 : 0) + (a.a_var1 ? a.nbo1 : 1) * (a.a_var2 ? b2 : 0);
+  const int pb = (a.b_var1 ? b1 : 0) + (a.b_var1 ? a.nbo1 : 1) * (a.b_var2 ? b2 : 0);
+
+  double S[4][kMaxChunks];
+#pragma unroll
+  for (int e = 0; e < 4; ++e)
+#pragma unroll
+    for (int c = 0; c < kMaxChunks; ++c) S[e][c] = 0.0;
+  const long long plane = a.n_pad * a.m_pad;
+  const long long pos = j * a.m_pad + i0;
+  for (int l = 0; l < a.L; ++l) {
+    uint32_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (int sp = 0; sp < a.splits; ++sp) {
+      const uint32_t word = *reinterpret_cast<const uint32_t*>(
+          a.R + ((static_cast<long long>(sp) * a.L + l) * a.nbatch + b) * plane + pos);
+      s0 += word & 0xffu;
+      s1 += (word >> 8) & 0xffu;
+      s2 += (word >> 16) & 0xffu;
+      s3 += word >> 24;
+    }
+    const uint32_t p = a.p[l], bm = a.barrett[l];
+    const double r[4] = {double(mod_u32(s0, p, bm)), double(mod_u32(s1, p, bm)),
+                         double(mod_u32(s2, p, bm)), double(mod_u32(s3, p, bm))};
+#pragma unroll
+    for (int c = 0; c < kMaxChunks; ++c) {
+      const double wc = a.w[l][c];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) S[e][c] = fma(r[e], wc, S[e][c]);
+    }
+  }
+  const int sb = a.shift_b[pb * a.rows_b + j];
+  double* Cb = a.C + b1 * a.sCo1 + b2 * a.sCo2 + j * a.ldc;
+  constexpr double kChunk = 68719476736.0;  // 2^36
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const long long i = i0 + e;
+    if (i >= a.m) break;
+    // chunks above nch are zero, so running over all kMaxChunks is exact
+    double approx = 0.0;
+#pragma unroll
+    for (int c = kMaxChunks - 1; c >= 0; --c) approx = fma(approx, kChunk, S[e][c]);
+    const double q = rint(approx * a.inv_m);
+    double v = 0.0;
+#pragma unroll
+    for (int c = kMaxChunks - 1; c >= 0; --c) v = fma(v, kChunk, fma(-q, a.mc[c], S[e][c]));
+    const int sa = a.shift_a[pa * a.rows_a + i];
+    double out = a.alpha * ldexp(v, -(sa + sb));
+    if (a.beta != 0.0) out = fma(a.beta, Cb[i], out);
+    Cb[i] = out;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+  static std::once_flag once;
+  static EncodeTiled fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  });
+  if (!fn) throw Error(kErrCuda, "cuTensorMapEncodeTiled is not available");
+  return fn;
+}
+
+// 2-D uint8 map over rows x k_pad bytes, box = box_rows x 128 bytes, 128-byte swizzle.
+CUtensorMap make_map(const uint8_t* base, long long rows, long long k_pad, int box_rows) {
+  CUtensorMap m;
+  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(k_pad), static_cast<cuuint64_t>(rows)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(k_pad)};
+  const cuuint32_t box[2] = {static_cast<cuuint32_t>(kTileK), static_cast<cuuint32_t>(box_rows)};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(base),
+                                 dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    throw Error(kErrCuda, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+  return m;
+}
+
+constexpr int kStages = 2;  // 2 CTAs per SM (96 KiB of stages each, 2 x 256 TMEM columns)
+constexpr size_t kMmaSmem =
+    size_t(kStages) * (kBytesJ + kBytesI) + 1024 /*alignment*/ + 256 /*barriers*/;
+
+long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
+
+struct Timer {
+  int kind;
+  double work;
+  std::string shape;
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaStream_t s;
+  Timer(int kind_, double work_, std::string shape_, cudaStream_t s_)
+      : kind(kind_), work(work_), shape(std::move(shape_)), s(s_) {
+    if (!profile_enabled()) return;
+    UW12_CUDA(cudaEventCreate(&a));
+    UW12_CUDA(cudaEventCreate(&b));
+    UW12_CUDA(cudaEventRecord(a, s));
+  }
+  void stop() {
+    if (!a) return;
+    UW12_CUDA(cudaEventRecord(b, s));
+    profile_record(kind, a, b, work, shape);
+    a = b = nullptr;
+  }
+};
+
+// Runs one GEMM whose temporaries fit.  d.nbo2 == 1 or both batch dims are
+// handled through the plane maps.
+void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
+  const int L = cs.L;
+  const long long nbo1 = d.nbo1, nbo2 = d.nbo2, nbatch = nbo1 * nbo2;
+  const long long k_total = d.k * d.nbr1 * d.nbr2;
+  const long long k_pad = round_up(k_total, kTileK);
+  const long long m_pad = round_up(d.m, kTileI), n_pad = round_up(d.n, kTileJ);
+  const int a_var1 = d.sAo1 != 0 && nbo1 > 1, a_var2 = d.sAo2 != 0 && nbo2 > 1;
+  const int b_var1 = d.sBo1 != 0 && nbo1 > 1, b_var2 = d.sBo2 != 0 && nbo2 > 1;
+  const int pa1 = a_var1 ? int(nbo1) : 1, pa2 = a_var2 ? int(nbo2) : 1;
+  const int pb1 = b_var1 ? int(nbo1) : 1, pb2 = b_var2 ? int(nbo2) : 1;
+  const long long planes_a = pa1 * pa2, planes_b = pb1 * pb2;
+
+  // K chunks: <= kMaxKChunk bytes each; more chunks when the tile grid alone
+  // would leave SMs idle.
+  const long long kb_total = k_pad / kTileK;
+  const long long tiles_j = n_pad / kTileJ, tiles_i = m_pad / kTileI;
+  const long long ctas = tiles_j * tiles_i * L * nbatch;
+  long long splits = (k_pad + kMaxKChunk - 1) / kMaxKChunk;
+  const long long want = (2 * 148 * 2 + ctas - 1) / ctas;
+  splits = std::max(splits, std::min(want, std::max<long long>(1, kb_total / 8)));
+  splits = std::min(splits, std::max<long long>(1, 65535 / nbatch));
+  long long kb_per = (kb_total + splits - 1) / splits;
+  kb_per = std::min<long long>(kb_per, kMaxKChunk / kTileK);
+  splits = (kb_total + kb_per - 1) / kb_per;
+  if (splits * nbatch > 65535) throw Error(kErrInvalid, "split-precision GEMM: too many batches");
+
+  DevBuf resA((L * planes_a * m_pad * k_pad + 7) / 8, s);
+  DevBuf resB((L * planes_b * n_pad * k_pad + 7) / 8, s);
+  DevBuf shA((planes_a * d.m + 1) / 2, s), shB((planes_b * d.n + 1) / 2, s);
+  DevBuf exA((planes_a * d.m + 1) / 2, s), exB((planes_b * d.n + 1) / 2, s);
+  unsigned* ea = reinterpret_cast<unsigned*>(exA.get());
+  unsigned* eb = reinterpret_cast<unsigned*>(exB.get());
+  DevBuf R((splits * L * nbatch * n_pad * m_pad + 7) / 8, s);
+  uint8_t* ra = reinterpret_cast<uint8_t*>(resA.get());
+  uint8_t* rb = reinterpret_cast<uint8_t*>(resB.get());
+  int* sa = reinterpret_cast<int*>(shA.get());
+  int* sb = reinterpret_cast<int*>(shB.get());
+
+  // ---- operand views: A rows = i (m), B rows = j (n)
+  OperandView va{d.A, d.m, d.k, k_total,
+                 d.a_kcontig ? d.lda : 1, d.a_kcontig ? 1 : d.lda, d.sAr1, d.sAr2, d.nbr1,
+                 d.sAo1, d.sAo2, pa1, pa2};
+  OperandView vb{d.B, d.n, d.k, k_total,
+                 d.b_ncontig ? 1 : d.ldb, d.b_ncontig ? d.ldb : 1, d.sBr1, d.sBr2, d.nbr1,
+                 d.sBo1, d.sBo2, pb1, pb2};
+  ResidueMods mods;
+  mods.L = L;
+  for (int l = 0; l < L; ++l) {
+    mods.pd[l] = cs.pd[l];
+    mods.inv_p[l] = cs.inv_p[l];
+  }
+  {
+    const double bytes = 8.0 * double(planes_a * d.m + planes_b * d.n) * double(k_total) * 2.0 +
+                         double(L) * double(planes_a * m_pad + planes_b * n_pad) * double(k_pad);
+    Timer tm(kProfSplitPrep, bytes, "prep", s);
+    auto prep = [&](const OperandView& v, long long planes, long long rows_pad, int* sh,
+                    unsigned* ep, uint8_t* out) {
+      UW12_CUDA(cudaMemsetAsync(ep, 0, planes * v.rows * sizeof(unsigned), s));
+      dim3 g(static_cast<unsigned>(rows_pad / 32), static_cast<unsigned>(k_pad / 128),
+             static_cast<unsigned>(planes));
+      if (v.ks == 1)
+        k_row_exponent<true><<<g, 256, 0, s>>>(v, ep);
+      else
+        k_row_exponent<false><<<g, 256, 0, s>>>(v, ep);
+      UW12_LAUNCHED();
+      const long long nsh = planes * v.rows;
+      k_exponent_to_shift<<<static_cast<unsigned>((nsh + 255) / 256), 256, 0, s>>>(ep, nsh, beta,
+                                                                                  sh);
+      UW12_LAUNCHED();
+      if (v.ks == 1)
+        k_residues<true><<<g, 256, 0, s>>>(v, sh, mods, int(planes), rows_pad, k_pad, out);
+      else
+        k_residues<false><<<g, 256, 0, s>>>(v, sh, mods, int(planes), rows_pad, k_pad, out);
+      UW12_LAUNCHED();
+    };
+    prep(va, planes_a, m_pad, sa, ea, ra);
+    prep(vb, planes_b, n_pad, sb, eb, rb);
+    tm.stop();
+  }
+
+  // ---- int8 products
+  {
+    static std::mutex attr_mu;
+    static bool attr_set[64] = {};
+    {
+      int dev = 0;
+      UW12_CUDA(cudaGetDevice(&dev));
+      std::lock_guard<std::mutex> lk(attr_mu);
+      if (!attr_set[dev]) {
+        UW12_CUDA(cudaFuncSetAttribute(k_i8_mma<kStages>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(kMmaSmem)));
+        attr_set[dev] = true;
+      }
+    }
+    const CUtensorMap tmj = make_map(rb, L * planes_b * n_pad, k_pad, kTileJ);
+    const CUtensorMap tmi = make_map(ra, L * planes_a * m_pad, k_pad, kTileI);
+    MmaArgs ma{};
+    ma.tiles_j = static_cast<int>(tiles_j);
+    ma.L = L;
+    ma.splits = static_cast<int>(splits);
+    ma.nbatch = static_cast<int>(nbatch);
+    ma.nbo1 = static_cast<int>(nbo1);
+    ma.a_var1 = a_var1; ma.a_var2 = a_var2; ma.b_var1 = b_var1; ma.b_var2 = b_var2;
+    ma.planes_a = static_cast<int>(planes_a);
+    ma.planes_b = static_cast<int>(planes_b);
+    ma.m_pad = m_pad;
+    ma.n_pad = n_pad;
+    ma.kb_per_split = static_cast<int>(kb_per);
+    ma.kb_total = static_cast<int>(kb_total);
+    for (int l = 0; l < L; ++l) {
+      ma.p[l] = cs.p[l];
+      ma.barrett[l] = cs.barrett[l];
+      ma.off[l] = cs.off[l];
+    }
+    ma.R = reinterpret_cast<uint8_t*>(R.get());
+    ma.err = err_flag();
+    const double ops = 2.0 * double(d.m) * double(d.n) * double(k_total) * double(L) * nbatch;
+    char shape[160];
+    std::snprintf(shape, sizeof(shape), "i8 %lld %lld %lld %lld L%d s%lld", d.m, d.n, k_total,
+                  nbatch, L, splits);
+    Timer tm(kProfI8Mma, ops, shape, s);
+    dim3 grid(static_cast<unsigned>(tiles_j * tiles_i), static_cast<unsigned>(L),
+              static_cast<unsigned>(splits * nbatch));
+    k_i8_mma<kStages><<<grid, kThreads, kMmaSmem, s>>>(tmj, tmi, ma);
+    UW12_LAUNCHED();
+    tm.stop();
+  }
+
+  // ---- CRT reconstruction
+  {
+    CrtArgs ca{};
+    ca.R = reinterpret_cast<const uint8_t*>(R.get());
+    ca.m = d.m; ca.n = d.n; ca.m_pad = m_pad; ca.n_pad = n_pad;
+    ca.splits = static_cast<int>(splits);
+    ca.L = L;
+    ca.nch = cs.nch;
+    ca.nbatch = static_cast<int>(nbatch);
+    ca.nbo1 = static_cast<int>(nbo1);
+    ca.shift_a = sa; ca.shift_b = sb;
+    ca.a_var1 = a_var1; ca.a_var2 = a_var2; ca.b_var1 = b_var1; ca.b_var2 = b_var2;
+    ca.rows_a = d.m; ca.rows_b = d.n;
+    ca.C = d.C; ca.ldc = d.ldc; ca.sCo1 = d.sCo1; ca.sCo2 = d.sCo2;
+    ca.alpha = d.alpha; ca.beta = d.beta;
+    for (int l = 0; l < L; ++l) {
+      ca.p[l] = cs.p[l];
+      ca.barrett[l] = cs.barrett[l];
+      for (int c = 0; c < kMaxChunks; ++c) ca.w[l][c] = cs.w[l][c];
+    }
+    for (int c = 0; c < kMaxChunks; ++c) ca.mc[c] = cs.mc[c];
+    ca.inv_m = cs.inv_m;
+    const long long i4 = (d.m + 3) / 4;
+    const long long threads = i4 * d.n * nbatch;
+    const double bytes = double(splits * L) * double(d.m * d.n * nbatch) +
+                         8.0 * double(d.m * d.n * nbatch) * (d.beta != 0.0 ? 2.0 : 1.0);
+    Timer tm(kProfSplitCrt, bytes, "crt", s);
+    k_crt<<<static_cast<unsigned>((threads + 255) / 256), 256, 0, s>>>(ca, i4);
+    UW12_LAUNCHED();
+    tm.stop();
+  }
+}
+
+long long slab_bytes(long long L, long long m, long long n, long long k_total, long long nbatch,
+                     long long planes_a, long long planes_b) {
+  const long long k_pad = round_up(k_total, kTileK);
+  const long long m_pad = round_up(m, kTileI), n_pad = round_up(n, kTileJ);
+  const long long splits = std::max<long long>(1, (k_pad + kMaxKChunk - 1) / kMaxKChunk);
+  return L * (planes_a * m_pad + planes_b * n_pad) * k_pad +
+         std::max<long long>(splits, 4) * L * nbatch * m_pad * n_pad;
+}
+
+constexpr long long kSlabBudget = 8LL << 30;  // temporaries of one slab
+
+// Splits the GEMM into slabs (batches, then rows i / columns j) whose
+// temporaries stay within kSlabBudget, and runs each.
+void run_slabs(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
+  const long long L = cs.L;
+  const long long k_total = d.k * d.nbr1 * d.nbr2;
+  auto planes = [](long long var1n, long long var2n) { return var1n * var2n; };
+  // 1. batches: one bo2 at a time, then ranges of bo1
+  if (d.nbo2 > 1 &&
+      slab_bytes(L, d.m, d.n, k_total, d.nbo1 * d.nbo2,
+                 planes(d.sAo1 ? d.nbo1 : 1, d.sAo2 ? d.nbo2 : 1),
+                 planes(d.sBo1 ? d.nbo1 : 1, d.sBo2 ? d.nbo2 : 1)) > kSlabBudget) {
+    for (long long b2 = 0; b2 < d.nbo2; ++b2) {
+      GemmDesc e = d;
+      e.nbo2 = 1;
+      e.A += b2 * d.sAo2; e.B += b2 * d.sBo2; e.C += b2 * d.sCo2;
+      e.sAo2 = e.sBo2 = e.sCo2 = 0;
+      run_slabs(e, cs, beta, s);
+    }
+    return;
+  }
+  if (d.nbo1 > 1) {
+    long long nb = d.nbo1;
+    while (nb > 1 && slab_bytes(L, d.m, d.n, k_total, nb * d.nbo2, d.sAo1 ? nb : 1,
+                                d.sBo1 ? nb : 1) > kSlabBudget)
+      nb = (nb + 1) / 2;
+    if (nb < d.nbo1) {
+      for (long long b0 = 0; b0 < d.nbo1; b0 += nb) {
+        GemmDesc e = d;
+        e.nbo1 = std::min(nb, d.nbo1 - b0);
+        e.A += b0 * d.sAo1; e.B += b0 * d.sBo1; e.C += b0 * d.sCo1;
+        run_slabs(e, cs, beta, s);
+      }
+      return;
+    }
+  }
+  // 2. rows i / columns j
+  const long long nbatch = d.nbo1 * d.nbo2;
+  const long long pa = (d.sAo1 && d.nbo1 > 1 ? d.nbo1 : 1) * (d.sAo2 && d.nbo2 > 1 ? d.nbo2 : 1);
+  const long long pb = (d.sBo1 && d.nbo1 > 1 ? d.nbo1 : 1) * (d.sBo2 && d.nbo2 > 1 ? d.nbo2 : 1);
+  long long ms = round_up(d.m, kTileI), ns = round_up(d.n, kTileJ);
+  while (slab_bytes(L, ms, ns, k_total, nbatch, pa, pb) > kSlabBudget) {
+    if (ms >= ns && ms > kTileI)
+      ms = round_up(ms / 2, kTileI);
+    else if (ns > kTileJ)
+      ns = round_up(ns / 2, kTileJ);
+    else
+      break;
+  }
+  for (long long i0 = 0; i0 < d.m; i0 += ms)
+    for (long long j0 = 0; j0 < d.n; j0 += ns) {
+      GemmDesc e = d;
+      e.m = std::min(ms, d.m - i0);
+      e.n = std::min(ns, d.n - j0);
+      e.A += i0 * (d.a_kcontig ? d.lda : 1);
+      e.B += j0 * (d.b_ncontig ? 1 : d.ldb);
+      e.C += i0 + j0 * d.ldc;
+      run_core(e, cs, beta, s);
+    }
+}
+
+}  // namespace
+
+void set_split_moduli(int n_moduli) {
+  if (n_moduli < 0 || n_moduli > kOzakiMaxModuli)
+    throw Error(kErrInvalid, "number of split-precision moduli must be 0..16");
+  g_split_moduli = n_moduli;
+}
+
+int split_moduli() { return g_split_moduli; }
+
+void set_split_min_flops(double flops) {
+  if (!(flops >= 0.0)) throw Error(kErrInvalid, "split-precision threshold must be >= 0");
+  g_split_min_flops = flops;
+}
+
+double split_min_flops() { return g_split_min_flops; }
+
+int ozaki_bits(int n_moduli, long long k_total) {
+  const Consts& cs = consts_for(n_moduli);
+  const double kb = std::ceil(std::log2(double(std::max<long long>(k_total, 1))));
+  const int beta = static_cast<int>(std::floor((cs.log2_m - 2.0 - kb) / 2.0));
+  return std::min(beta, 52);
+}
+
+bool ozaki_supported(const GemmDesc& d) {
+  const long long k_total = d.k * d.nbr1 * d.nbr2;
+  return d.m <= (1LL << 30) && d.n <= (1LL << 30) && k_total <= 65535LL * kTileK &&
+         d.nbo1 * d.nbo2 <= 65535;
+}
+
+void gemm_ozaki(const GemmDesc& d, int n_moduli) {
+  if (n_moduli < 1 || n_moduli > kOzakiMaxModuli)
+    throw Error(kErrInvalid, "number of split-precision moduli must be 1..16");
+  if (d.m <= 0 || d.n <= 0 || d.nbo1 <= 0 || d.nbo2 <= 0) return;
+  if (d.k <= 0 || d.nbr1 <= 0 || d.nbr2 <= 0) {
+    gemm_dmma(d);  // C = beta C
+    return;
+  }
+  if (!ozaki_supported(d)) throw Error(kErrInvalid, "split-precision GEMM: shape too large");
+  const long long k_total = d.k * d.nbr1 * d.nbr2;
+  const int beta = ozaki_bits(n_moduli, k_total);
+  if (beta < 4)
+    throw Error(kErrInvalid, "split-precision GEMM: too few moduli for a contraction of " +
+                                 std::to_string(k_total) + " terms");
+  cudaStream_t s = current_stream();
+  const Consts& cs = consts_for(n_moduli);
+  Timer tm(kProfSplitGemm,
+           2.0 * double(d.m) * double(d.n) * double(k_total) * double(d.nbo1 * d.nbo2), "split",
+           s);
+  run_slabs(d, cs, beta, s);
+  tm.stop();
+}
+
+int ozaki_error_read_and_clear() {
+  int* f = err_flag();
+  cudaStream_t s = current_stream();
+  int h = 0;
+  UW12_CUDA(cudaMemcpyAsync(&h, f, sizeof(int), cudaMemcpyDeviceToHost, s));
+  UW12_CUDA(cudaStreamSynchronize(s));
+  if (h) UW12_CUDA(cudaMemsetAsync(f, 0, sizeof(int), s));
+  return h;
+}
+
+}  // namespace uw12b
