@@ -544,7 +544,8 @@ void gemm(const GemmDesc& d) {
   if (L > 0) {
     const double flops = 2.0 * double(d.m) * double(d.n) * double(d.k) * double(d.nbo1) *
                          double(d.nbo2) * double(d.nbr1) * double(d.nbr2);
-    if (flops >= split_min_flops() && ozaki_supported(d)) {
+    const double min_flops = split_min_flops();
+    if (flops >= min_flops && (min_flops == 0.0 || ozaki_profitable(d)) && ozaki_supported(d)) {
       gemm_ozaki(d, L);
       return;
     }

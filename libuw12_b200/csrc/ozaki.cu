@@ -14,9 +14,9 @@
 //                 Warp roles: 0 TMA producer, 1 TMEM owner + MMA issuer,
 //                 2..5 epilogue (TMEM lane quarter = warp % 4);
 //   k_crt         per output element: sum the K-chunk residues mod p, CRT on
-//                 36-bit chunks in FP64 (exact integer arithmetic; the value is
-//                 rounded only when the chunks are joined, <= 2^-52 relative),
-//                 scale by 2^-(sa+sb), apply alpha / beta, store FP64.
+//                 <= 41-bit chunks in FP64 (exact integer arithmetic), join the
+//                 chunks error-free (TwoSum), scale by 2^-(sa+sb), apply
+//                 alpha / beta, store FP64.
 // The MMA's M side (TMEM lanes) runs over the output column j (B's n index)
 // and its N side over the output row i (A's m index), so that one thread of
 // the epilogue owns 256 consecutive i of one column j and the residue planes
@@ -39,12 +39,14 @@ namespace {
 // Pairwise-coprime moduli <= 256 (residues fit int8: [-128, 127]).
 constexpr uint32_t kModuli[kOzakiMaxModuli] = {256, 255, 253, 251, 247, 241, 239, 233,
                                                229, 227, 223, 217, 211, 199, 197, 193};
-constexpr int kChunkBits = 36;  // CRT weight chunks: r_l * chunk < 2^44, sums < 2^49
-constexpr int kMaxChunks = 4;   // 144 bits >= log2(M) for 16 moduli (~125.3)
+// CRT weights are split into nch chunks of cw <= 41 bits: r_l * chunk < 2^49
+// and the sum over <= 16 moduli < 2^53, so every chunk sum is exact in FP64.
+constexpr int kMaxChunkBits = 41;
+constexpr int kMaxChunks = 4;  // 4 x 41 bits >= log2(M) for 16 moduli (~125.3)
 constexpr long long kMaxKChunk = 65536;  // |acc| <= 65536 * 128^2 = 2^30 per split
 
 struct Consts {
-  int L = 0, nch = 0, beta = 0;
+  int L = 0, nch = 0, cw = 0, beta = 0;
   uint32_t p[kOzakiMaxModuli];
   uint32_t barrett[kOzakiMaxModuli];  // floor(2^32 / p)
   uint32_t off[kOzakiMaxModuli];      // multiple of p, >= 2^30
@@ -85,7 +87,9 @@ Consts make_consts(int L) {
   }
   int bits = 0;
   for (u128 t = M; t; t >>= 1) ++bits;
-  c.nch = (bits + kChunkBits - 1) / kChunkBits;
+  c.nch = (bits + kMaxChunkBits - 1) / kMaxChunkBits;
+  c.cw = (bits + c.nch - 1) / c.nch;
+  const int kChunkBits = c.cw;
   const u128 mask = (u128(1) << kChunkBits) - 1;
   for (int l = 0; l < L; ++l) {
     const u128 Ml = M / kModuli[l];
@@ -170,31 +174,73 @@ __device__ __forceinline__ void load_tile(const OperandView& v, int plane, long 
 }
 
 // Per row: exponent e of its largest element (2^(e-1) <= max|x| < 2^e),
-// stored as e + 2048 through atomicMax (0 = all zeros).  Grid: (row tiles,
-// k tiles, planes).
+// stored as e + 2048 through atomicMax (0 = all zeros).  One block covers 32
+// rows x kExpTileK k of one plane (grid: row tiles, k tiles, planes) and reads
+// straight into registers, 64 independent loads per thread: KCONTIG (rows
+// contiguous along k) lets each warp sweep 4 rows along k, otherwise each warp
+// takes every 8th k of all 32 rows (consecutive rows per warp load).
+constexpr int kExpTileK = 512;
+
 template <bool KCONTIG>
 __global__ void __launch_bounds__(256) k_row_exponent(OperandView v,
                                                       unsigned* __restrict__ eplus) {
-  __shared__ double tile[32][129];
-  __shared__ long long koff[128];
+  __shared__ long long koff[kExpTileK];
+  __shared__ double part[8][33];
   const int plane = blockIdx.z;
   const long long row0 = static_cast<long long>(blockIdx.x) * 32;
-  tile_k_offsets(v, static_cast<long long>(blockIdx.y) * 128, koff);
+  const long long k0 = static_cast<long long>(blockIdx.y) * kExpTileK;
+  for (int c = threadIdx.x; c < kExpTileK; c += 256) {
+    const long long kt = k0 + c;
+    long long off = -1;
+    if (kt < v.k_total) {
+      const long long r = kt / v.k, kk = kt - r * v.k;
+      off = kk * v.ks + (r % v.nbr1) * v.sr1 + (r / v.nbr1) * v.sr2;
+    }
+    koff[c] = off;
+  }
   __syncthreads();
-  load_tile<KCONTIG>(v, plane, row0, koff, tile);
-  __syncthreads();
-  // 8 warps x 4 rows: each warp reduces its rows across the 32 lanes
+  const double* pb = v.base + (plane % v.np1) * v.po1 + (plane / v.np1) * v.po2;
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  for (int rr = 0; rr < 4; ++rr) {
-    const int r = warp * 4 + rr;
-    double mx = fmax(fmax(fabs(tile[r][lane]), fabs(tile[r][lane + 32])),
-                     fmax(fabs(tile[r][lane + 64]), fabs(tile[r][lane + 96])));
-    for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    const long long row = row0 + r;
-    if (lane == 0 && row < v.rows && mx > 0.0) {
-      int e = 0;
-      frexp(mx, &e);
-      atomicMax(&eplus[plane * v.rows + row], static_cast<unsigned>(e + 2048));
+  if (KCONTIG) {
+#pragma unroll
+    for (int rr = 0; rr < 4; ++rr) {
+      const long long row = row0 + warp * 4 + rr;
+      double mx = 0.0;
+      if (row < v.rows) {
+        const double* rp = pb + row * v.rs;
+#pragma unroll
+        for (int t = 0; t < kExpTileK / 32; ++t) {
+          const long long ko = koff[lane + 32 * t];
+          if (ko >= 0) mx = fmax(mx, fabs(rp[ko]));
+        }
+      }
+      for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      if (lane == 0 && row < v.rows && mx > 0.0) {
+        int e = 0;
+        frexp(mx, &e);
+        atomicMax(&eplus[plane * v.rows + row], static_cast<unsigned>(e + 2048));
+      }
+    }
+  } else {
+    const long long row = row0 + lane;
+    double mx = 0.0;
+    if (row < v.rows) {
+      const double* rp = pb + row * v.rs;
+#pragma unroll 16
+      for (int t = 0; t < kExpTileK / 8; ++t) {
+        const long long ko = koff[warp + 8 * t];
+        if (ko >= 0) mx = fmax(mx, fabs(rp[ko]));
+      }
+    }
+    part[warp][lane] = mx;
+    __syncthreads();
+    if (warp == 0) {
+      for (int w = 1; w < 8; ++w) mx = fmax(mx, part[w][lane]);
+      if (row < v.rows && mx > 0.0) {
+        int e = 0;
+        frexp(mx, &e);
+        atomicMax(&eplus[plane * v.rows + row], static_cast<unsigned>(e + 2048));
+      }
     }
   }
 }
@@ -208,23 +254,40 @@ __global__ void k_exponent_to_shift(const unsigned* __restrict__ eplus, long lon
 
 struct ResidueMods {
   int L;
-  double pd[kOzakiMaxModuli], inv_p[kOzakiMaxModuli];
+  int pi[kOzakiMaxModuli];
+  double inv_p[kOzakiMaxModuli];
 };
 
-__device__ __forceinline__ uint32_t residue_byte(double v, double p, double inv_p) {
-  const double q = rint(v * inv_p);
-  double r = fma(-q, p, v);  // exact: an integer of magnitude <= p/2 + 1
-  if (r > 127.0) r -= p;
-  if (r < -128.0) r += p;
-  return static_cast<uint32_t>(static_cast<int>(r)) & 0xffu;
+// FP64 integer tricks that keep the conversion unit out of the inner loops:
+// (x + 1.5 2^52) - 1.5 2^52 rounds |x| < 2^51 to the nearest integer, and
+// the low word of r + 1.5 2^52 is the integer r as a two's-complement int32.
+constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
+__device__ __forceinline__ double round_int(double x) {
+  return __dadd_rn(__dadd_rn(x, kRound), -kRound);
+}
+__device__ __forceinline__ int int_of(double r) { return __double2loint(__dadd_rn(r, kRound)); }
+
+// Residues of the integer v (|v| <= 2^50) modulo p as int8 bytes.  With
+// q = rint(v / p) the remainder r = v - q p lies in [-(p-1)/2, (p-1)/2] for odd
+// p <= 255 and in [-128, 128] for p = 256; its low byte is r as int8 (128 as
+// -128, congruent mod 256).  fma(v, 1/p, 1.5 2^52) rounds v / p exactly (for
+// odd p, v / p is at least 1/(2p) >= 2^-9 away from a half-integer while the
+// product's error is below |v / p| 2^-53 < 2^-10.6; p = 256 is exact) and its
+// low word is q as an int32; with vl = v mod 2^32, r mod 2^32 = vl - q p.  One
+// DFMA and one integer multiply-add per residue.
+__device__ __forceinline__ uint32_t residue_low(int vl, double v, double inv_p, int p) {
+  const int q = __double2loint(fma(v, inv_p, kRound));
+  return static_cast<uint32_t>(vl - q * p);  // low byte = residue
 }
 
-// Tile of 32 rows x 128 k of one plane -> L residue planes.
-// out[((l * planes + plane) * rows_pad + row) * k_pad + kt], zeros in padding.
+// Tile of 32 rows x 128 k of one plane -> L residue rows per row: row r of
+// modulus l of a plane is out row ((plane * tiles + r / T) * L + l) * T + r % T
+// (T = tile_rows, the MMA tile height of this operand), each k_pad bytes;
+// zeros in padding.  The L residue rows of a tile are T * k_pad bytes apart.
 // Grid: (row tiles, k tiles, planes).
 template <bool KCONTIG>
 __global__ void __launch_bounds__(256) k_residues(OperandView v, const int* __restrict__ shift,
-                                                  ResidueMods mods, int planes,
+                                                  ResidueMods mods, int tile_rows,
                                                   long long rows_pad, long long k_pad,
                                                   uint8_t* __restrict__ out) {
   __shared__ double tile[32][129];
@@ -242,15 +305,35 @@ __global__ void __launch_bounds__(256) k_residues(OperandView v, const int* __re
     const int r = it * 8 + tid / 32;
     const long long row = row0 + r;
     const int sh = row < v.rows ? shift[plane * v.rows + row] : 0;
-    const double x0 = rint(ldexp(tile[r][c4], sh)), x1 = rint(ldexp(tile[r][c4 + 1], sh)),
-                 x2 = rint(ldexp(tile[r][c4 + 2], sh)), x3 = rint(ldexp(tile[r][c4 + 3], sh));
+    // row of modulus 0 in the residue layout ((plane * tiles + tile) * L + l) * tile_rows + r
+    const long long tile_base =
+        ((plane * (rows_pad / tile_rows) + row / tile_rows) * mods.L) * tile_rows + row % tile_rows;
+    double x0, x1, x2, x3;
+    if (sh > -1000 && sh < 1000) {  // 2^sh is a normal double: scale by one multiply
+      const double sc = ldexp(1.0, sh);
+      x0 = round_int(tile[r][c4] * sc);
+      x1 = round_int(tile[r][c4 + 1] * sc);
+      x2 = round_int(tile[r][c4 + 2] * sc);
+      x3 = round_int(tile[r][c4 + 3] * sc);
+    } else {
+      x0 = round_int(ldexp(tile[r][c4], sh));
+      x1 = round_int(ldexp(tile[r][c4 + 1], sh));
+      x2 = round_int(ldexp(tile[r][c4 + 2], sh));
+      x3 = round_int(ldexp(tile[r][c4 + 3], sh));
+    }
+    const int v0 = int_of(x0), v1 = int_of(x1), v2 = int_of(x2), v3 = int_of(x3);
+    uint8_t* dst = out + tile_base * k_pad + k0 + c4;
+    const long long lstep = static_cast<long long>(tile_rows) * k_pad;
+#pragma unroll 4
     for (int l = 0; l < mods.L; ++l) {
-      const double p = mods.pd[l], ip = mods.inv_p[l];
-      const uint32_t word = residue_byte(x0, p, ip) | (residue_byte(x1, p, ip) << 8) |
-                            (residue_byte(x2, p, ip) << 16) | (residue_byte(x3, p, ip) << 24);
-      uint8_t* dst =
-          out + ((static_cast<long long>(l) * planes + plane) * rows_pad + row) * k_pad + k0 + c4;
-      *reinterpret_cast<uint32_t*>(dst) = word;
+      const double ip = mods.inv_p[l];
+      const int p = mods.pi[l];
+      const uint32_t lo =
+          __byte_perm(residue_low(v0, x0, ip, p), residue_low(v1, x1, ip, p), 0x0040);
+      const uint32_t hi =
+          __byte_perm(residue_low(v2, x2, ip, p), residue_low(v3, x3, ip, p), 0x0040);
+      *reinterpret_cast<uint32_t*>(dst) = __byte_perm(lo, hi, 0x5410);
+      dst += lstep;
     }
   }
 }
@@ -378,6 +461,14 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
         "=r"(v[31])                                                                            \
       : "r"(taddr))
 
+// Product residues: byte (split, batch b, column j, modulus l, row i) at
+// (((split * nbatch + b) * n_pad + j) * L + l) * m_pad + i, so that the L
+// residues of one column lie within L * m_pad bytes of each other.
+__device__ __forceinline__ long long residue_offset(const MmaArgs& a, int split, int b,
+                                                    long long j, int l) {
+  return (((static_cast<long long>(split) * a.nbatch + b) * a.n_pad + j) * a.L + l) * a.m_pad;
+}
+
 __device__ __forceinline__ uint32_t mod_u32(uint32_t u, uint32_t p, uint32_t barrett) {
   uint32_t r = u - __umulhi(u, barrett) * p;
   return r >= p ? r - p : r;
@@ -408,10 +499,11 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int pb = (a.b_var1 ? b1 : 0) + (a.b_var1 ? a.nbo1 : 1) * (a.b_var2 ? b2 : 0);
   const int kb0 = split * a.kb_per_split;
   const int nkb = min(a.kb_per_split, a.kb_total - kb0);
-  const int yj = static_cast<int>((static_cast<long long>(l) * a.planes_b + pb) * a.n_pad +
-                                  static_cast<long long>(tj) * kTileJ);
-  const int yi = static_cast<int>((static_cast<long long>(l) * a.planes_a + pa) * a.m_pad +
-                                  static_cast<long long>(ti) * kTileI);
+  // residue rows: ((plane * tiles + tile) * L + l) * tile_rows + row in tile
+  const int yj = static_cast<int>(
+      ((static_cast<long long>(pb) * (a.n_pad / kTileJ) + tj) * a.L + l) * kTileJ);
+  const int yi = static_cast<int>(
+      ((static_cast<long long>(pa) * (a.m_pad / kTileI) + ti) * a.L + l) * kTileI);
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -481,9 +573,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (ok && nkb > 0) {
       const uint32_t p = a.p[l], bm = a.barrett[l], off = a.off[l];
       const long long j = static_cast<long long>(tj) * kTileJ + q * 32 + lane;
-      uint8_t* rowp =
-          a.R + ((static_cast<long long>(split) * a.L + l) * a.nbatch + b) * a.n_pad * a.m_pad +
-          j * a.m_pad + static_cast<long long>(ti) * kTileI;
+      uint8_t* rowp = a.R + residue_offset(a, split, b, j, l) + static_cast<long long>(ti) * kTileI;
 #pragma unroll 1
       for (int c = 0; c < kTileI / 32; ++c) {
         uint32_t v[32];
@@ -505,9 +595,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     } else if (nkb == 0) {
       // empty K chunk: residue 0
       const long long j = static_cast<long long>(tj) * kTileJ + q * 32 + lane;
-      uint4* dst = reinterpret_cast<uint4*>(
-          a.R + ((static_cast<long long>(split) * a.L + l) * a.nbatch + b) * a.n_pad * a.m_pad +
-          j * a.m_pad + static_cast<long long>(ti) * kTileI);
+      uint4* dst = reinterpret_cast<uint4*>(a.R + residue_offset(a, split, b, j, l) +
+                                            static_cast<long long>(ti) * kTileI);
       for (int c = 0; c < kTileI / 16; ++c) dst[c] = make_uint4(0, 0, 0, 0);
     }
   }
@@ -545,67 +634,162 @@ struct CrtArgs {
   double w[kOzakiMaxModuli][kMaxChunks];
   double mc[kMaxChunks];
   double inv_m;
+  int cw;  // CRT chunk width in bits
 };
 
-// One thread = 4 consecutive rows i of one column j of one batch.
-__global__ void __launch_bounds__(256) k_crt(const CrtArgs a, long long i4_count) {
-  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const long long per_b = i4_count * a.n;
-  if (t >= per_b * a.nbatch) return;
-  const int b = static_cast<int>(t / per_b);
-  const long long rem = t - b * per_b;
-  const long long j = rem / i4_count;
-  const long long i0 = (rem - j * i4_count) * 4;
+// One thread = 4 consecutive rows i of a column j of one batch; grid (row
+// blocks of 1024, columns strided by gridDim.y, batches).  The L residue words
+// of a column are loaded before any is used (one load per modulus and K chunk
+// in flight per thread), the K-chunk sums of the 4 bytes are kept as pairs of
+// 16-bit lanes, and the CRT runs on NCH chunks of cw bits.
+// x 2^e: one multiply by an exactly representable power of two when 2^e is a
+// normal double, ldexp otherwise.
+__device__ __forceinline__ double scale_pow2(double x, int e) {
+  if (e >= -1022 && e <= 1023)
+    return x * __longlong_as_double(static_cast<long long>(e + 1023) << 52);
+  return ldexp(x, e);
+}
+
+// s + e = a + b exactly (Knuth's TwoSum, six FP64 operations).
+__device__ __forceinline__ double two_sum(double a, double b, double& e) {
+  const double s = __dadd_rn(a, b);
+  const double bb = __dsub_rn(s, a);
+  e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
+  return s;
+}
+
+// sum_c d[c] 2^(cw c) for integer-valued doubles |d[c]| < 2^53: every term
+// d[c] 2^(cw c) is exact, the running sum is carried error-free (TwoSum) and
+// the integer errors are added at the end, so the result equals the exact sum
+// whenever that is a double and is within one unit in the last place
+// otherwise.
+template <int NCH>
+__device__ __forceinline__ double join_chunks(const double (&d)[NCH], double chunk) {
+  double pw = 1.0;
+  double terms[NCH];
+#pragma unroll
+  for (int c = 0; c < NCH; ++c) {
+    terms[c] = d[c] * pw;  // exact: a power-of-two scaling
+    pw *= chunk;
+  }
+  double sum = terms[NCH - 1], err = 0.0;
+#pragma unroll
+  for (int c = NCH - 2; c >= 0; --c) {
+    double e;
+    sum = two_sum(sum, terms[c], e);
+    err += e;
+  }
+  return sum + err;
+}
+
+// Byte b (0..3) of w as a double: the byte placed in the low word under the
+// exponent of 2^52, minus 2^52.
+__device__ __forceinline__ double byte_to_double(uint32_t w, int b) {
+  return __dsub_rn(__hiloint2double(0x43300000, static_cast<int>(__byte_perm(w, 0, 0x4440 + b))),
+                   4503599627370496.0);
+}
+
+// Residue (< 2^16) to double without the conversion unit.
+__device__ __forceinline__ double small_to_double(uint32_t r) {
+  return __dsub_rn(__hiloint2double(0x43300000, static_cast<int>(r)), 4503599627370496.0);
+}
+
+// REDUCE: several K chunks, whose residue sums are reduced mod p; with one K
+// chunk the stored residues (already in [0, p)) enter the CRT sum directly.
+template <int NCH, bool REDUCE>
+__global__ void __launch_bounds__(256, 2) k_crt(const CrtArgs a) {
+  const long long i0 = (static_cast<long long>(blockIdx.x) * 256 + threadIdx.x) * 4;
+  if (i0 >= a.m) return;
+  const int b = blockIdx.z;
   const int b1 = b % a.nbo1, b2 = b / a.nbo1;
   const int pa = (a.a_var1 ? b1 : 0) + (a.a_var1 ? a.nbo1 : 1) * (a.a_var2 ? b2 : 0);
   const int pb = (a.b_var1 ? b1 : 0) + (a.b_var1 ? a.nbo1 : 1) * (a.b_var2 ? b2 : 0);
-
-  double S[4][kMaxChunks];
+  // residue layout of k_i8_mma: (((split * nbatch + b) * n_pad + j) * L + l) * m_pad + i
+  const long long lstride = a.m_pad;                                             // next modulus
+  const long long sstride = static_cast<long long>(a.nbatch) * a.n_pad * a.L * a.m_pad;  // K chunk
+  int sa[4];
 #pragma unroll
   for (int e = 0; e < 4; ++e)
+    sa[e] = i0 + e < a.m ? a.shift_a[pa * a.rows_a + i0 + e] : 0;
+  const double chunk = __longlong_as_double(static_cast<long long>(a.cw + 1023) << 52);  // 2^cw
+
+  for (long long j = blockIdx.y; j < a.n; j += gridDim.y) {
+    const uint8_t* base = a.R + (static_cast<long long>(b) * a.n_pad + j) * a.L * a.m_pad + i0;
+    // one residue word (4 rows) per modulus and K chunk, all loads issued first
+    uint32_t w0[kOzakiMaxModuli];
 #pragma unroll
-    for (int c = 0; c < kMaxChunks; ++c) S[e][c] = 0.0;
-  const long long plane = a.n_pad * a.m_pad;
-  const long long pos = j * a.m_pad + i0;
-  for (int l = 0; l < a.L; ++l) {
-    uint32_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-    for (int sp = 0; sp < a.splits; ++sp) {
-      const uint32_t word = *reinterpret_cast<const uint32_t*>(
-          a.R + ((static_cast<long long>(sp) * a.L + l) * a.nbatch + b) * plane + pos);
-      s0 += word & 0xffu;
-      s1 += (word >> 8) & 0xffu;
-      s2 += (word >> 16) & 0xffu;
-      s3 += word >> 24;
+    for (int l = 0; l < kOzakiMaxModuli; ++l)
+      if (l < a.L) w0[l] = __ldg(reinterpret_cast<const uint32_t*>(base + l * lstride));
+    double S[4][NCH];
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+#pragma unroll
+      for (int c = 0; c < NCH; ++c) S[e][c] = 0.0;
+    if (!REDUCE) {
+      // one K chunk: the stored residues (in [0, p)) enter the CRT sum directly
+#pragma unroll
+      for (int l = 0; l < kOzakiMaxModuli; ++l) {
+        if (l < a.L) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const double r = byte_to_double(w0[l], e);
+#pragma unroll
+            for (int c = 0; c < NCH; ++c) S[e][c] = fma(r, a.w[l][c], S[e][c]);
+          }
+        }
+      }
+    } else {
+      // K chunks: byte sums in 16-bit lanes (bytes 0, 2 and 1, 3), reduced mod p
+      uint32_t s02[kOzakiMaxModuli], s13[kOzakiMaxModuli];
+#pragma unroll
+      for (int l = 0; l < kOzakiMaxModuli; ++l) {
+        if (l < a.L) {
+          s02[l] = w0[l] & 0x00ff00ffu;
+          s13[l] = (w0[l] >> 8) & 0x00ff00ffu;
+        }
+      }
+      for (int sp = 1; sp < a.splits; ++sp) {
+#pragma unroll
+        for (int l = 0; l < kOzakiMaxModuli; ++l) {
+          if (l < a.L) {
+            const uint32_t w =
+                __ldg(reinterpret_cast<const uint32_t*>(base + sp * sstride + l * lstride));
+            s02[l] += w & 0x00ff00ffu;
+            s13[l] += (w >> 8) & 0x00ff00ffu;
+          }
+        }
+      }
+#pragma unroll
+      for (int l = 0; l < kOzakiMaxModuli; ++l) {
+        if (l < a.L) {
+          const uint32_t p = a.p[l], bm = a.barrett[l];
+          const uint32_t u[4] = {s02[l] & 0xffffu, s13[l] & 0xffffu, s02[l] >> 16, s13[l] >> 16};
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const double r = small_to_double(mod_u32(u[e], p, bm));
+#pragma unroll
+            for (int c = 0; c < NCH; ++c) S[e][c] = fma(r, a.w[l][c], S[e][c]);
+          }
+        }
+      }
     }
-    const uint32_t p = a.p[l], bm = a.barrett[l];
-    const double r[4] = {double(mod_u32(s0, p, bm)), double(mod_u32(s1, p, bm)),
-                         double(mod_u32(s2, p, bm)), double(mod_u32(s3, p, bm))};
+    const int sb = a.shift_b[pb * a.rows_b + j];
+    double* Cb = a.C + b1 * a.sCo1 + b2 * a.sCo2 + j * a.ldc;
 #pragma unroll
-    for (int c = 0; c < kMaxChunks; ++c) {
-      const double wc = a.w[l][c];
+    for (int e = 0; e < 4; ++e) {
+      const long long i = i0 + e;
+      if (i >= a.m) break;
+      double approx = 0.0;
 #pragma unroll
-      for (int e = 0; e < 4; ++e) S[e][c] = fma(r[e], wc, S[e][c]);
+      for (int c = NCH - 1; c >= 0; --c) approx = fma(approx, chunk, S[e][c]);
+      const double q = round_int(approx * a.inv_m);  // |q| < 2^13
+      double dig[NCH];
+#pragma unroll
+      for (int c = 0; c < NCH; ++c) dig[c] = fma(-q, a.mc[c], S[e][c]);  // exact
+      double out = a.alpha * scale_pow2(join_chunks<NCH>(dig, chunk), -(sa[e] + sb));
+      if (a.beta != 0.0) out = fma(a.beta, Cb[i], out);
+      Cb[i] = out;
     }
-  }
-  const int sb = a.shift_b[pb * a.rows_b + j];
-  double* Cb = a.C + b1 * a.sCo1 + b2 * a.sCo2 + j * a.ldc;
-  constexpr double kChunk = 68719476736.0;  // 2^36
-#pragma unroll
-  for (int e = 0; e < 4; ++e) {
-    const long long i = i0 + e;
-    if (i >= a.m) break;
-    // chunks above nch are zero, so running over all kMaxChunks is exact
-    double approx = 0.0;
-#pragma unroll
-    for (int c = kMaxChunks - 1; c >= 0; --c) approx = fma(approx, kChunk, S[e][c]);
-    const double q = rint(approx * a.inv_m);
-    double v = 0.0;
-#pragma unroll
-    for (int c = kMaxChunks - 1; c >= 0; --c) v = fma(v, kChunk, fma(-q, a.mc[c], S[e][c]));
-    const int sa = a.shift_a[pa * a.rows_a + i];
-    double out = a.alpha * ldexp(v, -(sa + sb));
-    if (a.beta != 0.0) out = fma(a.beta, Cb[i], out);
-    Cb[i] = out;
   }
 }
 
@@ -725,35 +909,38 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
   ResidueMods mods;
   mods.L = L;
   for (int l = 0; l < L; ++l) {
-    mods.pd[l] = cs.pd[l];
+    mods.pi[l] = static_cast<int>(cs.p[l]);
     mods.inv_p[l] = cs.inv_p[l];
   }
   {
     const double bytes = 8.0 * double(planes_a * d.m + planes_b * d.n) * double(k_total) * 2.0 +
                          double(L) * double(planes_a * m_pad + planes_b * n_pad) * double(k_pad);
     Timer tm(kProfSplitPrep, bytes, "prep", s);
-    auto prep = [&](const OperandView& v, long long planes, long long rows_pad, int* sh,
-                    unsigned* ep, uint8_t* out) {
+    auto prep = [&](const OperandView& v, long long planes, long long rows_pad, int tile_rows,
+                    int* sh, unsigned* ep, uint8_t* out) {
       UW12_CUDA(cudaMemsetAsync(ep, 0, planes * v.rows * sizeof(unsigned), s));
+      dim3 ge(static_cast<unsigned>(rows_pad / 32),
+              static_cast<unsigned>((k_pad + kExpTileK - 1) / kExpTileK),
+              static_cast<unsigned>(planes));
+      if (v.ks == 1)
+        k_row_exponent<true><<<ge, 256, 0, s>>>(v, ep);
+      else
+        k_row_exponent<false><<<ge, 256, 0, s>>>(v, ep);
       dim3 g(static_cast<unsigned>(rows_pad / 32), static_cast<unsigned>(k_pad / 128),
              static_cast<unsigned>(planes));
-      if (v.ks == 1)
-        k_row_exponent<true><<<g, 256, 0, s>>>(v, ep);
-      else
-        k_row_exponent<false><<<g, 256, 0, s>>>(v, ep);
       UW12_LAUNCHED();
       const long long nsh = planes * v.rows;
       k_exponent_to_shift<<<static_cast<unsigned>((nsh + 255) / 256), 256, 0, s>>>(ep, nsh, beta,
                                                                                   sh);
       UW12_LAUNCHED();
       if (v.ks == 1)
-        k_residues<true><<<g, 256, 0, s>>>(v, sh, mods, int(planes), rows_pad, k_pad, out);
+        k_residues<true><<<g, 256, 0, s>>>(v, sh, mods, tile_rows, rows_pad, k_pad, out);
       else
-        k_residues<false><<<g, 256, 0, s>>>(v, sh, mods, int(planes), rows_pad, k_pad, out);
+        k_residues<false><<<g, 256, 0, s>>>(v, sh, mods, tile_rows, rows_pad, k_pad, out);
       UW12_LAUNCHED();
     };
-    prep(va, planes_a, m_pad, sa, ea, ra);
-    prep(vb, planes_b, n_pad, sb, eb, rb);
+    prep(va, planes_a, m_pad, kTileI, sa, ea, ra);
+    prep(vb, planes_b, n_pad, kTileJ, sb, eb, rb);
     tm.stop();
   }
 
@@ -828,12 +1015,24 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
     }
     for (int c = 0; c < kMaxChunks; ++c) ca.mc[c] = cs.mc[c];
     ca.inv_m = cs.inv_m;
-    const long long i4 = (d.m + 3) / 4;
-    const long long threads = i4 * d.n * nbatch;
+    ca.cw = cs.cw;
     const double bytes = double(splits * L) * double(d.m * d.n * nbatch) +
                          8.0 * double(d.m * d.n * nbatch) * (d.beta != 0.0 ? 2.0 : 1.0);
     Timer tm(kProfSplitCrt, bytes, "crt", s);
-    k_crt<<<static_cast<unsigned>((threads + 255) / 256), 256, 0, s>>>(ca, i4);
+    const dim3 g(static_cast<unsigned>((d.m + 1023) / 1024),
+                 static_cast<unsigned>(std::min<long long>(d.n, 65535)),
+                 static_cast<unsigned>(nbatch));
+    const bool reduce = splits > 1;
+    switch (cs.nch * 2 + (reduce ? 1 : 0)) {
+      case 2: k_crt<1, false><<<g, 256, 0, s>>>(ca); break;
+      case 3: k_crt<1, true><<<g, 256, 0, s>>>(ca); break;
+      case 4: k_crt<2, false><<<g, 256, 0, s>>>(ca); break;
+      case 5: k_crt<2, true><<<g, 256, 0, s>>>(ca); break;
+      case 6: k_crt<3, false><<<g, 256, 0, s>>>(ca); break;
+      case 7: k_crt<3, true><<<g, 256, 0, s>>>(ca); break;
+      case 8: k_crt<4, false><<<g, 256, 0, s>>>(ca); break;
+      default: k_crt<4, true><<<g, 256, 0, s>>>(ca); break;
+    }
     UW12_LAUNCHED();
     tm.stop();
   }
@@ -931,7 +1130,15 @@ int ozaki_bits(int n_moduli, long long k_total) {
   const Consts& cs = consts_for(n_moduli);
   const double kb = std::ceil(std::log2(double(std::max<long long>(k_total, 1))));
   const int beta = static_cast<int>(std::floor((cs.log2_m - 2.0 - kb) / 2.0));
-  return std::min(beta, 52);
+  return std::min(beta, 50);  // |A'| <= 2^50: the FP64 rounding tricks stay exact
+}
+
+bool ozaki_profitable(const GemmDesc& d) {
+  // The operand preparation streams A and B (twice in FP64, once as L bytes
+  // per element) and costs about as much as 2mn/(m+n) ~ 800 FP64 FLOPs per
+  // operand element; thinner GEMMs are faster on the FP64 path.
+  const double m = double(d.m), n = double(d.n);
+  return 2.0 * m * n >= 800.0 * (m + n);
 }
 
 bool ozaki_supported(const GemmDesc& d) {

@@ -9,9 +9,11 @@
 //   2. for each of L pairwise-coprime moduli p_l <= 256 (M = prod p_l) the
 //      residues A' mod p_l and B' mod p_l are int8 matrices and their
 //      product is exact in int32 (K split into chunks of <= 65536);
-//   3. the Chinese remainder theorem rebuilds A'B' from the L residue
-//      products (FP64 arithmetic on 36-bit chunks, exact until the chunks are
-//      joined into one double: <= 2^-52 relative), and C = 2^-(sa_i + sb_j) A'B'.
+//   3. the Chinese remainder theorem rebuilds the integer A'B' exactly from
+//      the L residue products (FP64 arithmetic on <= 41-bit chunks), whose
+//      error-free sum gives A'B' to within one unit in the last place (exactly
+//      when it is a double), and C = 2^-(sa_i + sb_j) A'B' (products of
+//      small-integer matrices come out exact).
 // The only error is the rounding of A and B to beta bits relative to the
 // largest element of their row / column: |dC_ij| <= 2^-beta (max|a_i.| sum_k
 // |b_kj| + max|b_.j| sum_k |a_ik|) (beta = 48 for L = 14, K = 1500).
@@ -30,7 +32,8 @@ void set_split_moduli(int n_moduli);
 int split_moduli();
 constexpr double kOzakiMinFlops = 2e9;
 // Smallest GEMM (FLOPs) routed to the split-precision path on this host
-// thread (default kOzakiMinFlops; 0 routes every GEMM).
+// thread (default kOzakiMinFlops; GEMMs above it also have to pass
+// ozaki_profitable).  0 routes every GEMM, whatever its shape.
 void set_split_min_flops(double flops);
 double split_min_flops();
 
@@ -38,6 +41,8 @@ double split_min_flops();
 void gemm_ozaki(const GemmDesc& d, int n_moduli);
 // Shapes the split-precision kernels take (K <= 8.4M, m, n <= 2^30).
 bool ozaki_supported(const GemmDesc& d);
+// Whether the split path is expected to beat the FP64 path (2mn/(m+n) >= 800).
+bool ozaki_profitable(const GemmDesc& d);
 
 // beta (bits kept per operand element) for n_moduli moduli and a contraction
 // of k_total terms.
