@@ -7,12 +7,13 @@
 //                 that every element is below 2^beta in magnitude;
 //   k_residues    FP64 -> rint(x 2^shift) -> L int8 residue planes, K-major
 //                 (row r of plane (l, p) is K_pad contiguous bytes);
-//   k_i8_mma      one CTA = one 128 x 256 output tile of one modulus and one
-//                 K chunk: TMA (128-byte swizzled boxes) -> shared memory ->
-//                 tcgen05.mma.kind::i8 with the int32 accumulator in TMEM ->
-//                 tcgen05.ld -> residue mod p -> uint8 plane in HBM.
-//                 Warp roles: 0 TMA producer, 1 TMEM owner + MMA issuer,
-//                 2..5 epilogue (TMEM lane quarter = warp % 4);
+//   k_i8_mma      persistent, one CTA per SM; work item = one 128 x 256
+//                 output tile of one modulus and one K chunk: TMA (128-byte
+//                 swizzled boxes, 4-stage ring) -> shared memory ->
+//                 tcgen05.mma.kind::i8 with the int32 accumulator in TMEM (two
+//                 256-column buffers) -> tcgen05.ld -> residue mod p -> uint8
+//                 rows in HBM.  Warp roles: 0 TMA producer, 1 TMEM owner + MMA
+//                 issuer, 2..5 epilogue (TMEM lane quarter = warp % 4);
 //   k_crt         per output element: sum the K-chunk residues mod p, CRT on
 //                 <= 41-bit chunks in FP64 (exact integer arithmetic), join the
 //                 chunks error-free (TwoSum), scale by 2^-(sa+sb), apply
@@ -351,7 +352,8 @@ constexpr int kThreads = 192;
 constexpr unsigned long long kWaitLimitNs = 4000000000ULL;  // 4 s
 
 struct MmaArgs {
-  int tiles_j, L, splits, nbatch, nbo1;
+  int tiles_j, tiles_i, L, splits, nbatch, nbo1;
+  long long n_items;
   int a_var1, a_var2, b_var1, b_var2;  // operand planes vary with bo1 / bo2
   int planes_a, planes_b;
   long long m_pad, n_pad;
@@ -474,8 +476,45 @@ __device__ __forceinline__ uint32_t mod_u32(uint32_t u, uint32_t p, uint32_t bar
   return r >= p ? r - p : r;
 }
 
+// One work item = one 128 x 256 output tile of one modulus, one K chunk and
+// one batch; items are numbered tile fastest, then modulus, K chunk, batch.
+struct WorkItem {
+  int tj, ti, l, split, b, kb0, nkb, yj, yi;
+};
+
+__device__ __forceinline__ WorkItem decode_item(const MmaArgs& a, long long w) {
+  WorkItem it;
+  const long long tiles = static_cast<long long>(a.tiles_j) * a.tiles_i;
+  const long long tile = w % tiles;
+  long long rest = w / tiles;
+  it.tj = static_cast<int>(tile % a.tiles_j);
+  it.ti = static_cast<int>(tile / a.tiles_j);
+  it.l = static_cast<int>(rest % a.L);
+  rest /= a.L;
+  it.split = static_cast<int>(rest % a.splits);
+  it.b = static_cast<int>(rest / a.splits);
+  const int b1 = it.b % a.nbo1, b2 = it.b / a.nbo1;
+  const int pa = (a.a_var1 ? b1 : 0) + (a.a_var1 ? a.nbo1 : 1) * (a.a_var2 ? b2 : 0);
+  const int pb = (a.b_var1 ? b1 : 0) + (a.b_var1 ? a.nbo1 : 1) * (a.b_var2 ? b2 : 0);
+  it.kb0 = it.split * a.kb_per_split;
+  it.nkb = min(a.kb_per_split, a.kb_total - it.kb0);
+  // residue rows: ((plane * tiles + tile) * L + l) * tile_rows + row in tile
+  it.yj = static_cast<int>(
+      ((static_cast<long long>(pb) * (a.n_pad / kTileJ) + it.tj) * a.L + it.l) * kTileJ);
+  it.yi = static_cast<int>(
+      ((static_cast<long long>(pa) * (a.m_pad / kTileI) + it.ti) * a.L + it.l) * kTileI);
+  return it;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Persistent: one CTA per SM walks the work items blockIdx.x, + gridDim.x, ...
+// through a STAGES-deep TMA ring; two TMEM accumulators (2 x 256 columns) let
+// the epilogue of one item overlap the MMAs of the next.
 template <int STAGES>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, 1)
     k_i8_mma(const __grid_constant__ CUtensorMap tm_j, const __grid_constant__ CUtensorMap tm_i,
              const MmaArgs a) {
   extern __shared__ uint8_t smem_raw[];
@@ -486,31 +525,21 @@ __global__ void __launch_bounds__(kThreads, 2)
   uint64_t* bars = reinterpret_cast<uint64_t*>(si + STAGES * kBytesI);
   uint64_t* full = bars;
   uint64_t* empty = bars + STAGES;
-  uint64_t* acc_full = bars + 2 * STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 1);
+  uint64_t* acc_full = bars + 2 * STAGES;       // [2]
+  uint64_t* acc_empty = bars + 2 * STAGES + 2;  // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 4);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int tj = blockIdx.x % a.tiles_j, ti = blockIdx.x / a.tiles_j;
-  const int l = blockIdx.y;
-  const int split = blockIdx.z % a.splits, b = blockIdx.z / a.splits;
-  const int b1 = b % a.nbo1, b2 = b / a.nbo1;
-  const int pa = (a.a_var1 ? b1 : 0) + (a.a_var1 ? a.nbo1 : 1) * (a.a_var2 ? b2 : 0);
-  const int pb = (a.b_var1 ? b1 : 0) + (a.b_var1 ? a.nbo1 : 1) * (a.b_var2 ? b2 : 0);
-  const int kb0 = split * a.kb_per_split;
-  const int nkb = min(a.kb_per_split, a.kb_total - kb0);
-  // residue rows: ((plane * tiles + tile) * L + l) * tile_rows + row in tile
-  const int yj = static_cast<int>(
-      ((static_cast<long long>(pb) * (a.n_pad / kTileJ) + tj) * a.L + l) * kTileJ);
-  const int yi = static_cast<int>(
-      ((static_cast<long long>(pa) * (a.m_pad / kTileI) + ti) * a.L + l) * kTileI);
-
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(smem_u32(&full[s]), 1);
       mbar_init(smem_u32(&empty[s]), 1);
     }
-    mbar_init(smem_u32(acc_full), 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&acc_full[b]), 1);
+      mbar_init(smem_u32(&acc_empty[b]), 4);  // one arrival per epilogue warp
+    }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -518,7 +547,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
-                 "r"(static_cast<uint32_t>(kTileI))
+                 "r"(static_cast<uint32_t>(2 * kTileI))
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -529,75 +558,110 @@ __global__ void __launch_bounds__(kThreads, 2)
 
   if (warp == 0 && lane == 0) {
     // ---- TMA producer
-    int issued = 0;
-    for (int kb = 0; kb < nkb; ++kb) {
-      const int s = kb % STAGES;
-      const uint32_t ph = (kb / STAGES) & 1;
-      if (!mbar_wait(smem_u32(&empty[s]), ph ^ 1, abort_flag, a.err, 1)) break;
-      const uint32_t fb = smem_u32(&full[s]);
-      mbar_expect_tx(fb, kBytesJ + kBytesI);
-      const int x = (kb0 + kb) * kTileK;
-      tma_load_2d(smem_u32(sj + s * kBytesJ), &tm_j, x, yj, fb);
-      tma_load_2d(smem_u32(si + s * kBytesI), &tm_i, x, yi, fb);
-      ++issued;
+    long long pos = 0;  // ring position, continued across items
+    bool ok = true;
+    for (long long w = blockIdx.x; ok && w < a.n_items; w += gridDim.x) {
+      const WorkItem it = decode_item(a, w);
+      for (int kb = 0; kb < it.nkb; ++kb) {
+        const int s = static_cast<int>(pos % STAGES);
+        const uint32_t ph = static_cast<uint32_t>(pos / STAGES) & 1;
+        if (!mbar_wait(smem_u32(&empty[s]), ph ^ 1, abort_flag, a.err, 1)) {
+          ok = false;
+          break;
+        }
+        const uint32_t fb = smem_u32(&full[s]);
+        mbar_expect_tx(fb, kBytesJ + kBytesI);
+        const int x = (it.kb0 + kb) * kTileK;
+        tma_load_2d(smem_u32(sj + s * kBytesJ), &tm_j, x, it.yj, fb);
+        tma_load_2d(smem_u32(si + s * kBytesI), &tm_i, x, it.yi, fb);
+        ++pos;
+      }
     }
-    if (*abort_flag) {
+    if (!ok) {
       // let the copies already issued land before the CTA exits
-      for (int kb = max(0, issued - STAGES); kb < issued; ++kb)
-        (void)mbar_wait(smem_u32(&full[kb % STAGES]), (kb / STAGES) & 1, abort_flag, a.err, 1);
+      for (long long q = pos > STAGES ? pos - STAGES : 0; q < pos; ++q)
+        (void)mbar_wait(smem_u32(&full[q % STAGES]), static_cast<uint32_t>(q / STAGES) & 1,
+                        abort_flag, a.err, 1);
     }
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer
-    for (int kb = 0; kb < nkb; ++kb) {
-      const int s = kb % STAGES;
-      const uint32_t ph = (kb / STAGES) & 1;
-      if (!mbar_wait(smem_u32(&full[s]), ph, abort_flag, a.err, 2)) break;
+    long long pos = 0;
+    int t = 0, last_buf = -1;
+    uint32_t last_use = 0;
+    for (long long w = blockIdx.x; w < a.n_items; w += gridDim.x, ++t) {
+      const WorkItem it = decode_item(a, w);
+      const int buf = t & 1;
+      const uint32_t use = static_cast<uint32_t>(t >> 1);
+      if (!mbar_wait(smem_u32(&acc_empty[buf]), (use & 1) ^ 1, abort_flag, a.err, 2)) break;
       tc_fence_after();
-      const uint64_t dj = sw128_desc(smem_u32(sj + s * kBytesJ));
-      const uint64_t di = sw128_desc(smem_u32(si + s * kBytesI));
+      const uint32_t d = tmem + static_cast<uint32_t>(buf * kTileI);
+      bool ok = true;
+      for (int kb = 0; kb < it.nkb; ++kb) {
+        const int s = static_cast<int>(pos % STAGES);
+        const uint32_t ph = static_cast<uint32_t>(pos / STAGES) & 1;
+        if (!mbar_wait(smem_u32(&full[s]), ph, abort_flag, a.err, 2)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint64_t dj = sw128_desc(smem_u32(sj + s * kBytesJ));
+        const uint64_t di = sw128_desc(smem_u32(si + s * kBytesI));
 #pragma unroll
-      for (int kk = 0; kk < kTileK / kMmaK; ++kk) {
-        // advance along K inside the swizzle row: +32 bytes = +2 in the
-        // 16-byte address field
-        mma_i8(tmem, dj + 2 * kk, di + 2 * kk, (kb | kk) != 0);
+        for (int kk = 0; kk < kTileK / kMmaK; ++kk) {
+          // advance along K inside the swizzle row: +32 bytes = +2 in the
+          // 16-byte address field
+          mma_i8(d, dj + 2 * kk, di + 2 * kk, (kb | kk) != 0);
+        }
+        mma_commit(smem_u32(&empty[s]));
+        ++pos;
       }
-      mma_commit(smem_u32(&empty[s]));
+      mma_commit(smem_u32(&acc_full[buf]));  // also on failure, so the epilogue wakes
+      last_buf = buf;
+      last_use = use;
+      if (!ok) break;
     }
-    mma_commit(smem_u32(acc_full));
+    if (last_buf >= 0)  // every MMA of this CTA has completed before TMEM is released
+      (void)mbar_wait(smem_u32(&acc_full[last_buf]), last_use & 1, abort_flag, a.err, 4);
   } else if (warp >= 2) {
-    // ---- epilogue: TMEM -> residues mod p -> uint8 plane
+    // ---- epilogue: TMEM -> residues mod p -> uint8 rows
     const int q = warp & 3;  // TMEM lane quarter this warp may access
-    // warp-uniform, so that the .sync.aligned TMEM loads below are convergent
-    const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(acc_full), 0, abort_flag, a.err, 3));
-    tc_fence_after();
-    if (ok && nkb > 0) {
-      const uint32_t p = a.p[l], bm = a.barrett[l], off = a.off[l];
-      const long long j = static_cast<long long>(tj) * kTileJ + q * 32 + lane;
-      uint8_t* rowp = a.R + residue_offset(a, split, b, j, l) + static_cast<long long>(ti) * kTileI;
+    int t = 0;
+    for (long long w = blockIdx.x; w < a.n_items; w += gridDim.x, ++t) {
+      const WorkItem it = decode_item(a, w);
+      const int buf = t & 1;
+      const uint32_t use = static_cast<uint32_t>(t >> 1);
+      // warp-uniform, so that the .sync.aligned TMEM loads below are convergent
+      const bool ok =
+          __all_sync(0xffffffffu, mbar_wait(smem_u32(&acc_full[buf]), use & 1, abort_flag, a.err, 3));
+      tc_fence_after();
+      if (!ok) break;
+      const uint32_t p = a.p[it.l], bm = a.barrett[it.l], off = a.off[it.l];
+      const long long j = static_cast<long long>(it.tj) * kTileJ + q * 32 + lane;
+      uint8_t* rowp = a.R + residue_offset(a, it.split, it.b, j, it.l) +
+                      static_cast<long long>(it.ti) * kTileI;
+      const uint32_t tq = tmem + static_cast<uint32_t>(buf * kTileI) +
+                          (static_cast<uint32_t>(q * 32) << 16);
 #pragma unroll 1
       for (int c = 0; c < kTileI / 32; ++c) {
         uint32_t v[32];
-        UW12_TMEM_LD32(tmem + (static_cast<uint32_t>(q * 32) << 16) + c * 32, v);
+        UW12_TMEM_LD32(tq + c * 32, v);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        uint32_t w[8];
+        uint32_t wd[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
           uint32_t word = 0;
 #pragma unroll
-          for (int t = 0; t < 4; ++t)
-            word |= mod_u32(v[4 * e + t] + off, p, bm) << (8 * t);
-          w[e] = word;
+          for (int u = 0; u < 4; ++u) word |= mod_u32(v[4 * e + u] + off, p, bm) << (8 * u);
+          wd[e] = word;
         }
         uint4* dst = reinterpret_cast<uint4*>(rowp + c * 32);
-        dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
-        dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+        dst[0] = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+        dst[1] = make_uint4(wd[4], wd[5], wd[6], wd[7]);
       }
-    } else if (nkb == 0) {
-      // empty K chunk: residue 0
-      const long long j = static_cast<long long>(tj) * kTileJ + q * 32 + lane;
-      uint4* dst = reinterpret_cast<uint4*>(a.R + residue_offset(a, split, b, j, l) +
-                                            static_cast<long long>(ti) * kTileI);
-      for (int c = 0; c < kTileI / 16; ++c) dst[c] = make_uint4(0, 0, 0, 0);
+      // this warp's TMEM reads are done: release the accumulator
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&acc_empty[buf]));
     }
   }
 
@@ -605,13 +669,9 @@ __global__ void __launch_bounds__(kThreads, 2)
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    if (lane == 0) {
-      // all MMAs of this CTA have completed before TMEM is released
-      (void)mbar_wait(smem_u32(acc_full), 0, abort_flag, a.err, 4);
-    }
     __syncwarp();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(static_cast<uint32_t>(kTileI))
+                 "r"(static_cast<uint32_t>(2 * kTileI))
                  : "memory");
   }
 }
@@ -832,11 +892,19 @@ CUtensorMap make_map(const uint8_t* base, long long rows, long long k_pad, int b
   return m;
 }
 
-constexpr int kStages = 2;  // 2 CTAs per SM (96 KiB of stages each, 2 x 256 TMEM columns)
+constexpr int kStages = 4;  // 192 KiB of stages: one persistent CTA per SM, 512 TMEM columns
 constexpr size_t kMmaSmem =
     size_t(kStages) * (kBytesJ + kBytesI) + 1024 /*alignment*/ + 256 /*barriers*/;
 
 long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
+
+int num_sms() {
+  static int n[64] = {};
+  int dev = 0;
+  UW12_CUDA(cudaGetDevice(&dev));
+  if (!n[dev]) UW12_CUDA(cudaDeviceGetAttribute(&n[dev], cudaDevAttrMultiProcessorCount, dev));
+  return n[dev];
+}
 
 struct Timer {
   int kind;
@@ -879,7 +947,7 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
   const long long tiles_j = n_pad / kTileJ, tiles_i = m_pad / kTileI;
   const long long ctas = tiles_j * tiles_i * L * nbatch;
   long long splits = (k_pad + kMaxKChunk - 1) / kMaxKChunk;
-  const long long want = (2 * 148 * 2 + ctas - 1) / ctas;
+  const long long want = (2 * num_sms() + ctas - 1) / ctas;
   splits = std::max(splits, std::min(want, std::max<long long>(1, kb_total / 8)));
   splits = std::min(splits, std::max<long long>(1, 65535 / nbatch));
   long long kb_per = (kb_total + splits - 1) / splits;
@@ -963,6 +1031,8 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
     const CUtensorMap tmi = make_map(ra, L * planes_a * m_pad, k_pad, kTileI);
     MmaArgs ma{};
     ma.tiles_j = static_cast<int>(tiles_j);
+    ma.tiles_i = static_cast<int>(tiles_i);
+    ma.n_items = tiles_j * tiles_i * L * splits * nbatch;
     ma.L = L;
     ma.splits = static_cast<int>(splits);
     ma.nbatch = static_cast<int>(nbatch);
@@ -986,8 +1056,7 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
     std::snprintf(shape, sizeof(shape), "i8 %lld %lld %lld %lld L%d s%lld", d.m, d.n, k_total,
                   nbatch, L, splits);
     Timer tm(kProfI8Mma, ops, shape, s);
-    dim3 grid(static_cast<unsigned>(tiles_j * tiles_i), static_cast<unsigned>(L),
-              static_cast<unsigned>(splits * nbatch));
+    const unsigned grid = static_cast<unsigned>(std::min<long long>(ma.n_items, num_sms()));
     k_i8_mma<kStages><<<grid, kThreads, kMmaSmem, s>>>(tmj, tmi, ma);
     UW12_LAUNCHED();
     tm.stop();
