@@ -288,6 +288,33 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def int8_peak_tops(device):
+    """Dense int8 tensor-core throughput of a library GEMM (torch._int_mm,
+    8192^3, best of 5), the roofline denominator of the split-precision int8
+    kernel; (value, source)."""
+    import torch
+    n = 8192
+    try:
+        a = torch.randint(-128, 127, (n, n), dtype=torch.int8, device=device)
+        b = torch.randint(-128, 127, (n, n), dtype=torch.int8, device=device)
+        for _ in range(2):
+            torch._int_mm(a, b)
+        best = 1e30
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        del a, b
+        torch.cuda.empty_cache()
+        return 2.0 * n ** 3 / best / 1e12, "torch._int_mm int8 8192^3 burst measured in this run"
+    except Exception as exc:  # no int8 library GEMM: twice the measured bf16 peak
+        peaks = json.loads((Path(__file__).parent / "MEASURED_PEAKS.json").read_text())
+        return 2.0 * peaks["bf16_tflops"], f"2 x MEASURED_PEAKS bf16 burst ({type(exc).__name__})"
+
+
 def config_dict(args):
     N, M, R, occ, Ld = CONFIGS[args.config]
     return {"workload": f"uw12 energy+Fock {args.config}: N={N} AO, M={M} DF, R={R} RI, "
@@ -313,6 +340,9 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--split-moduli", default="14,10",
+                    help="moduli counts of the split-precision runs reported beside the FP64 "
+                         "headline ('' = none)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -394,6 +424,62 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         elapsed = float(tt.item())
     s_per_eval = elapsed / args.steps
+
+    # ---- split precision (int8 tensor-core GEMMs), same workload and timing
+    split = []
+    moduli = [int(x) for x in args.split_moduli.split(",") if x.strip()]
+    if moduli:
+        fock64 = fock_dev.clone()
+        i8_peak, i8_src = int8_peak_tops(device)
+        for Lm in moduli:
+            L.set_precision(Lm)
+            for _ in range(max(1, args.warmup - 1)):
+                e_split = step()
+            torch.cuda.synchronize(device)
+            L.profile_enable(True)
+            for kind in L.PROFILE_KINDS:
+                L.profile_read_kind(kind)
+            L.profile_phases()
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize(device)
+            sv0, sv1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            sv0.record(stream)
+            for _ in range(args.steps):
+                e_split = step()
+            sv1.record(stream)
+            torch.cuda.synchronize(device)
+            kinds = {k: L.profile_read_kind(k) for k in L.PROFILE_KINDS}
+            L.profile_phases()
+            L.profile_enable(False)
+            L.set_precision(0)
+            t_split = sv0.elapsed_time(sv1) / 1e3
+            if world > 1:
+                tt = torch.tensor([t_split], dtype=torch.float64, device=device)
+                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+                t_split = float(tt.item())
+            t_split /= args.steps
+            i8 = kinds["i8_mma"]
+            i8_tops = i8["work"] / (i8["ms"] / 1e3) / 1e12 if i8["ms"] else None
+            split.append({
+                "n_moduli": Lm, "bits_per_element_k1500": L.split_bits(Lm, 1500),
+                "s_per_eval": t_split, "speedup_vs_fp64": s_per_eval / t_split,
+                "energy": e_split, "energy_abs_err_vs_fp64_Eh": abs(e_split - energy),
+                "energy_rel_err_vs_fp64": abs(e_split - energy) / abs(energy),
+                "fock_max_rel_err_vs_fp64": float((fock_dev - fock64).abs().max() /
+                                                  fock64.abs().max()),
+                "ms_per_step": {"split_gemms": kinds["split_gemm"]["ms"] / args.steps,
+                                "i8_mma": i8["ms"] / args.steps,
+                                "operand_prep": kinds["split_prep"]["ms"] / args.steps,
+                                "crt": kinds["split_crt"]["ms"] / args.steps,
+                                "fp64_dmma_gemms": kinds["dgemm"]["ms"] / args.steps},
+                "roofline_i8_mma": {"bound": "tensor", "kernel": "k_i8_mma (tcgen05.mma kind::i8)",
+                                    "achieved": i8_tops, "peak": i8_peak, "unit": "TOPS",
+                                    "frac": i8_tops / i8_peak if i8_tops else None,
+                                    "peak_source": i8_src},
+            })
+        fock_dev.copy_(fock64)
+        del fock64
 
     # ---- end to end through the C-ABI from pinned host buffers
     e2e = None
@@ -493,6 +579,7 @@ def main():
             "phases_ms_per_step": phases,
             "gpu_launches": int(launches),
             "clocks": clk,
+            "split_precision": split,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -1232,8 +1232,11 @@ void gemm_ozaki(const GemmDesc& d, int n_moduli) {
                                  std::to_string(k_total) + " terms");
   cudaStream_t s = current_stream();
   const Consts& cs = consts_for(n_moduli);
+  char shape[160];
+  std::snprintf(shape, sizeof(shape), "split %lld %lld %lld %lld %lld L%d", d.m, d.n, d.k,
+                d.nbo1 * d.nbo2, d.nbr1 * d.nbr2, n_moduli);
   Timer tm(kProfSplitGemm,
-           2.0 * double(d.m) * double(d.n) * double(k_total) * double(d.nbo1 * d.nbo2), "split",
+           2.0 * double(d.m) * double(d.n) * double(k_total) * double(d.nbo1 * d.nbo2), shape,
            s);
   run_slabs(d, cs, beta, s);
   tm.stop();
