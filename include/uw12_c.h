@@ -90,6 +90,28 @@ int uw12c_form_fock(const uw12c_integrals* W, const uw12c_integrals* V,
                     double scale_same_spin, size_t print_level, double* energy, double* terms,
                     double* fock, int fock_mem_kind);
 
+/* Reverse mode of the direct terms (no counterpart in libuw12): with
+ * indirect_term = 0 (the opposite-spin form of uw12_energy, scale_same_spin
+ * entering only the direct same-spin pairs) the energy, terms and Fock
+ * (dE/dD, as uw12c_form_fock) plus the gradient of the energy with respect to
+ * the stored integrals:
+ *   dE_dX3[3]    W, V, WV: packed n_ao(n_ao+1)/2 x n_df, entry (mn|P) of the
+ *                packed storage (both triangle halves of sq(X3[:,P]) summed);
+ *   dE_dX3_ri[2] W, V: (n_ri n_ao) x n_df, the X3_ri layout;
+ *   dE_dX2[3]    W, V, WV: n_df x n_df symmetric (-J2^-1 G J2^-1; exact while
+ *                no metric eigenvalue is below the 1e-10 pseudo-inverse cut).
+ * Any array, or any of its entries, may be NULL (that gradient is skipped);
+ * grad_mem_kind says where the gradient buffers live.  The intermediates of the
+ * forward pass are recomputed, not kept between calls. */
+int uw12c_fock_backward(const uw12c_integrals* W, const uw12c_integrals* V,
+                        const uw12c_integrals* WV, const uw12c_abs* abs, size_t n_ao,
+                        size_t n_spin, const double* const* C, const size_t* ldc,
+                        const size_t* n_orb, const double* const* occ, const size_t* n_occ,
+                        const size_t* n_active, double scale_opp_spin, double scale_same_spin,
+                        double* energy, double* terms, double* fock, int fock_mem_kind,
+                        double* const* dE_dX3, double* const* dE_dX3_ri, double* const* dE_dX2,
+                        int grad_mem_kind);
+
 /* Replaces uw12::uw12_fock(double* fock, ...) (libuw12.hpp:157-169,
  * libuw12.cpp:184-214) in its raw-pointer form: C is the setup_orbitals
  * buffer (n_ao x n_orb*n_spin), occ the setup_occupations buffer

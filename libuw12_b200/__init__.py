@@ -86,6 +86,10 @@ def lib():
                                   c_d, c_sz, PD, PD, P, ctypes.c_int]
     L.uw12c_fock.argtypes = [P, P, P, P, P, P, c_sz, c_sz, c_sz, P, c_sz, c_sz, PSZ, c_d, c_d,
                              c_sz, PD]
+    L.uw12c_fock_backward.argtypes = [P, P, P, P, c_sz, c_sz, ctypes.POINTER(P), PSZ, PSZ,
+                                      ctypes.POINTER(P), PSZ, PSZ, c_d, c_d, PD, PD, P,
+                                      ctypes.c_int, ctypes.POINTER(P), ctypes.POINTER(P),
+                                      ctypes.POINTER(P), ctypes.c_int]
     L.uw12c_energy.argtypes = [P, P, P, P, P, c_sz, c_sz, c_sz, P, c_sz, c_sz, PSZ, c_d, c_d,
                                c_sz, PD]
     L.uw12c_set_stream.argtypes = [P]
@@ -356,6 +360,67 @@ def form_fock(W: BaseIntegrals, V: BaseIntegrals, WV: BaseIntegrals, abs_p: ABSP
     if fock is not None:
         focks = [np.array(fock[:, s * n_ao:(s + 1) * n_ao]) for s in range(n_spin)]
     return energy.value, focks, (terms[0], terms[1], terms[2])
+
+
+GRADIENT_NAMES = ("W3", "V3", "WV3", "W3_ri", "V3_ri", "W2", "V2", "WV2")
+
+
+def fock_backward(W: BaseIntegrals, V: BaseIntegrals, WV: BaseIntegrals, abs_p: ABSProjectors,
+                  orbitals: Sequence[np.ndarray], occupations: Sequence[np.ndarray],
+                  n_active: Sequence[int], scale_opp_spin: float, scale_same_spin: float,
+                  gradients: Sequence[str] = GRADIENT_NAMES, calculate_fock: bool = True,
+                  device_out: Optional[dict] = None):
+    """Reverse mode of the direct terms (``uw12c_fock_backward``).
+
+    Returns ``(energy, fock, (E2, E3, E4), grads)``: the energy, per-spin Fock
+    and terms of ``form_fock(..., indirect_term=False)`` and a dict of the
+    requested gradients of that energy with respect to the stored integrals
+    ("W3", "V3", "WV3" packed n_ao(n_ao+1)/2 x n_df; "W3_ri", "V3_ri"
+    (n_ri n_ao) x n_df; "W2", "V2", "WV2" n_df x n_df).  With ``device_out``
+    (name -> device pointer) the gradients are written to device memory and
+    the dict is empty.
+    """
+    n_spin = len(orbitals)
+    if n_spin < 1 or n_spin > 2 or len(occupations) != n_spin or len(n_active) != n_spin:
+        raise UW12LogicError("invalid number of spin channels")
+    n_ao = W.n_ao
+    Cs = [np.asfortranarray(np.asarray(c, dtype=np.float64)) for c in orbitals]
+    occs = [np.ascontiguousarray(np.asarray(o, dtype=np.float64).reshape(-1)) for o in occupations]
+    P = ctypes.c_void_p
+    c_ptrs = (P * n_spin)(*[_fptr(c) for c in Cs])
+    ldc = (ctypes.c_size_t * n_spin)(*[max(1, c.shape[0]) for c in Cs])
+    norb = (ctypes.c_size_t * n_spin)(*[c.shape[1] for c in Cs])
+    o_ptrs = (P * n_spin)(*[_fptr(o) for o in occs])
+    nocc = (ctypes.c_size_t * n_spin)(*[o.size for o in occs])
+    nact = (ctypes.c_size_t * n_spin)(*[int(a) for a in n_active])
+    shapes = {"W3": (W.n_ao * (W.n_ao + 1) // 2, W.n_df), "V3": (V.n_ao * (V.n_ao + 1) // 2, V.n_df),
+              "WV3": (WV.n_ao * (WV.n_ao + 1) // 2, WV.n_df),
+              "W3_ri": (W.n_ri * W.n_ao, W.n_df), "V3_ri": (V.n_ri * V.n_ao, V.n_df),
+              "W2": (W.n_df, W.n_df), "V2": (V.n_df, V.n_df), "WV2": (WV.n_df, WV.n_df)}
+    grads, ptr = {}, {}
+    for name in GRADIENT_NAMES:
+        if device_out is not None:
+            ptr[name] = P(device_out[name]) if name in device_out else P(0)
+        elif name in gradients:
+            grads[name] = np.zeros(shapes[name], order="F")
+            ptr[name] = _fptr(grads[name])
+        else:
+            ptr[name] = P(0)
+    d3 = (P * 3)(ptr["W3"], ptr["V3"], ptr["WV3"])
+    d3ri = (P * 2)(ptr["W3_ri"], ptr["V3_ri"])
+    d2 = (P * 3)(ptr["W2"], ptr["V2"], ptr["WV2"])
+    energy = ctypes.c_double()
+    terms = (ctypes.c_double * 3)()
+    fock = np.zeros((n_ao, n_ao * n_spin), order="F") if calculate_fock else None
+    _check(lib().uw12c_fock_backward(W.handle, V.handle, WV.handle, abs_p.handle, n_ao, n_spin,
+                                     c_ptrs, ldc, norb, o_ptrs, nocc, nact, float(scale_opp_spin),
+                                     float(scale_same_spin), ctypes.byref(energy), terms,
+                                     _fptr(fock) if fock is not None else P(0), MEM_HOST, d3,
+                                     d3ri, d2, MEM_DEVICE if device_out is not None else MEM_HOST))
+    focks = None
+    if fock is not None:
+        focks = [np.array(fock[:, s * n_ao:(s + 1) * n_ao]) for s in range(n_spin)]
+    return energy.value, focks, (terms[0], terms[1], terms[2]), grads
 
 
 def uw12_fock(W, V, WV, abs_p, orbitals, occ, n_active, scale_opp_spin, scale_same_spin,

@@ -138,7 +138,7 @@ void run_form_fock(const uw12c_integrals* W, const uw12c_integrals* V, const uw1
                    const size_t* ldc, const size_t* n_orb, const double* const* occ,
                    const size_t* n_occ, const size_t* n_active, int indirect, int calc,
                    double s_os, double s_ss, size_t print_level, double* energy, double* terms,
-                   double* fock, int fock_mem) {
+                   double* fock, int fock_mem, const uw12b::AdjointOutputs* adjoint = nullptr) {
   need(W && V && WV && abs && W->h && V->h && WV->h && abs->h, "null handle");
   need(C && ldc && n_orb && occ && n_occ && n_active, "null orbital/occupation argument");
   need(fock_mem == UW12C_MEM_HOST || fock_mem == UW12C_MEM_DEVICE, "bad fock_mem_kind");
@@ -197,7 +197,10 @@ void run_form_fock(const uw12c_integrals* W, const uw12c_integrals* V, const uw1
   rq.shard = uw12b::g_shard;
   rq.n_shards = uw12b::g_n_shards;
   DeviceGuard dg(w.device);
-  uw12b::form_fock(rq);
+  if (adjoint)
+    uw12b::form_fock_adjoint(rq, *adjoint);
+  else
+    uw12b::form_fock(rq);
   check_split_pipeline();
 }
 
@@ -419,6 +422,31 @@ int uw12c_dgemm(long long m, long long n, long long k, double alpha, const doubl
     need(m >= 0 && n >= 0 && k >= 0 && nbo1 >= 0 && nbo2 >= 0 && nbr1 >= 0 && nbr2 >= 0,
          "negative size");
     uw12b::gemm(d);
+  });
+}
+
+int uw12c_fock_backward(const uw12c_integrals* W, const uw12c_integrals* V,
+                        const uw12c_integrals* WV, const uw12c_abs* abs, size_t n_ao,
+                        size_t n_spin, const double* const* C, const size_t* ldc,
+                        const size_t* n_orb, const double* const* occ, const size_t* n_occ,
+                        const size_t* n_active, double scale_opp_spin, double scale_same_spin,
+                        double* energy, double* terms, double* fock, int fock_mem_kind,
+                        double* const* dE_dX3, double* const* dE_dX3_ri, double* const* dE_dX2,
+                        int grad_mem_kind) {
+  return guarded([&] {
+    need(grad_mem_kind == UW12C_MEM_HOST || grad_mem_kind == UW12C_MEM_DEVICE,
+         "bad grad_mem_kind");
+    need(uw12b::g_n_shards == 1, "the adjoint evaluates unsharded (uw12c_set_shard(0, 1))");
+    uw12b::AdjointOutputs ad;
+    for (int i = 0; i < 3; ++i) {
+      ad.dJ3[i] = dE_dX3 ? dE_dX3[i] : nullptr;
+      ad.dJ2[i] = dE_dX2 ? dE_dX2[i] : nullptr;
+    }
+    for (int i = 0; i < 2; ++i) ad.dJ3_ri[i] = dE_dX3_ri ? dE_dX3_ri[i] : nullptr;
+    ad.device_mem = grad_mem_kind == UW12C_MEM_DEVICE;
+    run_form_fock(W, V, WV, abs, n_ao, n_spin, C, ldc, n_orb, occ, n_occ, n_active, 0,
+                  fock != nullptr, scale_opp_spin, scale_same_spin, 0, energy, terms, fock,
+                  fock_mem_kind, &ad);
   });
 }
 

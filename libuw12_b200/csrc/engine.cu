@@ -323,6 +323,48 @@ struct SpinDims {
   size_t o = 0, a = 0, c = 0, ooff = 0, aoff = 0;
 };
 
+// Occupation-weighted occupied orbitals Co (utils.hpp:289-310) of both spins side
+// by side (N x o_tot) and their active (last n_active) columns Ca (freeze_core,
+// utils.hpp:235-253; N x a_tot), on the device.
+void upload_orbitals(const FockRequest& rq, std::vector<SpinDims>& sd, size_t& o_tot,
+                     size_t& a_tot, DevBuf& Co, DevBuf& Ca) {
+  const int ns = rq.n_spin;
+  const size_t N = rq.n_ao;
+  cudaStream_t st = current_stream();
+  sd.assign(ns, SpinDims{});
+  o_tot = a_tot = 0;
+  for (int s = 0; s < ns; ++s) {
+    sd[s].o = rq.n_occ[s];
+    sd[s].a = rq.n_active[s];
+    sd[s].c = sd[s].o - sd[s].a;
+    sd[s].ooff = o_tot;
+    sd[s].aoff = a_tot;
+    o_tot += sd[s].o;
+    a_tot += sd[s].a;
+  }
+  Co.alloc(N * o_tot);
+  Ca.alloc(N * a_tot);
+  DevBuf wts(o_tot);
+  std::vector<double> w(o_tot);
+  const double per = (ns == 1) ? 2.0 : 1.0;
+  for (int s = 0; s < ns; ++s)
+    for (size_t k = 0; k < sd[s].o; ++k) w[sd[s].ooff + k] = std::sqrt(rq.occ[s][k] / per);
+  if (o_tot)
+    UW12_CUDA(cudaMemcpyAsync(wts.get(), w.data(), o_tot * sizeof(double), cudaMemcpyHostToDevice,
+                              st));
+  for (int s = 0; s < ns; ++s) {
+    if (!sd[s].o) continue;
+    UW12_CUDA(cudaMemcpy2DAsync(Co.get() + N * sd[s].ooff, N * sizeof(double), rq.C[s],
+                                rq.ldc[s] * sizeof(double), N * sizeof(double), sd[s].o,
+                                cudaMemcpyHostToDevice, st));
+  }
+  if (o_tot) scale_rc(Co.get(), LL(N), LL(N), LL(o_tot), nullptr, wts.get(), 1.0, Co.get(), LL(N));
+  for (int s = 0; s < ns; ++s)
+    if (sd[s].a)
+      UW12_CUDA(cudaMemcpyAsync(Ca.get() + N * sd[s].aoff, Co.get() + N * (sd[s].ooff + sd[s].c),
+                                N * sd[s].a * sizeof(double), cudaMemcpyDeviceToDevice, st));
+}
+
 }  // namespace
 
 // --------------------------------------------------------------------------
@@ -357,43 +399,12 @@ void form_fock(const FockRequest& rq) {
     return std::make_pair(total * shard / n_shards, total * (shard + 1) / n_shards);
   };
 
-  std::vector<SpinDims> sd(ns);
+  std::vector<SpinDims> sd;
   size_t o_tot = 0, a_tot = 0;
-  for (int s = 0; s < ns; ++s) {
-    sd[s].o = rq.n_occ[s];
-    sd[s].a = rq.n_active[s];
-    sd[s].c = sd[s].o - sd[s].a;
-    sd[s].ooff = o_tot;
-    sd[s].aoff = a_tot;
-    o_tot += sd[s].o;
-    a_tot += sd[s].a;
-  }
-
   PhaseClock clock;
   clock.mark("orbitals");
-  // ---- occupation-weighted orbitals (utils.hpp:289-310), freeze_core (:235-253)
-  DevBuf Co(N * o_tot), Ca(N * a_tot), wts(o_tot);
-  {
-    std::vector<double> w(o_tot);
-    const double per = (ns == 1) ? 2.0 : 1.0;
-    for (int s = 0; s < ns; ++s)
-      for (size_t k = 0; k < sd[s].o; ++k) w[sd[s].ooff + k] = std::sqrt(rq.occ[s][k] / per);
-    if (o_tot)
-      UW12_CUDA(cudaMemcpyAsync(wts.get(), w.data(), o_tot * sizeof(double),
-                                cudaMemcpyHostToDevice, st));
-    for (int s = 0; s < ns; ++s) {
-      if (!sd[s].o) continue;
-      UW12_CUDA(cudaMemcpy2DAsync(Co.get() + N * sd[s].ooff, N * sizeof(double), rq.C[s],
-                                  rq.ldc[s] * sizeof(double), N * sizeof(double), sd[s].o,
-                                  cudaMemcpyHostToDevice, st));
-    }
-    if (o_tot) scale_rc(Co.get(), LL(N), LL(N), LL(o_tot), nullptr, wts.get(), 1.0, Co.get(), LL(N));
-    for (int s = 0; s < ns; ++s)
-      if (sd[s].a)
-        UW12_CUDA(cudaMemcpyAsync(Ca.get() + N * sd[s].aoff, Co.get() + N * (sd[s].ooff + sd[s].c),
-                                  N * sd[s].a * sizeof(double), cudaMemcpyDeviceToDevice, st));
-  }
-  auto Co_s = [&](int s) { return Co.get() + N * sd[s].ooff; };
+  DevBuf Co, Ca;
+  upload_orbitals(rq, sd, o_tot, a_tot, Co, Ca);
   auto Ca_s = [&](int s) { return Ca.get() + N * sd[s].aoff; };
 
   DevBuf acc(kSlots);
@@ -896,6 +907,361 @@ void form_fock(const FockRequest& rq) {
     res("Total UW12 energy", total);
     std::fflush(stdout);
   }
+}
+
+// --------------------------------------------------------------------------
+// reverse mode of the direct terms
+// --------------------------------------------------------------------------
+// Energy of the direct terms, with f = f(s, s') the spin factor
+// (four_electron_utils.cpp:9-30) and everything in the metric eigenbasis:
+//   E = sum_{s,s'} f [ 1/2 X_D[s] . (L_WV X_D[s'])        (two_electron.cpp:37-81)
+//                    + 1/2 < t~[s'], t[s] >               (four_electron.cpp:80-137)
+//                    - < X[s], t~[s'] > ]                 (direct_utils.cpp:136-157)
+// t = B2_W^T B2_V, t~ = L_W t L_V, X = Wst_W^T (I (x) S^-1) Wst_V.  Reverse sweep:
+//   tbar[s] = sum_s' f (1/2 t~[s'] + L_W (1/2 t[s'] - X[s']) L_V),
+//   Xbar[s] = -sum_s' f t~[s'];
+//   B2bar_W = B2_V tbar^T, B2bar_V = B2_W tbar; Wstbar_W = SV_V Xbar^T,
+//   Wstbar_V = SW_W Xbar (SW = (I (x) S^-1) Wst);
+//   B1bar = Ca B2bar (+ the AO rows of Wstbar), Bribar = the RI rows of Wstbar;
+//   B1bar_0 = B1bar P2^T, Bribar_0 = Bribar P2^T;
+//   dE/dJ3_0[:, A] = packed-symmetric sum of B1bar_0[:, A] Co^T (N x N per A),
+//   dE/dJ3_ri_0[:, A] = Bribar_0[:, A] Ca^T (R x N per A);
+//   dE/dJ3_0^WV = 1/2 n_spin lower(D, 2) (P2 Xbar_D)^T, Xbar_D[s] = sum_s' f L X_D[s'].
+// In the original aux basis E depends on each metric only through K = J2^-1
+// (e.g. <t~[s'], t[s]> = tr(T0[s']^T K_W T0[s] K_V)), so dE/dJ2 = -K (dE/dK) K,
+// which in the eigenbasis (Q = P2 L) reads
+//   dE/dJ2_W  = -sym(Q_W [sum_s 1/2 T_s L_V t[s]^T - X[s] L_V T_s^T] Q_W^T),
+//   dE/dJ2_V  = -sym(Q_V [sum_s 1/2 t[s]^T L_W T_s - T_s^T L_W X[s]] Q_V^T),
+//   dE/dJ2_WV = -1/2 sum_{s,s'} f (Q X_D[s]) (Q X_D[s'])^T,
+// with T_s = sum_s' f t[s'].
+void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
+  FockRequest rq = rq_in;
+  rq.indirect = false;
+  if (rq.n_shards > 1) throw Error(kErrInvalid, "the adjoint evaluates unsharded");
+  form_fock(rq);
+
+  const IntegralsHandle& W = *rq.W;
+  const IntegralsHandle& V = *rq.V;
+  const IntegralsHandle& WV = *rq.WV;
+  const AbsHandle& AB = *rq.abs;
+  const int ns = rq.n_spin;
+  const size_t N = rq.n_ao, np = packed_size(N);
+  const size_t MW = W.n_df, MV = V.n_df, MX = WV.n_df;
+  const size_t R = W.n_ri, Rp = N + R;
+  const double two = (ns == 1) ? 2.0 : 1.0;
+  cudaStream_t st = current_stream();
+  const size_t budget = auto_budget_doubles(rq.mem_budget);
+  double F[2][2] = {{0, 0}, {0, 0}};
+  for (int s = 0; s < ns; ++s)
+    for (int sp = 0; sp < ns; ++sp) F[s][sp] = spin_factor(ns, s, sp, rq.s_os, rq.s_ss);
+
+  std::vector<SpinDims> sd;
+  size_t o_tot = 0, a_tot = 0;
+  DevBuf Co, Ca;
+  upload_orbitals(rq, sd, o_tot, a_tot, Co, Ca);
+  auto Ca_s = [&](int s) { return Ca.get() + N * sd[s].aoff; };
+
+  // output targets: the caller's device buffers, or device staging for host outputs
+  std::vector<std::pair<DevBuf, double*>> staged;
+  auto target = [&](double* user, size_t n) -> double* {
+    if (!user) return nullptr;
+    if (out.device_mem) return user;
+    staged.emplace_back(DevBuf(n), user);
+    return staged.back().first.get();
+  };
+  double* gJ3[3] = {target(out.dJ3[0], np * MW), target(out.dJ3[1], np * MV),
+                    target(out.dJ3[2], np * MX)};
+  double* gJ3ri[2] = {target(out.dJ3_ri[0], R * N * MW), target(out.dJ3_ri[1], R * N * MV)};
+  double* gJ2[3] = {target(out.dJ2[0], MW * MW), target(out.dJ2[1], MV * MV),
+                    target(out.dJ2[2], MX * MX)};
+
+  // ---- forward intermediates (as in form_fock): B2, Wst, (I (x) S^-1) Wst per X, spin
+  struct PerX {
+    std::vector<DevBuf> B2, Wst, SW;
+  };
+  PerX XW, XV;
+  for (int which = 0; which < 2; ++which) {
+    const IntegralsHandle& X = which == 0 ? W : V;
+    PerX& P = which == 0 ? XW : XV;
+    const size_t M = X.n_df;
+    P.B2.resize(ns);
+    P.Wst.resize(ns);
+    P.SW.resize(ns);
+    DevBuf H(N * o_tot * M);
+    transform_ao(X, Co.get(), o_tot, H.get(), budget / 2);
+    DevBuf H2(R * a_tot * M);
+    if (a_tot) {
+      GemmDesc g = gemm_nn(LL(R), LL(a_tot), LL(N), 1.0, X.J3_ri_0.get(), LL(R), Ca.get(), LL(N),
+                           0.0, H2.get(), LL(R));
+      g.nbo1 = LL(M);
+      g.sAo1 = LL(R * N);
+      g.sCo1 = LL(R * a_tot);
+      gemm(g);
+    }
+    for (int s = 0; s < ns; ++s) {
+      const size_t o = sd[s].o, a = sd[s].a, c = sd[s].c;
+      if (!a) continue;
+      DevBuf B1(N * o * M);
+      gemm(gemm_nn(LL(N * o), LL(M), LL(M), 1.0, H.get() + N * sd[s].ooff, LL(N * o_tot),
+                   X.P2.get(), LL(M), 0.0, B1.get(), LL(N * o)));
+      P.B2[s].alloc(a * o * M);
+      GemmDesc g3 = gemm_nn(LL(a), LL(o * M), LL(N), 1.0, Ca_s(s), LL(N), B1.get(), LL(N), 0.0,
+                            P.B2[s].get(), LL(a));
+      g3.a_kcontig = true;
+      gemm(g3);
+      P.Wst[s].alloc(Rp * a * M);
+      copy3d(B1.get() + N * c, LL(N), LL(N * o), P.Wst[s].get(), LL(Rp), LL(Rp * a), LL(N),
+             LL(a), LL(M));
+      GemmDesc g2 = gemm_nn(LL(R), LL(M), LL(M), 1.0, H2.get() + R * sd[s].aoff, LL(R * a_tot),
+                            X.P2.get(), LL(M), 0.0, P.Wst[s].get() + N, LL(Rp * a));
+      g2.nbo1 = LL(a);
+      g2.sAo1 = LL(R);
+      g2.sCo1 = LL(Rp);
+      gemm(g2);
+      P.SW[s].alloc(Rp * a * M);
+      gemm(gemm_nn(LL(Rp), LL(a * M), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp), P.Wst[s].get(),
+                   LL(Rp), 0.0, P.SW[s].get(), LL(Rp)));
+    }
+  }
+  // X, t, t~ per spin (zero for a spin without active orbitals)
+  std::vector<DevBuf> Xab(ns), tab(ns), ttl(ns);
+  for (int s = 0; s < ns; ++s) {
+    const size_t o = sd[s].o, a = sd[s].a;
+    Xab[s].alloc(MW * MV);
+    tab[s].alloc(MW * MV);
+    ttl[s].alloc(MW * MV);
+    if (a == 0) {
+      Xab[s].zero();
+      tab[s].zero();
+      ttl[s].zero();
+      continue;
+    }
+    GemmDesc gx = gemm_nn(LL(MW), LL(MV), LL(Rp * a), 1.0, XW.Wst[s].get(), LL(Rp * a),
+                          XV.SW[s].get(), LL(Rp * a), 0.0, Xab[s].get(), LL(MW));
+    gx.a_kcontig = true;
+    gemm(gx);
+    GemmDesc gt = gemm_nn(LL(MW), LL(MV), LL(a * o), 1.0, XW.B2[s].get(), LL(a * o),
+                          XV.B2[s].get(), LL(a * o), 0.0, tab[s].get(), LL(MW));
+    gt.a_kcontig = true;
+    gemm(gt);
+    scale_rc(tab[s].get(), LL(MW), LL(MW), LL(MV), W.lam.get(), V.lam.get(), 1.0, ttl[s].get(),
+             LL(MW));
+  }
+
+  // ---- adjoints of t and X
+  std::vector<DevBuf> tbar(ns), Xbar(ns);
+  for (int s = 0; s < ns; ++s) {
+    const double* mats[6];
+    double coefs[6];
+    int scaled[6];
+    int nt = 0;
+    for (int sp = 0; sp < ns; ++sp) {
+      mats[nt] = ttl[sp].get(); coefs[nt] = 0.5 * F[s][sp]; scaled[nt++] = 0;
+      mats[nt] = tab[sp].get(); coefs[nt] = 0.5 * F[sp][s]; scaled[nt++] = 1;
+      mats[nt] = Xab[sp].get(); coefs[nt] = -F[sp][s]; scaled[nt++] = 1;
+    }
+    tbar[s].alloc(MW * MV);
+    lincomb(tbar[s].get(), LL(MW), LL(MV), nt, mats, coefs, scaled, W.lam.get(), V.lam.get());
+    nt = 0;
+    for (int sp = 0; sp < ns; ++sp) {
+      mats[nt] = ttl[sp].get(); coefs[nt] = -F[s][sp]; scaled[nt++] = 0;
+    }
+    Xbar[s].alloc(MW * MV);
+    lincomb(Xbar[s].get(), LL(MW), LL(MV), nt, mats, coefs, scaled, nullptr, nullptr);
+  }
+
+  // ---- dE/dJ3_0 and dE/dJ3_ri_0 of W and V
+  for (int which = 0; which < 2; ++which) {
+    const IntegralsHandle& X = which == 0 ? W : V;
+    const size_t M = X.n_df;
+    double* g3 = gJ3[which];
+    double* g3ri = gJ3ri[which];
+    if (!g3 && !g3ri) continue;
+    DevBuf Bb1(N * o_tot * M), Bbri(R * a_tot * M);
+    Bb1.zero();
+    for (int s = 0; s < ns; ++s) {
+      const size_t o = sd[s].o, a = sd[s].a, c = sd[s].c;
+      if (!a) continue;
+      // B2bar (a*o x M)
+      DevBuf B2b(a * o * M);
+      if (which == 0) {
+        GemmDesc g = gemm_nn(LL(a * o), LL(MW), LL(MV), 1.0, XV.B2[s].get(), LL(a * o),
+                             tbar[s].get(), LL(MW), 0.0, B2b.get(), LL(a * o));
+        g.b_ncontig = true;
+        gemm(g);
+      } else {
+        gemm(gemm_nn(LL(a * o), LL(MV), LL(MW), 1.0, XW.B2[s].get(), LL(a * o), tbar[s].get(),
+                     LL(MW), 0.0, B2b.get(), LL(a * o)));
+      }
+      // B1bar_A (N x o) = Ca_s B2bar_A, into the spin block of Bb1
+      GemmDesc g1 = gemm_nn(LL(N), LL(o), LL(a), 1.0, Ca_s(s), LL(N), B2b.get(), LL(a), 0.0,
+                            Bb1.get() + N * sd[s].ooff, LL(N));
+      g1.nbo1 = LL(M);
+      g1.sBo1 = LL(a * o);
+      g1.sCo1 = LL(N * o_tot);
+      gemm(g1);
+      // Wstbar (R'a x M)
+      DevBuf Wsb(Rp * a * M);
+      if (which == 0) {
+        GemmDesc g = gemm_nn(LL(Rp * a), LL(MW), LL(MV), 1.0, XV.SW[s].get(), LL(Rp * a),
+                             Xbar[s].get(), LL(MW), 0.0, Wsb.get(), LL(Rp * a));
+        g.b_ncontig = true;
+        gemm(g);
+      } else {
+        gemm(gemm_nn(LL(Rp * a), LL(MV), LL(MW), 1.0, XW.SW[s].get(), LL(Rp * a), Xbar[s].get(),
+                     LL(MW), 0.0, Wsb.get(), LL(Rp * a)));
+      }
+      // AO rows -> active orbitals of B1bar; RI rows -> Bribar
+      copy3d(Wsb.get(), LL(Rp), LL(Rp * a), Bb1.get() + N * (sd[s].ooff + c), LL(N),
+             LL(N * o_tot), LL(N), LL(a), LL(M), 1.0, 1.0);
+      copy3d(Wsb.get() + N, LL(Rp), LL(Rp * a), Bbri.get() + R * sd[s].aoff, LL(R),
+             LL(R * a_tot), LL(R), LL(a), LL(M));
+    }
+    if (g3) {
+      // B1bar_0 = B1bar P2^T, then per aux function the packed symmetric sum of B1bar_0 Co^T
+      DevBuf Bb10(N * o_tot * M);
+      GemmDesc gp = gemm_nn(LL(N * o_tot), LL(M), LL(M), 1.0, Bb1.get(), LL(N * o_tot),
+                            X.P2.get(), LL(M), 0.0, Bb10.get(), LL(N * o_tot));
+      gp.b_ncontig = true;
+      gemm(gp);
+      const size_t ac = std::max<size_t>(1, std::min(M, budget / (2 * N * N)));
+      DevBuf G(N * N * ac);
+      for (size_t a0 = 0; a0 < M; a0 += ac) {
+        const size_t na = std::min(ac, M - a0);
+        GemmDesc g = gemm_nn(LL(N), LL(N), LL(o_tot), 1.0, Bb10.get() + N * o_tot * a0, LL(N),
+                             Co.get(), LL(N), 0.0, G.get(), LL(N));
+        g.b_ncontig = true;
+        g.nbo1 = LL(na);
+        g.sAo1 = LL(N * o_tot);
+        g.sCo1 = LL(N * N);
+        gemm(g);
+        pack_sym_sum(G.get(), LL(N), LL(na), g3 + np * a0, LL(np));
+      }
+    }
+    if (g3ri) {
+      if (a_tot == 0) {
+        UW12_CUDA(cudaMemsetAsync(g3ri, 0, R * N * M * sizeof(double), st));
+      } else {
+        DevBuf Bbri0(R * a_tot * M);
+        GemmDesc gp = gemm_nn(LL(R * a_tot), LL(M), LL(M), 1.0, Bbri.get(), LL(R * a_tot),
+                              X.P2.get(), LL(M), 0.0, Bbri0.get(), LL(R * a_tot));
+        gp.b_ncontig = true;
+        gemm(gp);
+        GemmDesc g = gemm_nn(LL(R), LL(N), LL(a_tot), 1.0, Bbri0.get(), LL(R), Ca.get(), LL(N),
+                             0.0, g3ri, LL(R));
+        g.b_ncontig = true;
+        g.nbo1 = LL(M);
+        g.sAo1 = LL(R * a_tot);
+        g.sCo1 = LL(R * N);
+        gemm(g);
+      }
+    }
+  }
+
+  // ---- metric gradients of W and V: -sym(Q A Q^T), Q = P2 L
+  for (int which = 0; which < 2; ++which) {
+    double* g2 = gJ2[which];
+    if (!g2) continue;
+    const IntegralsHandle& X = which == 0 ? W : V;
+    const IntegralsHandle& Y = which == 0 ? V : W;  // the other potential
+    const size_t M = X.n_df;
+    DevBuf Amat(M * M), Ts(M * M), tmp(M * M);
+    Amat.zero();
+    for (int s = 0; s < ns; ++s) {
+      const double* mats[2];
+      double coefs[2];
+      for (int sp = 0; sp < ns; ++sp) {
+        mats[sp] = tab[sp].get();
+        coefs[sp] = F[s][sp];
+      }
+      lincomb(Ts.get(), LL(MW), LL(MV), ns, mats, coefs, nullptr, nullptr, nullptr);
+      if (which == 0) {
+        // A_W += 1/2 T_s L_V t[s]^T - X[s] L_V T_s^T
+        scale_rc(Ts.get(), LL(MW), LL(MW), LL(MV), nullptr, Y.lam.get(), 1.0, tmp.get(), LL(MW));
+        GemmDesc g = gemm_nn(LL(MW), LL(MW), LL(MV), 0.5, tmp.get(), LL(MW), tab[s].get(), LL(MW),
+                             1.0, Amat.get(), LL(MW));
+        g.b_ncontig = true;
+        gemm(g);
+        scale_rc(Xab[s].get(), LL(MW), LL(MW), LL(MV), nullptr, Y.lam.get(), 1.0, tmp.get(),
+                 LL(MW));
+        g = gemm_nn(LL(MW), LL(MW), LL(MV), -1.0, tmp.get(), LL(MW), Ts.get(), LL(MW), 1.0,
+                    Amat.get(), LL(MW));
+        g.b_ncontig = true;
+        gemm(g);
+      } else {
+        // A_V += 1/2 t[s]^T L_W T_s - T_s^T L_W X[s]
+        scale_rc(Ts.get(), LL(MW), LL(MW), LL(MV), Y.lam.get(), nullptr, 1.0, tmp.get(), LL(MW));
+        GemmDesc g = gemm_nn(LL(MV), LL(MV), LL(MW), 0.5, tab[s].get(), LL(MW), tmp.get(), LL(MW),
+                             1.0, Amat.get(), LL(MV));
+        g.a_kcontig = true;
+        gemm(g);
+        scale_rc(Xab[s].get(), LL(MW), LL(MW), LL(MV), Y.lam.get(), nullptr, 1.0, tmp.get(),
+                 LL(MW));
+        g = gemm_nn(LL(MV), LL(MV), LL(MW), -1.0, Ts.get(), LL(MW), tmp.get(), LL(MW), 1.0,
+                    Amat.get(), LL(MV));
+        g.a_kcontig = true;
+        gemm(g);
+      }
+    }
+    DevBuf Q(M * M), QA(M * M);
+    scale_rc(X.P2.get(), LL(M), LL(M), LL(M), nullptr, X.lam.get(), 1.0, Q.get(), LL(M));
+    gemm(gemm_nn(LL(M), LL(M), LL(M), 1.0, Q.get(), LL(M), Amat.get(), LL(M), 0.0, QA.get(),
+                 LL(M)));
+    GemmDesc g = gemm_nn(LL(M), LL(M), LL(M), -1.0, QA.get(), LL(M), Q.get(), LL(M), 0.0,
+                         tmp.get(), LL(M));
+    g.b_ncontig = true;
+    gemm(g);
+    symmetrise(tmp.get(), LL(M), LL(M), g2, LL(M));
+  }
+
+  // ---- WV: dE/dJ3_0 and dE/dJ2 through the fitted density
+  if (gJ3[2] || gJ2[2]) {
+    DevBuf dmat(np * ns), XDr(MX * ns), XD(MX * ns), XDb(MX * ns), vb(MX * ns);
+    for (int s = 0; s < ns; ++s)
+      pack_density(Ca_s(s), LL(N), LL(N), LL(sd[s].a), two, dmat.get() + np * s);
+    GemmDesc g = gemm_nn(LL(MX), ns, LL(np), 1.0, WV.J3_0.get(), LL(np), dmat.get(), LL(np), 0.0,
+                         XDr.get(), LL(MX));
+    g.a_kcontig = true;
+    gemm(g);
+    g = gemm_nn(LL(MX), ns, LL(MX), 0.5 * ns, WV.P2.get(), LL(MX), XDr.get(), LL(MX), 0.0,
+                XD.get(), LL(MX));
+    g.a_kcontig = true;
+    gemm(g);
+    double coef[4] = {0, 0, 0, 0};
+    for (int s = 0; s < ns; ++s)
+      for (int sp = 0; sp < ns; ++sp) coef[s * ns + sp] = F[s][sp];
+    if (gJ3[2]) {
+      // Xbar_D[s] = L sum_s' f X_D[s'];  dJ3 = 1/2 n_spin dmat (P2 Xbar_D)^T
+      combine_vecs(XD.get(), LL(MX), ns, coef, WV.lam.get(), XDb.get());
+      gemm(gemm_nn(LL(MX), ns, LL(MX), 1.0, WV.P2.get(), LL(MX), XDb.get(), LL(MX), 0.0, vb.get(),
+                   LL(MX)));
+      GemmDesc gd = gemm_nn(LL(np), LL(MX), ns, 0.5 * ns, dmat.get(), LL(np), vb.get(), LL(MX),
+                            0.0, gJ3[2], LL(np));
+      gd.b_ncontig = true;
+      gemm(gd);
+    }
+    if (gJ2[2]) {
+      // U = Q X_D = P2 (L X_D); dJ2 = -1/2 U (U F)^T
+      DevBuf LX(MX * ns), U(MX * ns), UF(MX * ns);
+      scale_rc(XD.get(), LL(MX), LL(MX), ns, WV.lam.get(), nullptr, 1.0, LX.get(), LL(MX));
+      gemm(gemm_nn(LL(MX), ns, LL(MX), 1.0, WV.P2.get(), LL(MX), LX.get(), LL(MX), 0.0, U.get(),
+                   LL(MX)));
+      for (int s = 0; s < ns; ++s) {
+        const double* mats[2] = {U.get(), U.get() + MX};
+        double coefs[2] = {F[s][0], ns > 1 ? F[s][1] : 0.0};
+        lincomb(UF.get() + MX * s, LL(MX), 1, ns, mats, coefs, nullptr, nullptr, nullptr);
+      }
+      GemmDesc gd = gemm_nn(LL(MX), LL(MX), ns, -0.5, U.get(), LL(MX), UF.get(), LL(MX), 0.0,
+                            gJ2[2], LL(MX));
+      gd.b_ncontig = true;
+      gemm(gd);
+    }
+  }
+
+  for (auto& sg : staged)
+    UW12_CUDA(cudaMemcpyAsync(sg.second, sg.first.get(), sg.first.size() * sizeof(double),
+                              cudaMemcpyDeviceToHost, st));
+  UW12_CUDA(cudaStreamSynchronize(st));
 }
 
 std::string phase_profile_read() {

@@ -85,6 +85,23 @@ struct FockRequest {
 
 void form_fock(const FockRequest& rq);
 
+// Reverse mode of the direct terms (form_fock with indirect_term = false):
+// the gradient of their energy with respect to the stored integrals.  Any
+// pointer may be null (that gradient is skipped); device or host memory per
+// device_mem.  Layouts are those of the inputs: dJ3 packed
+// n_ao(n_ao+1)/2 x n_df (both triangle halves of (mn|P) summed into the packed
+// entry), dJ3_ri (n_ri n_ao) x n_df, dJ2 n_df x n_df symmetric.  The metric
+// gradient is -J2^-1 G J2^-1 (no eigenvector derivatives), exact when no metric
+// eigenvalue falls below the pseudo-inverse cut-off (1e-10).  The energy and
+// Fock of rq (direct terms) are computed first.
+struct AdjointOutputs {
+  double* dJ3[3] = {nullptr, nullptr, nullptr};  // W, V, WV
+  double* dJ3_ri[2] = {nullptr, nullptr};        // W, V
+  double* dJ2[3] = {nullptr, nullptr, nullptr};  // W, V, WV
+  bool device_mem = false;
+};
+void form_fock_adjoint(const FockRequest& rq, const AdjointOutputs& out);
+
 // Device time per schedule phase accumulated while GEMM profiling is on
 // ("name=ms;..."); reading resets the accumulators.
 std::string phase_profile_read();

@@ -64,14 +64,16 @@ __global__ void k_scale_rc(const double* __restrict__ X, long long ldx, long lon
 
 __global__ void k_copy3d(const double* __restrict__ src, long long s1, long long s2, double* dst,
                          long long d1, long long d2, long long n0, long long n1, long long n2,
-                         double alpha) {
+                         double alpha, double beta) {
   const long long total = n0 * n1 * n2;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
        idx += (long long)gridDim.x * blockDim.x) {
     const long long i = idx % n0;
     const long long rest = idx / n0;
     const long long j = rest % n1, l = rest / n1;
-    dst[i + d1 * j + d2 * l] = alpha * src[i + s1 * j + s2 * l];
+    double* d = dst + i + d1 * j + d2 * l;
+    const double v = alpha * src[i + s1 * j + s2 * l];
+    *d = beta != 0.0 ? v + beta * *d : v;
   }
 }
 
@@ -238,6 +240,50 @@ __global__ void k_combine_vecs(const double* __restrict__ U, long long m, int ns
   }
 }
 
+struct LincombArgs {
+  const double* M[kMaxLincomb];
+  double coef[kMaxLincomb];
+  int scaled[kMaxLincomb];
+};
+
+__global__ void k_lincomb(double* Y, long long m, long long n, int nt, LincombArgs a,
+                          const double* __restrict__ r, const double* __restrict__ c) {
+  const long long total = m * n;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long i = idx % m, j = idx / m;
+    const double rc = (r ? r[i] : 1.0) * (c ? c[j] : 1.0);
+    double plain = 0.0, sc = 0.0;
+    for (int q = 0; q < nt; ++q) {
+      if (a.coef[q] == 0.0) continue;
+      if (a.scaled[q])
+        sc += a.coef[q] * a.M[q][idx];
+      else
+        plain += a.coef[q] * a.M[q][idx];
+    }
+    Y[idx] = plain + rc * sc;
+  }
+}
+
+// out[i(i+1)/2 + j, a] = G[i, j, a] + G[j, i, a] (j < i), G[i, i, a] (j = i):
+// the gradient of a function of sq(x) with respect to the packed x.
+__global__ void k_pack_sym_sum(const double* __restrict__ G, long long n, long long na,
+                               double* out, long long ldo) {
+  const long long np = n * (n + 1) / 2;
+  const long long total = np * na;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long p = idx % np, a = idx / np;
+    // row i of the packed index: i(i+1)/2 <= p < (i+1)(i+2)/2
+    long long i = static_cast<long long>((sqrt(8.0 * double(p) + 1.0) - 1.0) * 0.5);
+    while (i * (i + 1) / 2 > p) --i;
+    while ((i + 1) * (i + 2) / 2 <= p) ++i;
+    const long long j = p - i * (i + 1) / 2;
+    const double* g = G + n * n * a;
+    out[p + ldo * a] = (i == j) ? g[i + n * i] : g[i + n * j] + g[j + n * i];
+  }
+}
+
 __global__ void k_scale_pinv_cols(double* Q, long long n, const double* __restrict__ lam,
                                   double tol) {
   const long long total = n * n;
@@ -302,11 +348,11 @@ void scale_rc(const double* X, long long ldx, long long rows, long long cols, co
 }
 
 void copy3d(const double* src, long long s1, long long s2, double* dst, long long d1,
-            long long d2, long long n0, long long n1, long long n2, double alpha) {
+            long long d2, long long n0, long long n1, long long n2, double alpha, double beta) {
   const long long total = n0 * n1 * n2;
   if (total <= 0) return;
   k_copy3d<<<grid_for(total), kT, 0, current_stream()>>>(src, s1, s2, dst, d1, d2, n0, n1, n2,
-                                                          alpha);
+                                                          alpha, beta);
   UW12_LAUNCHED();
 }
 
@@ -384,6 +430,28 @@ void combine_vecs(const double* U, long long m, int ns, const double* coef, cons
   VecArgs a{};
   for (int q = 0; q < ns * ns; ++q) a.coef[q] = coef[q];
   k_combine_vecs<<<grid_for(m * ns), kT, 0, current_stream()>>>(U, m, ns, a, w, V);
+  UW12_LAUNCHED();
+}
+
+void lincomb(double* Y, long long m, long long n, int nt, const double* const* mats,
+             const double* coefs, const int* scaled, const double* r, const double* c) {
+  const long long total = m * n;
+  if (total <= 0) return;
+  if (nt > kMaxLincomb) throw Error(kErrInvalid, "lincomb: too many terms");
+  LincombArgs a{};
+  for (int q = 0; q < nt; ++q) {
+    a.M[q] = mats[q];
+    a.coef[q] = coefs[q];
+    a.scaled[q] = scaled ? scaled[q] : 0;
+  }
+  k_lincomb<<<grid_for(total), kT, 0, current_stream()>>>(Y, m, n, nt, a, r, c);
+  UW12_LAUNCHED();
+}
+
+void pack_sym_sum(const double* G, long long n, long long na, double* out, long long ldo) {
+  const long long total = n * (n + 1) / 2 * na;
+  if (total <= 0) return;
+  k_pack_sym_sum<<<grid_for(total), kT, 0, current_stream()>>>(G, n, na, out, ldo);
   UW12_LAUNCHED();
 }
 

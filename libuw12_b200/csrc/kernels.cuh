@@ -22,9 +22,11 @@ void pack_density(const double* C, long long ldc, long long n, long long nc, dou
 void scale_rc(const double* X, long long ldx, long long rows, long long cols, const double* r,
               const double* c, double alpha, double* Y, long long ldy);
 
-// 3-D strided copy / scale: dst[i + d1*j + d2*l] = alpha * src[i + s1*j + s2*l].
+// 3-D strided copy / scale: dst[i + d1*j + d2*l] = alpha * src[i + s1*j + s2*l]
+// (+ beta * dst when beta != 0).
 void copy3d(const double* src, long long s1, long long s2, double* dst, long long d1,
-            long long d2, long long n0, long long n1, long long n2, double alpha = 1.0);
+            long long d2, long long n0, long long n1, long long n2, double alpha = 1.0,
+            double beta = 0.0);
 
 // acc[slot] += coef * sum_{i<rows, j<cols} x[i + ldx*j] * y[i + ldy*j] * rw[i] * cw[j]
 // (rw / cw may be null).  Two-pass, fixed-order reduction.
@@ -60,6 +62,15 @@ void combine_vecs(const double* U, long long m, int ns, const double* coef, cons
 
 // P2 = Q * diag(pinv(lambda)) with |lambda| <= tol -> 0; in place on Q (n x n).
 void scale_pinv_cols(double* Q, long long n, const double* lambda, double tol);
+// Y (m x n, contiguous) = sum_q coef_q M_q, the terms with scaled_q != 0
+// multiplied elementwise by r_i c_j (r, c may be null); at most kMaxLincomb terms.
+constexpr int kMaxLincomb = 8;
+void lincomb(double* Y, long long m, long long n, int nt, const double* const* mats,
+             const double* coefs, const int* scaled, const double* r, const double* c);
+// Gradient with respect to packed symmetric storage: out[:, a] (ldo >= n(n+1)/2)
+// from the n x n matrices G[:, :, a] (consecutive, n*n apart), G_ij + G_ji off
+// the diagonal.
+void pack_sym_sum(const double* G, long long n, long long na, double* out, long long ldo);
 
 // A = I (n x n, column-major).
 void set_identity(double* A, long long n);

@@ -1,0 +1,150 @@
+"""CPU restatement of the adjoint of the direct UW12 terms (test infrastructure).
+
+libuw12 has no adjoint; this numpy version of the reverse sweep that the CUDA
+path implements is the checker for it, and is itself checked against central
+finite differences of the oracle energy (tests/test_adjoint_math.py).
+
+Energy of the direct terms (``form_fock(..., indirect_term=False)``), summed
+over spin pairs with the spin factor f(s, s'):
+    E2 = 1/2 f X_D[s] . (L_WV X_D[s'])          (two_electron.cpp:37-81)
+    E4 = 1/2 f < t~[s'], t[s] >                  (four_electron.cpp:80-137)
+    E3 = -f < X[s], t~[s'] >                     (direct_utils.cpp:136-157)
+with t = B2_W^T B2_V, t~ = L_W t L_V, X = Wst_W^T (I (x) S^-1) Wst_V in the
+metric eigenbasis.  In the original aux basis these depend on the metrics
+only through K = J2^-1, so dE/dJ2 = -K G K with G = dE/dK, which in the
+eigenbasis is a product of the M x M intermediates (no eigenvector
+derivatives); dE/dJ3 follows the transforms backwards with P2 fixed.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from oracle import uw12_oracle as O
+
+
+def spin_factor(ns, s, sp, s_os, s_ss):
+    return O.get_energy_spin_factor(ns, s, sp, s_os, s_ss)
+
+
+def direct_energy(W, V, WV, abs_p, orbitals, occ, n_active, s_os, s_ss):
+    """Energy of the direct terms through the oracle."""
+    return O.form_fock(W, V, WV, abs_p, orbitals, occ, n_active, False, False, s_os,
+                       s_ss).energy
+
+
+def _pack_sym_sum(G):
+    """Gradient on the packed lower triangle of a symmetric matrix: G[i,j] + G[j,i]
+    off the diagonal, G[i,i] on it; packed row i(i+1)/2 + j, j <= i."""
+    n = G.shape[0]
+    out = np.zeros(n * (n + 1) // 2)
+    for i in range(n):
+        for j in range(i + 1):
+            out[i * (i + 1) // 2 + j] = G[i, j] + (G[j, i] if i != j else 0.0)
+    return out
+
+
+def direct_adjoint(Wb, Vb, WVb, abs_p, orbitals, occ, n_active, s_os, s_ss):
+    """dE/d(J3_0, J3_ri_0, J2) of W, V and dE/d(J3_0, J2) of WV for the direct terms."""
+    ns = len(orbitals)
+    Co = O.occupation_weighted_orbitals(orbitals, occ)
+    Ca = O.freeze_core(Co, n_active)
+    W = O.Integrals(Wb, Co, Ca)
+    V = O.Integrals(Vb, Co, Ca)
+    WV = O.Integrals(WVb, Co, Ca)
+    N = Co[0].shape[0]
+    F = np.array([[spin_factor(ns, s, sp, s_os, s_ss) for sp in range(ns)] for s in range(ns)])
+    lw, lv, lx = W.df_vals, V.df_vals, WV.df_vals
+    Sinv = np.block([[abs_p.s_inv_ao_ao, abs_p.s_inv_ao_ri], [abs_p.s_inv_ri_ao, abs_p.s_inv_ri_ri]])
+    R = abs_p.s_inv_ri_ri.shape[0]
+    Rp = N + R
+
+    def stacked(X, s):
+        """Wst: per active orbital j, AO rows (B1 orbital c+j) then RI rows (Bri orbital j)."""
+        B1 = X.get_X3idx_one_trans()[s]
+        Bri = X.get_X3idx_one_trans_ri()[s]
+        o = Co[s].shape[1]
+        a = Ca[s].shape[1]
+        c = o - a
+        M = B1.shape[1]
+        out = np.zeros((Rp * a, M))
+        for j in range(a):
+            out[Rp * j:Rp * j + N] = B1[N * (c + j):N * (c + j + 1)]
+            out[Rp * j + N:Rp * (j + 1)] = Bri[R * j:R * (j + 1)]
+        return out
+
+    t = O.calculate_tab(W, V)
+    tt = O.calculate_ttilde(W, V, t)
+    Wst = [stacked(W, s) for s in range(ns)]
+    Vst = [stacked(V, s) for s in range(ns)]
+    Sop = [np.kron(np.eye(Ca[s].shape[1]), Sinv) for s in range(ns)]
+    X = [Wst[s].T @ Sop[s] @ Vst[s] for s in range(ns)]
+    XD = WV.get_X_D()
+
+    # ---- adjoints of the M x M intermediates
+    tbar, Xbar = [], []
+    for s in range(ns):
+        tb = sum(0.5 * F[s, sp] * tt[sp] for sp in range(ns))
+        ttb = sum(F[sp, s] * (0.5 * t[sp] - X[sp]) for sp in range(ns))
+        tbar.append(tb + lw[:, None] * ttb * lv[None, :])
+        Xbar.append(-sum(F[s, sp] * tt[sp] for sp in range(ns)))
+
+    def three_index_grads(Xi, which):
+        """dE/dJ3_0 and dE/dJ3_ri_0 of W (which=0) or V (which=1) at fixed P2."""
+        P2 = Xi.P2
+        M = P2.shape[0]
+        g3 = np.zeros((N * (N + 1) // 2, M))
+        g3ri = np.zeros((R * N, M))
+        for s in range(ns):
+            o, a = Co[s].shape[1], Ca[s].shape[1]
+            c = o - a
+            if a == 0:
+                continue
+            B2o = (V if which == 0 else W).get_X3idx_two_trans()[s]
+            B2bar = B2o @ (tbar[s].T if which == 0 else tbar[s])  # (a o) x M
+            if which == 0:
+                Wstbar = (Sop[s] @ Vst[s]) @ Xbar[s].T
+            else:
+                Wstbar = (Sop[s] @ Wst[s]) @ Xbar[s]
+            B1bar = (Ca[s] @ B2bar.reshape((a, o * M), order="F")).reshape((N * o, M), order="F")
+            Brbar = np.zeros((R * a, M))
+            for j in range(a):
+                B1bar[N * (c + j):N * (c + j + 1)] += Wstbar[Rp * j:Rp * j + N]
+                Brbar[R * j:R * (j + 1)] = Wstbar[Rp * j + N:Rp * (j + 1)]
+            B10bar = B1bar @ P2.T
+            Brbar0 = Brbar @ P2.T
+            for A in range(M):
+                G = B10bar[:, A].reshape((N, o), order="F") @ Co[s].T
+                g3[:, A] += _pack_sym_sum(G)
+                g3ri[:, A] += (Brbar0[:, A].reshape((R, a), order="F") @ Ca[s].T).reshape(-1, order="F")
+        return g3, g3ri
+
+    gW3, gW3ri = three_index_grads(W, 0)
+    gV3, gV3ri = three_index_grads(V, 1)
+
+    # ---- WV: E2 = 1/2 f XD[s] . (L XD[s']), XD = 1/2 ns P2^T J3_0^T lower(D, 2)
+    D = O.construct_density(Ca)
+    gWV3 = np.zeros_like(WVb.J3_0)
+    for s in range(ns):
+        XDbar = sum(F[s, sp] * lx * XD[sp] for sp in range(ns))
+        vbar = WV.P2 @ XDbar
+        gWV3 += 0.5 * ns * np.outer(O.lower(D[s], 2.0), vbar)
+
+    # ---- metrics: dE/dJ2 = -Q [.] Q^T, Q = P2 L
+    def sym(A):
+        return 0.5 * (A + A.T)
+
+    QW, QV, QX = W.P2 * lw[None, :], V.P2 * lv[None, :], WV.P2 * lx[None, :]
+    AW = np.zeros((lw.size, lw.size))
+    AV = np.zeros((lv.size, lv.size))
+    AX = np.zeros((lx.size, lx.size))
+    for s in range(ns):
+        for sp in range(ns):
+            f = F[s, sp]
+            AW += 0.5 * f * (t[sp] * lv[None, :]) @ t[s].T - f * (X[s] * lv[None, :]) @ t[sp].T
+            AV += 0.5 * f * (t[s].T * lw[None, :]) @ t[sp] - f * (t[sp].T * lw[None, :]) @ X[s]
+            AX += 0.5 * f * np.outer(XD[s], XD[sp])
+    gW2 = -sym(QW @ AW @ QW.T)
+    gV2 = -sym(QV @ AV @ QV.T)
+    gX2 = -sym(QX @ AX @ QX.T)
+    return {"W3": gW3, "W3_ri": gW3ri, "W2": gW2, "V3": gV3, "V3_ri": gV3ri, "V2": gV2,
+            "WV3": gWV3, "WV2": gX2}
