@@ -340,6 +340,8 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the forward+backward (adjoint) report")
     ap.add_argument("--split-moduli", default="14,10",
                     help="moduli counts of the split-precision runs reported beside the FP64 "
                          "headline ('' = none)")
@@ -481,6 +483,66 @@ def main():
         fock_dev.copy_(fock64)
         del fock64
 
+    # ---- reverse mode: forward + backward of the direct terms (s_ss = 0), FP64
+    # and split precision, all gradients written to device buffers
+    adjoint = None
+    if not args.no_adjoint and world == 1:
+        shapes = {"W3": N * (N + 1) // 2 * M, "V3": N * (N + 1) // 2 * M,
+                  "WV3": N * (N + 1) // 2 * M, "W3_ri": R * N * M, "V3_ri": R * N * M,
+                  "W2": M * M, "V2": M * M, "WV2": M * M}
+        gbuf = {k: torch.empty(v, dtype=torch.float64, device=device) for k, v in shapes.items()}
+        gptr = {k: b.data_ptr() for k, b in gbuf.items()}
+
+        def backward():
+            return L.fock_backward(W, V, WV, A, orbs, occs, act, args.s_os, 0.0,
+                                   calculate_fock=True, device_out=gptr)[0]
+
+        def fwd_direct():
+            return L.form_fock(W, V, WV, A, orbs, occs, act, False, True, args.s_os, 0.0,
+                               fock_out=fock_dev.data_ptr())[0]
+
+        def max_rel_diff(a, b, chunk=1 << 26):
+            """max|a - b| / max|b| without full-size temporaries."""
+            d = max(float((a[i:i + chunk] - b[i:i + chunk]).abs().max())
+                    for i in range(0, a.numel(), chunk))
+            r = max(float(b[i:i + chunk].abs().max()) for i in range(0, b.numel(), chunk))
+            return d / r if r > 0 else d
+
+        def timed(fn, n):
+            # same free memory (and so the same automatic chunk budget) for every arm
+            torch.cuda.empty_cache()
+            L.trim_memory()
+            fn()
+            torch.cuda.synchronize(device)
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            for _ in range(n):
+                val = fn()
+            a1.record(stream)
+            torch.cuda.synchronize(device)
+            return a0.elapsed_time(a1) / 1e3 / n, val
+
+        t_fwd, e_fwd = timed(fwd_direct, args.steps)
+        t_bwd, e_bwd = timed(backward, args.steps)
+        ref_g = {k: b.clone() for k, b in gbuf.items()}
+        adjoint = {"scales": [args.s_os, 0.0], "terms": "direct (indirect_term = 0)",
+                   "fp64": {"forward_s": t_fwd, "forward_backward_s": t_bwd, "energy": e_bwd,
+                            "energy_equals_forward": e_bwd == e_fwd},
+                   "gradient_bytes": int(sum(v for v in shapes.values()) * 8)}
+        splits = []
+        for Lm in moduli:
+            L.set_precision(Lm)
+            t_s, e_s = timed(backward, args.steps)
+            L.set_precision(0)
+            errs = {k: max_rel_diff(gbuf[k], ref_g[k]) for k in gbuf}
+            splits.append({"n_moduli": Lm, "forward_backward_s": t_s,
+                           "speedup_vs_fp64_forward_backward": t_bwd / t_s,
+                           "energy_rel_err_vs_fp64": abs(e_s - e_bwd) / abs(e_bwd),
+                           "gradient_max_rel_err_vs_fp64": errs})
+        adjoint["split_precision"] = splits
+        del gbuf, ref_g
+        torch.cuda.empty_cache()
+
     # ---- end to end through the C-ABI from pinned host buffers
     e2e = None
     if not args.no_e2e:
@@ -580,6 +642,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clk,
             "split_precision": split,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -451,6 +451,11 @@ def set_shard(shard: int, n_shards: int):
     _check(lib().uw12c_set_shard(int(shard), int(n_shards)))
 
 
+def trim_memory():
+    """Return the device memory the library keeps reserved between calls."""
+    _check(lib().uw12c_trim_memory())
+
+
 def set_memory_budget(nbytes: int):
     _check(lib().uw12c_set_memory_budget(int(nbytes)))
 

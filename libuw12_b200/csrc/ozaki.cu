@@ -1205,9 +1205,12 @@ int ozaki_bits(int n_moduli, long long k_total) {
 bool ozaki_profitable(const GemmDesc& d) {
   // The operand preparation streams A and B (twice in FP64, once as L bytes
   // per element) and costs about as much as 2mn/(m+n) ~ 800 FP64 FLOPs per
-  // operand element; thinner GEMMs are faster on the FP64 path.
+  // operand element; thinner GEMMs are faster on the FP64 path.  The CRT
+  // reconstruction costs about as much per output element as an FP64 dot
+  // product of a few hundred terms, so short contractions stay FP64 too.
   const double m = double(d.m), n = double(d.n);
-  return 2.0 * m * n >= 800.0 * (m + n);
+  const long long k_total = d.k * d.nbr1 * d.nbr2;
+  return 2.0 * m * n >= 800.0 * (m + n) && k_total >= 512;
 }
 
 bool ozaki_supported(const GemmDesc& d) {

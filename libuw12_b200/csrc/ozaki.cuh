@@ -41,7 +41,8 @@ double split_min_flops();
 void gemm_ozaki(const GemmDesc& d, int n_moduli);
 // Shapes the split-precision kernels take (K <= 8.4M, m, n <= 2^30).
 bool ozaki_supported(const GemmDesc& d);
-// Whether the split path is expected to beat the FP64 path (2mn/(m+n) >= 800).
+// Whether the split path is expected to beat the FP64 path
+// (2mn/(m+n) >= 800 and a contraction of at least 512 terms).
 bool ozaki_profitable(const GemmDesc& d);
 
 // beta (bits kept per operand element) for n_moduli moduli and a contraction
