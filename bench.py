@@ -288,6 +288,36 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def batched_workload(device, n_mol=64, seed=2024):
+    """64 molecules, N ~ U[20, 300], M = 3N, R = 4N, n_occ = round(N/10), even
+    index closed shell and odd index UHF with n_beta = n_alpha - 1, decay 8;
+    inputs generated per molecule with a seed derived from (seed, index)."""
+    import torch
+    import libuw12_b200 as L
+    rng = np.random.default_rng(seed)
+    mols = []
+    for i in range(n_mol):
+        N = int(rng.integers(20, 301))
+        o = max(1, int(round(N / 10)))
+        occ = (o,) if i % 2 == 0 else (o, max(1, o - 1))
+        cfg = (N, 3 * N, 4 * N, occ, 8.0)
+        t, orbs, occs = make_device_inputs(cfg, seed * 1000 + i, device)
+        mols.append({
+            "W": L.setup_base_integrals(t["W3"].data_ptr(), t["W2"].data_ptr(),
+                                        t["W3_ri"].data_ptr(), n_ao=N, n_df=3 * N, n_ri=4 * N,
+                                        device=True),
+            "V": L.setup_base_integrals(t["V3"].data_ptr(), t["V2"].data_ptr(),
+                                        t["V3_ri"].data_ptr(), n_ao=N, n_df=3 * N, n_ri=4 * N,
+                                        device=True),
+            "WV": L.setup_base_integrals(t["WV3"].data_ptr(), t["WV2"].data_ptr(), None, n_ao=N,
+                                         n_df=3 * N, device=True),
+            "abs": L.setup_abs_projectors(t["S"].data_ptr(), N, 4 * N, device=True),
+            "orbitals": orbs, "occ": occs, "n_active": list(occ), "n_ao": N})
+        del t
+        torch.cuda.empty_cache()  # the handles hold their own copies
+    return mols
+
+
 def int8_peak_tops(device):
     """Dense int8 tensor-core throughput of a library GEMM (torch._int_mm,
     8192^3, best of 5), the roofline denominator of the split-precision int8
@@ -340,6 +370,8 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched many-molecule report")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the forward+backward (adjoint) report")
     ap.add_argument("--split-moduli", default="14,10",
@@ -611,6 +643,39 @@ def main():
                          f"at {args.ref_iters} iterations each, loop time extrapolated "
                          f"(measured {te_:.1f} s); numpy/OpenBLAS on all host threads"}
 
+    # ---- batched evaluation of 64 molecules of uneven size (one call), after
+    # the c1 workload has left the device
+    batched = None
+    if not args.no_batched and world == 1:
+        if args.no_e2e:  # the end-to-end arm has not released them
+            for h in (W, V, WV, A):
+                h.close()
+            del t
+        torch.cuda.empty_cache()
+        L.trim_memory()
+        mols = batched_workload(device)
+        batched = {"workload": "64 molecules, N ~ U[20,300], M = 3N, R = 4N, n_occ = round(N/10),"
+                               " half closed shell, half UHF (n_beta = n_alpha - 1), scales "
+                               f"({args.s_os}, {args.s_ss}), energy + Fock, FP64",
+                   "n_ao_range": [min(m["n_ao"] for m in mols), max(m["n_ao"] for m in mols)]}
+        for n_streams in (1, 8):
+            L.fock_batched(mols, indirect, True, args.s_os, args.s_ss, n_streams=n_streams)
+            torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                L.fock_batched(mols, indirect, True, args.s_os, args.s_ss, n_streams=n_streams)
+            torch.cuda.synchronize(device)
+            dt = (time.perf_counter() - t0) / args.steps
+            batched[f"s_per_batch_{n_streams}_streams"] = dt
+            batched[f"molecules_per_s_{n_streams}_streams"] = len(mols) / dt
+        batched["speedup_8_vs_1_stream"] = (batched["s_per_batch_1_streams"] /
+                                            batched["s_per_batch_8_streams"])
+        for m in mols:
+            for k in ("W", "V", "WV", "abs"):
+                m[k].close()
+        del mols
+        L.trim_memory()
+
     flops = canonical_flops(N, M, R, occ, act, same_spin=indirect, fock=True)
     gemm_tf = prof["flops"] / (prof["ms"] / 1e3) / 1e12 if prof["ms"] > 0 else None
     bpg = read_profile_traffic()
@@ -643,6 +708,7 @@ def main():
             "clocks": clk,
             "split_precision": split,
             "adjoint": adjoint,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -90,6 +90,37 @@ int uw12c_form_fock(const uw12c_integrals* W, const uw12c_integrals* V,
                     double scale_same_spin, size_t print_level, double* energy, double* terms,
                     double* fock, int fock_mem_kind);
 
+/* One molecule of a batched evaluation: the arguments of uw12c_form_fock. */
+typedef struct uw12c_molecule {
+  const uw12c_integrals* W;
+  const uw12c_integrals* V;
+  const uw12c_integrals* WV;
+  const uw12c_abs* abs;
+  size_t n_ao, n_spin;
+  const double* const* C;
+  const size_t* ldc;
+  const size_t* n_orb;
+  const double* const* occ;
+  const size_t* n_occ;
+  const size_t* n_active;
+  double* energy; /* host scalar */
+  double* terms;  /* host [3] or NULL */
+  double* fock;   /* n_ao x (n_ao n_spin) or NULL */
+  int fock_mem_kind;
+} uw12c_molecule;
+
+/* Evaluates n molecules of any sizes (no counterpart in libuw12, which takes
+ * one system per call): uw12c_form_fock for each, with n_streams host worker
+ * threads (0 = 8; the calling thread is one of them), each with its own
+ * CUDA stream and an equal share of the memory budget, taking molecules
+ * largest first, so that the evaluations of small molecules overlap on the
+ * GPU.  The calling thread's split-precision settings apply to every
+ * molecule.  statuses (n entries, may be NULL) receives each molecule's
+ * status; the call returns the first failure. */
+int uw12c_fock_batched(const uw12c_molecule* mols, size_t n, int indirect_term,
+                       int calculate_fock, double scale_opp_spin, double scale_same_spin,
+                       size_t n_streams, int* statuses);
+
 /* Reverse mode of the direct terms (no counterpart in libuw12): with
  * indirect_term = 0 (the opposite-spin form of uw12_energy, scale_same_spin
  * entering only the direct same-spin pairs) the energy, terms and Fock

@@ -86,6 +86,8 @@ def lib():
                                   c_d, c_sz, PD, PD, P, ctypes.c_int]
     L.uw12c_fock.argtypes = [P, P, P, P, P, P, c_sz, c_sz, c_sz, P, c_sz, c_sz, PSZ, c_d, c_d,
                              c_sz, PD]
+    L.uw12c_fock_batched.argtypes = [P, c_sz, ctypes.c_int, ctypes.c_int, c_d, c_d, c_sz,
+                                     ctypes.POINTER(ctypes.c_int)]
     L.uw12c_fock_backward.argtypes = [P, P, P, P, c_sz, c_sz, ctypes.POINTER(P), PSZ, PSZ,
                                       ctypes.POINTER(P), PSZ, PSZ, c_d, c_d, PD, PD, P,
                                       ctypes.c_int, ctypes.POINTER(P), ctypes.POINTER(P),
@@ -360,6 +362,65 @@ def form_fock(W: BaseIntegrals, V: BaseIntegrals, WV: BaseIntegrals, abs_p: ABSP
     if fock is not None:
         focks = [np.array(fock[:, s * n_ao:(s + 1) * n_ao]) for s in range(n_spin)]
     return energy.value, focks, (terms[0], terms[1], terms[2])
+
+
+class _Molecule(ctypes.Structure):
+    _fields_ = [("W", ctypes.c_void_p), ("V", ctypes.c_void_p), ("WV", ctypes.c_void_p),
+                ("abs", ctypes.c_void_p), ("n_ao", ctypes.c_size_t), ("n_spin", ctypes.c_size_t),
+                ("C", ctypes.c_void_p), ("ldc", ctypes.c_void_p), ("n_orb", ctypes.c_void_p),
+                ("occ", ctypes.c_void_p), ("n_occ", ctypes.c_void_p),
+                ("n_active", ctypes.c_void_p), ("energy", ctypes.c_void_p),
+                ("terms", ctypes.c_void_p), ("fock", ctypes.c_void_p),
+                ("fock_mem_kind", ctypes.c_int)]
+
+
+def fock_batched(molecules: Sequence[dict], indirect_term: bool, calculate_fock: bool,
+                 scale_opp_spin: float, scale_same_spin: float, n_streams: int = 8):
+    """``uw12c_fock_batched``: ``form_fock`` for many molecules in one call.
+
+    Each molecule is a dict with W, V, WV (BaseIntegrals), abs (ABSProjectors),
+    orbitals, occ and n_active as for ``form_fock``.  Returns a list of
+    ``(energy, fock, (E2, E3, E4))`` in input order.
+    """
+    keep = []  # ctypes arrays and numpy buffers alive until the call returns
+    arr = (_Molecule * max(1, len(molecules)))()
+    outs = []
+    P = ctypes.c_void_p
+    for i, m in enumerate(molecules):
+        n_spin = len(m["orbitals"])
+        n_ao = m["W"].n_ao
+        Cs = [np.asfortranarray(np.asarray(c, dtype=np.float64)) for c in m["orbitals"]]
+        occs = [np.ascontiguousarray(np.asarray(o, dtype=np.float64).reshape(-1))
+                for o in m["occ"]]
+        c_ptrs = (P * n_spin)(*[_fptr(c) for c in Cs])
+        ldc = (ctypes.c_size_t * n_spin)(*[max(1, c.shape[0]) for c in Cs])
+        norb = (ctypes.c_size_t * n_spin)(*[c.shape[1] for c in Cs])
+        o_ptrs = (P * n_spin)(*[_fptr(o) for o in occs])
+        nocc = (ctypes.c_size_t * n_spin)(*[o.size for o in occs])
+        nact = (ctypes.c_size_t * n_spin)(*[int(a) for a in m["n_active"]])
+        energy = ctypes.c_double()
+        terms = (ctypes.c_double * 3)()
+        fock = np.zeros((n_ao, n_ao * n_spin), order="F") if calculate_fock else None
+        keep += [Cs, occs, c_ptrs, ldc, norb, o_ptrs, nocc, nact, energy, terms, fock]
+        arr[i] = _Molecule(m["W"].handle, m["V"].handle, m["WV"].handle, m["abs"].handle, n_ao,
+                           n_spin, ctypes.cast(c_ptrs, P), ctypes.cast(ldc, P),
+                           ctypes.cast(norb, P), ctypes.cast(o_ptrs, P), ctypes.cast(nocc, P),
+                           ctypes.cast(nact, P), ctypes.cast(ctypes.pointer(energy), P),
+                           ctypes.cast(terms, P), _fptr(fock) if fock is not None else P(0),
+                           MEM_HOST)
+        outs.append((energy, fock, terms, n_ao, n_spin))
+    statuses = (ctypes.c_int * max(1, len(molecules)))()
+    _check(lib().uw12c_fock_batched(ctypes.cast(arr, P), len(molecules),
+                                    int(bool(indirect_term)), int(bool(calculate_fock)),
+                                    float(scale_opp_spin), float(scale_same_spin),
+                                    int(n_streams), statuses))
+    res = []
+    for energy, fock, terms, n_ao, n_spin in outs:
+        focks = None
+        if fock is not None:
+            focks = [np.array(fock[:, s * n_ao:(s + 1) * n_ao]) for s in range(n_spin)]
+        res.append((energy.value, focks, (terms[0], terms[1], terms[2])))
+    return res
 
 
 GRADIENT_NAMES = ("W3", "V3", "WV3", "W3_ri", "V3_ri", "W2", "V2", "WV2")

@@ -7,6 +7,9 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
+#include <vector>
+#include <algorithm>
 
 #include "../../include/uw12_c.h"
 #include "engine.cuh"
@@ -22,6 +25,8 @@ namespace {
 std::atomic<unsigned long long> g_launches{0};
 thread_local cudaStream_t g_stream = nullptr;
 std::atomic<size_t> g_budget{0};
+// Per-thread budget of the worker threads of a batched evaluation (0 = none).
+thread_local size_t g_budget_override = 0;
 thread_local size_t g_shard = 0, g_n_shards = 1;
 thread_local int g_last_status = UW12C_OK;
 thread_local std::string g_last_msg;
@@ -193,7 +198,7 @@ void run_form_fock(const uw12c_integrals* W, const uw12c_integrals* V, const uw1
   rq.terms = terms;
   rq.fock = fock;
   rq.fock_device = fock_mem == UW12C_MEM_DEVICE;
-  rq.mem_budget = uw12b::g_budget.load();
+  rq.mem_budget = uw12b::g_budget_override ? uw12b::g_budget_override : uw12b::g_budget.load();
   rq.shard = uw12b::g_shard;
   rq.n_shards = uw12b::g_n_shards;
   DeviceGuard dg(w.device);
@@ -447,6 +452,84 @@ int uw12c_fock_backward(const uw12c_integrals* W, const uw12c_integrals* V,
     run_form_fock(W, V, WV, abs, n_ao, n_spin, C, ldc, n_orb, occ, n_occ, n_active, 0,
                   fock != nullptr, scale_opp_spin, scale_same_spin, 0, energy, terms, fock,
                   fock_mem_kind, &ad);
+  });
+}
+
+int uw12c_fock_batched(const uw12c_molecule* mols, size_t n, int indirect_term,
+                       int calculate_fock, double scale_opp_spin, double scale_same_spin,
+                       size_t n_streams, int* statuses) {
+  return guarded([&] {
+    need(mols != nullptr || n == 0, "null molecule array");
+    if (n == 0) return;
+    const size_t workers = std::min(n, n_streams ? n_streams : size_t(8));
+    // largest molecules first, so that the tail of the batch is short
+    std::vector<size_t> order(n);
+    for (size_t i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t a, size_t b) { return mols[a].n_ao > mols[b].n_ao; });
+    // the caller's per-thread settings apply to every worker; concurrent
+    // evaluations share the memory budget (the explicit one, or 45% of the
+    // free device memory now)
+    const int moduli = uw12b::split_moduli();
+    const double min_flops = uw12b::split_min_flops();
+    size_t total_budget = uw12b::g_budget.load();
+    if (!total_budget) {
+      size_t free_b = 0, total_b = 0;
+      UW12_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      total_budget = static_cast<size_t>(0.45 * double(free_b));
+    }
+    const size_t worker_budget = std::max<size_t>(total_budget / workers, size_t(64) << 20);
+    std::atomic<size_t> next{0};
+    std::vector<int> st(n, UW12C_OK);
+    std::vector<std::string> msg(n);
+    auto work = [&] {
+      cudaStream_t stream = nullptr;
+      int dev = -1;
+      uw12b::set_split_moduli(moduli);
+      uw12b::set_split_min_flops(min_flops);
+      uw12b::g_budget_override = worker_budget;
+      for (size_t q; (q = next.fetch_add(1)) < n;) {
+        const size_t i = order[q];
+        const uw12c_molecule& m = mols[i];
+        st[i] = guarded([&] {
+          need(m.W && m.W->h, "null handle");
+          if (m.W->h->device != dev) {
+            if (stream) cudaStreamDestroy(stream);
+            dev = m.W->h->device;
+            UW12_CUDA(cudaSetDevice(dev));
+            UW12_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+            uw12b::g_stream = stream;
+          }
+          run_form_fock(m.W, m.V, m.WV, m.abs, m.n_ao, m.n_spin, m.C, m.ldc, m.n_orb, m.occ,
+                        m.n_occ, m.n_active, indirect_term, calculate_fock, scale_opp_spin,
+                        scale_same_spin, 0, m.energy, m.terms, m.fock, m.fock_mem_kind);
+        });
+        if (st[i] != UW12C_OK) msg[i] = uw12b::g_last_msg;
+      }
+      if (stream) {
+        cudaStreamSynchronize(stream);
+        cudaStreamDestroy(stream);
+      }
+      uw12b::g_stream = nullptr;
+      uw12b::g_budget_override = 0;
+    };
+    std::vector<std::thread> pool;
+    for (size_t w = 1; w < workers; ++w) pool.emplace_back(work);
+    {
+      // the calling thread works too; its stream and device are restored afterwards
+      const cudaStream_t saved = uw12b::g_stream;
+      int saved_dev = 0;
+      cudaGetDevice(&saved_dev);
+      work();
+      uw12b::g_stream = saved;
+      cudaSetDevice(saved_dev);
+    }
+    for (auto& t : pool) t.join();
+    if (statuses)
+      for (size_t i = 0; i < n; ++i) statuses[i] = st[i];
+    for (size_t i = 0; i < n; ++i)
+      if (st[i] != UW12C_OK)
+        throw Error(st[i], "molecule " + std::to_string(i) + ": " + msg[i]);
   });
 }
 
