@@ -13,8 +13,10 @@
 #include <cfloat>
 #include <cmath>
 #include <cstddef>
+#include <fstream>
 #include <functional>
 #include <memory>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -60,6 +62,44 @@ class Vec : public Mat {
 inline size_t n_rows(const Mat& m) { return m.n_rows(); }
 inline size_t n_cols(const Mat& m) { return m.n_cols(); }
 inline size_t n_elem(const Mat& m) { return m.n_elem(); }
+inline double elem(const Mat& m, size_t i, size_t j) { return m(i, j); }
+inline const double* mem_ptr(const Mat& m) { return m.memptr(); }
+
+/// Load a matrix from a comma-separated text file, one matrix row per line
+/// (linalg::load_csv, src/utils/linalg.hpp:1070-1104).  Blank lines are
+/// skipped; a missing file, an unparsable cell or rows of different lengths
+/// throw std::runtime_error("cannot read data from file").
+inline Mat load_csv(const std::string& filepath) {
+  std::ifstream in(filepath);
+  if (!in) throw std::runtime_error("cannot read data from file");
+  std::vector<std::vector<double>> rows;
+  std::string line;
+  while (std::getline(in, line)) {
+    if (!line.empty() && line.back() == '\r') line.pop_back();
+    if (line.find_first_not_of(" \t") == std::string::npos) continue;
+    std::vector<double> row;
+    std::stringstream ls(line);
+    std::string cell;
+    while (std::getline(ls, cell, ',')) {
+      try {
+        size_t used = 0;
+        row.push_back(std::stod(cell, &used));
+        if (cell.find_first_not_of(" \t", used) != std::string::npos)
+          throw std::runtime_error("cannot read data from file");
+      } catch (const std::logic_error&) {
+        throw std::runtime_error("cannot read data from file");
+      }
+    }
+    if (!rows.empty() && row.size() != rows.front().size())
+      throw std::runtime_error("cannot read data from file");
+    rows.push_back(std::move(row));
+  }
+  const size_t r = rows.size(), c = r ? rows.front().size() : 0;
+  Mat m(r, c);
+  for (size_t i = 0; i < r; ++i)
+    for (size_t j = 0; j < c; ++j) m(i, j) = rows[i][j];
+  return m;
+}
 
 }  // namespace linalg
 

@@ -64,3 +64,42 @@ def test_shard_arguments_are_validated_without_touching_the_device(uw12lib):
         uw12lib.set_shard(3, 2)
     assert L.uw12c_set_shard(1, 2) == 0
     assert L.uw12c_set_shard(0, 1) == 0
+
+
+def _compile(uw12lib, src, out):
+    import subprocess
+    lib_dir = uw12lib.library_path().parent
+    return subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Werror", f"-I{ROOT / 'include'}",
+                           str(src), "-o", str(out), f"-L{lib_dir}", "-luw12_b200",
+                           f"-Wl,-rpath,{lib_dir}"], capture_output=True, text=True)
+
+
+def test_fixture_regression_driver_compiles(uw12lib, tmp_path):
+    r = _compile(uw12lib, ROOT / "libuw12_b200" / "examples" / "fixture_regression.cpp",
+                 tmp_path / "fixture_regression")
+    assert r.returncode == 0, r.stderr
+
+
+def test_load_csv_reads_libuw12_csv_files(uw12lib, tmp_path):
+    """load_csv of the C++ drop-in: libuw12's CSV format (one row per line,
+    %.16e cells), blank lines, and the error on ragged or unparsable files
+    (no device needed)."""
+    import subprocess
+    import numpy as np
+    exe = tmp_path / "csv_check"
+    r = _compile(uw12lib, ROOT / "tests" / "cpp" / "csv_check.cpp", exe)
+    assert r.returncode == 0, r.stderr
+    rng = np.random.default_rng(4)
+    a = rng.standard_normal((7, 5)) * np.exp(rng.uniform(-30, 30, (7, 5)))
+    f = tmp_path / "a.csv"
+    np.savetxt(f, a, delimiter=",", fmt="%.16e")
+    f.write_text(f.read_text() + "\n")
+    out = subprocess.run([str(exe), str(f)], capture_output=True, text=True).stdout.split()
+    assert out[:2] == ["7", "5"]
+    assert np.array_equal(np.array([float(x) for x in out[2:]]), a.reshape(-1, order="F"))
+    bad = tmp_path / "bad.csv"
+    bad.write_text("1.0,2.0\n3.0\n")
+    r = subprocess.run([str(exe), str(bad)], capture_output=True, text=True)
+    assert r.returncode == 1 and "cannot read data from file" in r.stdout
+    r = subprocess.run([str(exe), str(tmp_path / "missing.csv")], capture_output=True, text=True)
+    assert r.returncode == 1 and "cannot read data from file" in r.stdout
