@@ -62,6 +62,31 @@ int uw12c_integrals_create(const double* X3, const double* X2, const double* X3_
  * n_ao(n_ao+1)/2 x n_df) and their eigenvalues; no RI. */
 int uw12c_integrals_create_eigenbasis(const double* J3, const double* df_vals, size_t n_ao,
                                       size_t n_df, int mem_kind, uw12c_integrals** out);
+/* A producer of three-index integrals: writes aux functions [first, first +
+ * count) as the columns of out (leading dimension ld >= the tensor's rows:
+ * n_ao(n_ao+1)/2 packed AO rows, or n_ri*n_ao RI rows) and returns 0, or
+ * non-zero on failure.  For device producers out is device memory and the
+ * work goes on the CUDA stream `stream` (a cudaStream_t); for host producers
+ * out is host memory. */
+typedef int (*uw12c_block_fn)(void* user, size_t first, size_t count, double* out, size_t ld,
+                              void* stream);
+/* Replaces the BaseIntegrals(two_index_fn, three_index_fn, three_index_ri_fn,
+ * df_sizes, n_ao, n_df, n_ri, store_ao_integrals, store_ri_integrals)
+ * constructors (src/integrals/base_integrals.hpp:52-72,
+ * base_integrals.cpp:40-186).  X2 is the metric (n_df x n_df); the
+ * three-index tensors come from the producers, each called with its own user
+ * pointer (three_index_ri may be NULL: no RI).  A stored tensor is produced once, during this call, and kept on the
+ * device; an unstored one (integral-direct mode) is produced again, in aux
+ * blocks, at every use, so inputs larger than device memory can be evaluated;
+ * the user data must then outlive the handle, and the producers may be called from
+ * several host threads (batched evaluations).  x2_mem_kind says where X2
+ * lives, block_mem_kind where the producers' out buffers are (device memory:
+ * device producers; host memory: staged through pinned memory). */
+int uw12c_integrals_create_callback(const double* X2, int x2_mem_kind,
+                                    uw12c_block_fn three_index, void* user,
+                                    uw12c_block_fn three_index_ri, void* user_ri, size_t n_ao,
+                                    size_t n_df, size_t n_ri, int store_ao, int store_ri,
+                                    int block_mem_kind, uw12c_integrals** out);
 int uw12c_integrals_destroy(uw12c_integrals* h);
 /* BaseIntegrals::get_number_ao/df/ri (src/integrals/base_integrals.hpp:196-202). */
 int uw12c_integrals_dims(const uw12c_integrals* h, size_t* n_ao, size_t* n_df, size_t* n_ri);
@@ -265,6 +290,17 @@ int uw12c_profile_read_kind(int kind, unsigned long long* launches, double* ms, 
  * (n_ri*n_ao) x n_df. */
 int uw12c_synth_three_index(double* out_device, int kind, size_t n_ao, size_t n_ri, size_t n_df,
                             unsigned long long seed, unsigned long long tag, double decay);
+/* The same tensors as a device producer for uw12c_integrals_create_callback
+ * (user = a uw12c_synth_spec*): columns [first, first + count) of the tensor
+ * uw12c_synth_three_index writes, generated on the device. */
+typedef struct uw12c_synth_spec {
+  int kind;
+  size_t n_ao, n_ri;
+  unsigned long long seed, tag;
+  double decay;
+} uw12c_synth_spec;
+int uw12c_synth_block(void* spec, size_t first, size_t count, double* out, size_t ld,
+                      void* stream);
 
 #ifdef __cplusplus
 }

@@ -86,6 +86,9 @@ def lib():
                                   c_d, c_sz, PD, PD, P, ctypes.c_int]
     L.uw12c_fock.argtypes = [P, P, P, P, P, P, c_sz, c_sz, c_sz, P, c_sz, c_sz, PSZ, c_d, c_d,
                              c_sz, PD]
+    L.uw12c_integrals_create_callback.argtypes = [P, ctypes.c_int, BLOCK_FN, P, BLOCK_FN, P,
+                                                  c_sz, c_sz, c_sz, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_int, ctypes.POINTER(P)]
     L.uw12c_fock_batched.argtypes = [P, c_sz, ctypes.c_int, ctypes.c_int, c_d, c_d, c_sz,
                                      ctypes.POINTER(ctypes.c_int)]
     L.uw12c_fock_backward.argtypes = [P, P, P, P, c_sz, c_sz, ctypes.POINTER(P), PSZ, PSZ,
@@ -255,6 +258,78 @@ def setup_base_integrals(X3, X2, X3_ri=None, n_ao: Optional[int] = None,
                                       n_ri if X3_ri is not None else 0, MEM_HOST, ctypes.byref(h))
     _check(st)
     return BaseIntegrals(h)
+
+
+BLOCK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t,
+                            ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
+
+
+class SynthSpec(ctypes.Structure):
+    """``uw12c_synth_spec``: the synthetic tensors of ``synth_three_index``."""
+    _fields_ = [("kind", ctypes.c_int), ("n_ao", ctypes.c_size_t), ("n_ri", ctypes.c_size_t),
+                ("seed", ctypes.c_ulonglong), ("tag", ctypes.c_ulonglong),
+                ("decay", ctypes.c_double)]
+
+
+def setup_base_integrals_callback(X2, three_index, three_index_ri=None, n_ao: int = 0,
+                                  n_df: int = 0, n_ri: int = 0, store_ao: bool = True,
+                                  store_ri: bool = True, device: bool = False,
+                                  user: int = 0, user_ri: int = 0) -> BaseIntegrals:
+    """``BaseIntegrals`` from producers of the three-index integrals
+    (``uw12c_integrals_create_callback``; the callback constructors of
+    src/integrals/base_integrals.hpp:52-72).
+
+    ``three_index`` / ``three_index_ri`` are Python callables
+    ``f(first, count, out_ptr, ld, stream_ptr)`` writing aux functions
+    [first, first + count) as columns of ``out`` (device memory when
+    ``device``, else host memory), or raw function pointers (ints) of C
+    producers called with ``user`` / ``user_ri`` (the library's own
+    ``synth_producer()`` is a device producer).  Unstored tensors are produced
+    again at every use (integral-direct mode).  ``X2`` is the metric: a host
+    array, or a device pointer (int).
+    """
+    keep = []
+
+    def as_fn(f):
+        if f is None:
+            return BLOCK_FN()
+        if isinstance(f, int):
+            return ctypes.cast(ctypes.c_void_p(f), BLOCK_FN)
+
+        def tramp(_user, first, count, out, ld, stream):
+            try:
+                f(first, count, out or 0, ld, stream or 0)
+                return 0
+            except Exception:  # reported to the library as a failed producer
+                return 1
+
+        cf = BLOCK_FN(tramp)
+        keep.append(cf)
+        return cf
+
+    x2_device = isinstance(X2, int)
+    if x2_device:
+        x2 = ctypes.c_void_p(X2)
+    else:
+        X2 = _col_major(np.asarray(X2, dtype=np.float64), n_df, n_df)
+        keep.append(X2)
+        x2 = _fptr(X2)
+    h = ctypes.c_void_p()
+    if isinstance(three_index, int) and not device:
+        raise UW12LogicError("native producers write device memory: pass device=True")
+    _check(lib().uw12c_integrals_create_callback(
+        x2, MEM_DEVICE if x2_device else MEM_HOST, as_fn(three_index), ctypes.c_void_p(user),
+        as_fn(three_index_ri), ctypes.c_void_p(user_ri), n_ao, n_df,
+        n_ri if three_index_ri is not None else 0, int(store_ao), int(store_ri),
+        MEM_DEVICE if device else MEM_HOST, ctypes.byref(h)))
+    out = BaseIntegrals(h)
+    out._producers = keep  # the producers must outlive the handle
+    return out
+
+
+def synth_producer() -> int:
+    """Address of ``uw12c_synth_block``, a native device producer (user = SynthSpec*)."""
+    return ctypes.cast(lib().uw12c_synth_block, ctypes.c_void_p).value
 
 
 def base_integrals_eigenbasis(J3, df_vals) -> BaseIntegrals:

@@ -18,6 +18,9 @@
 
 namespace uw12b {
 
+void synth_three_index_block(double* out, size_t ld, int kind, size_t n_ao, size_t n_ri,
+                             size_t first, size_t count, unsigned long long seed,
+                             unsigned long long tag, double decay, cudaStream_t stream);
 void synth_three_index(double* out, int kind, size_t n_ao, size_t n_ri, size_t n_df,
                        unsigned long long seed, unsigned long long tag, double decay);
 
@@ -453,6 +456,105 @@ int uw12c_fock_backward(const uw12c_integrals* W, const uw12c_integrals* V,
                   fock != nullptr, scale_opp_spin, scale_same_spin, 0, energy, terms, fock,
                   fock_mem_kind, &ad);
   });
+}
+
+namespace {
+
+// A user's uw12c_block_fn as an engine producer.  Host producers write into a
+// pinned staging buffer (at most kStageDoubles doubles per call; the requested
+// block is split into column groups) that is copied to the device; the buffer
+// is reused under a mutex, so producers may be called from several host
+// threads (batched evaluations) one at a time per tensor.
+struct UserProducer {
+  static constexpr size_t kStageDoubles = size_t(1) << 25;  // 256 MiB
+  uw12c_block_fn fn;
+  void* user;
+  bool host;
+  size_t rows;
+  std::mutex mu;
+  double* stage = nullptr;
+  size_t stage_n = 0;
+  ~UserProducer() {
+    if (stage) cudaFreeHost(stage);
+  }
+  void operator()(size_t first, size_t count, double* out, size_t ld, cudaStream_t s) {
+    auto call = [&](size_t f, size_t c, double* o, size_t l) {
+      const int rc = fn(user, f, c, o, l, static_cast<void*>(s));
+      if (rc != 0)
+        throw uw12b::Error(UW12C_ERR_RUNTIME,
+                           "three-index integral callback returned " + std::to_string(rc));
+    };
+    if (!host) {
+      call(first, count, out, ld);
+      return;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    const size_t per = std::max<size_t>(1, std::min(count, kStageDoubles / rows));
+    if (stage_n < rows * per) {
+      if (stage) cudaFreeHost(stage);
+      stage = nullptr;
+      stage_n = 0;
+      UW12_CUDA(cudaMallocHost(reinterpret_cast<void**>(&stage), rows * per * sizeof(double)));
+      stage_n = rows * per;
+    }
+    for (size_t c0 = 0; c0 < count; c0 += per) {
+      const size_t nc = std::min(per, count - c0);
+      UW12_CUDA(cudaStreamSynchronize(s));  // the previous copy out of the stage is done
+      call(first + c0, nc, stage, rows);
+      UW12_CUDA(cudaMemcpy2DAsync(out + ld * c0, ld * sizeof(double), stage,
+                                  rows * sizeof(double), rows * sizeof(double), nc,
+                                  cudaMemcpyHostToDevice, s));
+    }
+    UW12_CUDA(cudaStreamSynchronize(s));
+  }
+};
+
+uw12b::AuxProducer wrap_producer(uw12c_block_fn fn, void* user, bool host, size_t rows) {
+  if (!fn) return {};
+  auto p = std::make_shared<UserProducer>();
+  p->fn = fn;
+  p->user = user;
+  p->host = host;
+  p->rows = rows;
+  return [p](size_t f, size_t c, double* o, size_t l, cudaStream_t s) { (*p)(f, c, o, l, s); };
+}
+
+}  // namespace
+
+int uw12c_integrals_create_callback(const double* X2, int x2_mem_kind,
+                                    uw12c_block_fn three_index, void* user,
+                                    uw12c_block_fn three_index_ri, void* user_ri, size_t n_ao,
+                                    size_t n_df, size_t n_ri, int store_ao, int store_ri,
+                                    int block_mem_kind, uw12c_integrals** out) {
+  return guarded([&] {
+    need(out != nullptr, "null output handle");
+    need(x2_mem_kind == UW12C_MEM_HOST || x2_mem_kind == UW12C_MEM_DEVICE, "bad x2_mem_kind");
+    need(block_mem_kind == UW12C_MEM_HOST || block_mem_kind == UW12C_MEM_DEVICE,
+         "bad block_mem_kind");
+    need(three_index != nullptr, "null three-index callback");
+    *out = nullptr;
+    const bool host = block_mem_kind == UW12C_MEM_HOST;
+    auto ao = wrap_producer(three_index, user, host, n_ao * (n_ao + 1) / 2);
+    auto ri = wrap_producer(three_index_ri, user_ri, host, n_ri * n_ao);
+    auto h = std::make_unique<uw12c_integrals>();
+    h->h.reset(uw12b::integrals_create_producer(X2, x2_mem_kind == UW12C_MEM_DEVICE,
+                                                std::move(ao), std::move(ri), n_ao,
+                                                n_df, n_ri, store_ao != 0, store_ri != 0));
+    *out = h.release();
+  });
+}
+
+int uw12c_synth_block(void* spec, size_t first, size_t count, double* out, size_t ld,
+                      void* stream) {
+  if (!spec) return 1;
+  const auto* sp = static_cast<const uw12c_synth_spec*>(spec);
+  try {
+    uw12b::synth_three_index_block(out, ld, sp->kind, sp->n_ao, sp->n_ri, first, count, sp->seed,
+                                   sp->tag, sp->decay, static_cast<cudaStream_t>(stream));
+  } catch (...) {
+    return 2;
+  }
+  return 0;
 }
 
 int uw12c_fock_batched(const uw12c_molecule* mols, size_t n, int indirect_term,

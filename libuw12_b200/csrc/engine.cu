@@ -97,6 +97,49 @@ size_t auto_budget_doubles(size_t requested_bytes) {
 
 inline long long LL(size_t v) { return static_cast<long long>(v); }
 
+// Metric eigendecomposition (base_integrals.cpp:155-166): P2 = Q pinv(Lambda),
+// df_vals = Lambda, after libuw12's symmetry check.
+void setup_metric(IntegralsHandle* h, const double* X2, bool device_mem) {
+  cudaStream_t s = current_stream();
+  const size_t n_df = h->n_df;
+  h->P2.alloc(n_df * n_df);
+  upload(h->P2.get(), X2, n_df * n_df, device_mem, s);
+  require_symmetric(h->P2.get(), n_df, "matrix must be symmetric");
+  h->lam.alloc(n_df);
+  eigh(h->P2.get(), n_df, h->lam.get());
+  scale_pinv_cols(h->P2.get(), LL(n_df), h->lam.get(), 1e-10);
+  h->lam_host.resize(n_df);
+  UW12_CUDA(cudaMemcpyAsync(h->lam_host.data(), h->lam.get(), n_df * sizeof(double),
+                            cudaMemcpyDeviceToHost, s));
+  UW12_CUDA(cudaStreamSynchronize(s));
+}
+
+// Columns [a0, a0 + na) of X's AO (ri = false: Np rows) or RI (ri = true:
+// R N rows) three-index tensor, column-major with leading dimension = rows: a
+// pointer into the stored tensor, or the producer's output in `scratch`
+// (integral-direct mode).
+const double* aux_block(const IntegralsHandle& X, bool ri, size_t a0, size_t na,
+                        DevBuf& scratch) {
+  const size_t rows = ri ? X.n_ri * X.n_ao : packed_size(X.n_ao);
+  const DeviceArray& stored = ri ? X.J3_ri_0 : X.J3_0;
+  if (stored.get()) return stored.get() + rows * a0;
+  const AuxProducer& fn = ri ? X.ri_fn : X.ao_fn;
+  if (!fn) throw_runtime(ri ? "J3_ri_0 not stored" : "J3_0 not stored");
+  if (scratch.size() < rows * na) scratch.alloc(rows * na);
+  fn(a0, na, scratch.get(), rows, current_stream());
+  return scratch.get();
+}
+
+// Aux functions per block when looping over a tensor: all of them when it is
+// stored (one block, the tensor itself), else as many as a quarter of the
+// budget holds.
+size_t aux_step(const IntegralsHandle& X, bool ri, size_t budget) {
+  const DeviceArray& stored = ri ? X.J3_ri_0 : X.J3_0;
+  if (stored.get()) return X.n_df;
+  const size_t rows = ri ? X.n_ri * X.n_ao : packed_size(X.n_ao);
+  return std::max<size_t>(1, std::min(X.n_df, budget / (4 * rows)));
+}
+
 }  // namespace
 
 // --------------------------------------------------------------------------
@@ -122,15 +165,44 @@ IntegralsHandle* integrals_create(const double* X3, const double* X2, const doub
       h->J3_ri_0.alloc(n_ri * n_ao * n_df);
       upload(h->J3_ri_0.get(), X3_ri, n_ri * n_ao * n_df, device_mem, s);
     }
-    h->P2.alloc(n_df * n_df);
-    upload(h->P2.get(), X2, n_df * n_df, device_mem, s);
-    require_symmetric(h->P2.get(), n_df, "matrix must be symmetric");
-    h->lam.alloc(n_df);
-    eigh(h->P2.get(), n_df, h->lam.get());
-    scale_pinv_cols(h->P2.get(), LL(n_df), h->lam.get(), 1e-10);
-    h->lam_host.resize(n_df);
-    UW12_CUDA(cudaMemcpyAsync(h->lam_host.data(), h->lam.get(), n_df * sizeof(double),
-                              cudaMemcpyDeviceToHost, s));
+    setup_metric(h, X2, device_mem);
+  } catch (...) {
+    delete h;
+    throw;
+  }
+  return h;
+}
+
+IntegralsHandle* integrals_create_producer(const double* X2, bool x2_device, AuxProducer ao_fn,
+                                           AuxProducer ri_fn, size_t n_ao, size_t n_df,
+                                           size_t n_ri, bool store_ao, bool store_ri) {
+  if (n_ao == 0) throw_runtime("Number of ao orbitals is zero");
+  if (n_df == 0) throw_runtime("Number of density-fitting basis functions is zero");
+  if (!X2 || !ao_fn) throw Error(kErrInvalid, "null metric or three-index producer");
+  if (ri_fn && n_ri == 0) throw_runtime("Three index ri integrals given but n_ri is zero");
+  auto h = new IntegralsHandle();
+  try {
+    UW12_CUDA(cudaGetDevice(&h->device));
+    cudaStream_t s = current_stream();
+    h->n_ao = n_ao;
+    h->n_df = n_df;
+    h->n_ri = ri_fn ? n_ri : 0;
+    setup_metric(h, X2, x2_device);
+    const size_t np = packed_size(n_ao);
+    if (store_ao) {
+      h->J3_0.alloc(np * n_df);
+      ao_fn(0, n_df, h->J3_0.get(), np, s);
+    } else {
+      h->ao_fn = std::move(ao_fn);
+    }
+    if (ri_fn) {
+      if (store_ri) {
+        h->J3_ri_0.alloc(n_ri * n_ao * n_df);
+        ri_fn(0, n_df, h->J3_ri_0.get(), n_ri * n_ao, s);
+      } else {
+        h->ri_fn = std::move(ri_fn);
+      }
+    }
     UW12_CUDA(cudaStreamSynchronize(s));
   } catch (...) {
     delete h;
@@ -278,16 +350,51 @@ double spin_factor(int ns, int s, int sp, double s_os, double s_ss) {
   return (s == sp) ? s_ss : s_os;
 }
 
+// XDr (M x ns) = J3_0^T dmat: the unscaled fitted densities of libuw12's
+// get_X_D (integrals.cpp:347-378), over aux blocks.
+void fitted_density_raw(const IntegralsHandle& X, const double* dmat, int ns, double* XDr,
+                        size_t budget) {
+  const size_t M = X.n_df, np = packed_size(X.n_ao);
+  DevBuf scratch;
+  const size_t step = aux_step(X, false, budget);
+  for (size_t b0 = 0; b0 < M; b0 += step) {
+    const size_t nb = std::min(step, M - b0);
+    GemmDesc g = gemm_nn(LL(nb), ns, LL(np), 1.0, aux_block(X, false, b0, nb, scratch), LL(np),
+                         dmat, LL(np), 0.0, XDr + b0, LL(M));
+    g.a_kcontig = true;
+    gemm(g);
+  }
+}
+
+// H2 (R*na x M) = [J3_ri_0[:,A] (R x N) Cm] for every A (transform_second_index,
+// transformations.hpp:130-158), over aux blocks.
+void ri_transform(const IntegralsHandle& X, const double* Cm, size_t na, double* H2,
+                  size_t budget) {
+  const size_t N = X.n_ao, R = X.n_ri, M = X.n_df;
+  DevBuf scratch;
+  const size_t step = aux_step(X, true, budget);
+  for (size_t b0 = 0; b0 < M; b0 += step) {
+    const size_t nb = std::min(step, M - b0);
+    GemmDesc g = gemm_nn(LL(R), LL(na), LL(N), 1.0, aux_block(X, true, b0, nb, scratch), LL(R),
+                         Cm, LL(N), 0.0, H2 + R * na * b0, LL(R));
+    g.nbo1 = LL(nb);
+    g.sAo1 = LL(R * N);
+    g.sCo1 = LL(R * na);
+    gemm(g);
+  }
+}
+
 // H (N*nc x M) = [sq(J3_0[:,A]) Cm] for every A, chunked over A.
 void transform_ao(const IntegralsHandle& X, const double* Cm, size_t nc, double* H,
                   size_t budget) {
   const size_t N = X.n_ao, M = X.n_df, np = packed_size(N);
   if (nc == 0) return;
-  const size_t ac = std::max<size_t>(1, std::min(M, budget / (N * N)));
-  DevBuf U(N * N * ac);
+  const size_t ac = std::max<size_t>(1, std::min(M, budget / (N * N + (X.J3_0.get() ? 0 : np))));
+  DevBuf U(N * N * ac), scratch;
   for (size_t a0 = 0; a0 < M; a0 += ac) {
     const size_t na = std::min(ac, M - a0);
-    unpack_sym(X.J3_0.get() + np * a0, LL(np), LL(N), LL(na), U.get(), LL(N), LL(N * N));
+    unpack_sym(aux_block(X, false, a0, na, scratch), LL(np), LL(N), LL(na), U.get(), LL(N),
+               LL(N * N));
     GemmDesc g = gemm_nn(LL(N), LL(nc), LL(N), 1.0, U.get(), LL(N), Cm, LL(N), 0.0,
                          H + N * nc * a0, LL(N));
     g.nbo1 = LL(na);
@@ -422,12 +529,9 @@ void form_fock(const FockRequest& rq) {
   if (lead) {
     DevBuf dmat(np * ns), XDr(MX * ns), XD(MX * ns);
     for (int s = 0; s < ns; ++s) pack_density(Ca_s(s), LL(N), LL(N), LL(sd[s].a), two, dmat.get() + np * s);
-    GemmDesc g = gemm_nn(LL(MX), ns, LL(np), 1.0, WV.J3_0.get(), LL(np), dmat.get(), LL(np), 0.0,
-                         XDr.get(), LL(MX));
-    g.a_kcontig = true;
-    gemm(g);
-    g = gemm_nn(LL(MX), ns, LL(MX), 0.5 * ns, WV.P2.get(), LL(MX), XDr.get(), LL(MX), 0.0,
-                XD.get(), LL(MX));
+    fitted_density_raw(WV, dmat.get(), ns, XDr.get(), budget);
+    GemmDesc g = gemm_nn(LL(MX), ns, LL(MX), 0.5 * ns, WV.P2.get(), LL(MX), XDr.get(), LL(MX), 0.0,
+                         XD.get(), LL(MX));
     g.a_kcontig = true;
     gemm(g);
     double coef[4] = {0, 0, 0, 0};
@@ -444,8 +548,16 @@ void form_fock(const FockRequest& rq) {
       combine_vecs(XD.get(), LL(MX), ns, coef, WV.lam.get(), vc.get());
       gemm(gemm_nn(LL(MX), ns, LL(MX), 1.0, WV.P2.get(), LL(MX), vc.get(), LL(MX), 0.0, u.get(),
                    LL(MX)));
-      gemm(gemm_nn(LL(np), ns, LL(MX), 1.0, WV.J3_0.get(), LL(np), u.get(), LL(MX), 0.0, gv.get(),
-                   LL(np)));
+      {
+        // gv = J3_0 u, accumulated over aux blocks
+        DevBuf scratch;
+        const size_t step = aux_step(WV, false, budget);
+        for (size_t b0 = 0; b0 < MX; b0 += step) {
+          const size_t nb = std::min(step, MX - b0);
+          gemm(gemm_nn(LL(np), ns, LL(nb), 1.0, aux_block(WV, false, b0, nb, scratch), LL(np),
+                       u.get() + b0, LL(MX), b0 ? 1.0 : 0.0, gv.get(), LL(np)));
+        }
+      }
       for (int s = 0; s < ns; ++s)
         unpack_sym(gv.get() + np * s, LL(np), LL(N), 1, Fp[s].get(), LL(N), 0, 1.0, 1.0);
     }
@@ -506,14 +618,7 @@ void form_fock(const FockRequest& rq) {
       }
     }
     DevBuf H2(R * a_tot * M);
-    if (a_tot) {
-      GemmDesc g = gemm_nn(LL(R), LL(a_tot), LL(N), 1.0, X.J3_ri_0.get(), LL(R), Ca.get(), LL(N),
-                           0.0, H2.get(), LL(R));
-      g.nbo1 = LL(M);
-      g.sAo1 = LL(R * N);
-      g.sCo1 = LL(R * a_tot);
-      gemm(g);
-    }
+    if (a_tot) ri_transform(X, Ca.get(), a_tot, H2.get(), budget);
     for (int s = 0; s < ns; ++s) {
       const size_t o = sd[s].o, a = sd[s].a, c = sd[s].c;
       if (!a) continue;
@@ -641,28 +746,40 @@ void form_fock(const FockRequest& rq) {
       const size_t ac = tile_chunk(ahi - alo, 1,
                                    std::max<size_t>(1, std::min(ahi - alo, budget / per_a)));
       DevBuf sbuf(np * ac), Gst(Rp * N * ac), Lb(Rp * N * ac), Hb(Rp * N * ac);
+      DevBuf scrW, scrWr, scrV, scrVr;
+      const size_t vstep = aux_step(V, false, budget), vrstep = aux_step(V, true, budget);
       for (size_t a0 = alo; a0 < ahi; a0 += ac) {
         const size_t na = std::min(ac, ahi - a0);
         // G_W chunk, AO rows then RI rows of each (R' x N) block
-        unpack_sym(W.J3_0.get() + np * a0, LL(np), LL(N), LL(na), Gst.get(), LL(Rp), LL(Rp * N));
-        copy3d(W.J3_ri_0.get() + R * N * a0, LL(R), LL(R * N), Gst.get() + N, LL(Rp), LL(Rp * N),
-               LL(R), LL(N), LL(na));
+        unpack_sym(aux_block(W, false, a0, na, scrW), LL(np), LL(N), LL(na), Gst.get(), LL(Rp),
+                   LL(Rp * N));
+        copy3d(aux_block(W, true, a0, na, scrWr), LL(R), LL(R * N), Gst.get() + N, LL(Rp),
+               LL(Rp * N), LL(R), LL(N), LL(na));
         gemm(gemm_nn(LL(Rp), LL(N * na), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp), Gst.get(), LL(Rp),
                      0.0, Lb.get(), LL(Rp)));
         for (size_t q = 0; q < tdx_spins.size(); ++q) {
           const double* T2 = T2s[q].get();
-          GemmDesc gs = gemm_nn(LL(np), LL(na), LL(MV), 1.0, V.J3_0.get(), LL(np), T2 + a0,
-                                LL(MW), 0.0, sbuf.get(), LL(np));
-          gs.b_ncontig = true;
-          gemm(gs);
+          // s = J3_0^V T2^T and p = J3_ri_0^V T2^T, accumulated over V's aux blocks
+          for (size_t b0 = 0; b0 < MV; b0 += vstep) {
+            const size_t nb = std::min(vstep, MV - b0);
+            GemmDesc gs = gemm_nn(LL(np), LL(na), LL(nb), 1.0, aux_block(V, false, b0, nb, scrV),
+                                  LL(np), T2 + a0 + MW * b0, LL(MW), b0 ? 1.0 : 0.0, sbuf.get(),
+                                  LL(np));
+            gs.b_ncontig = true;
+            gemm(gs);
+          }
           unpack_sym(sbuf.get(), LL(np), LL(N), LL(na), Hb.get(), LL(Rp), LL(Rp * N));
-          GemmDesc gp = gemm_nn(LL(R), LL(na), LL(MV), 1.0, V.J3_ri_0.get(), LL(R * N), T2 + a0,
-                                LL(MW), 0.0, Hb.get() + N, LL(Rp * N));
-          gp.b_ncontig = true;
-          gp.nbo1 = LL(N);
-          gp.sAo1 = LL(R);
-          gp.sCo1 = LL(Rp);
-          gemm(gp);
+          for (size_t b0 = 0; b0 < MV; b0 += vrstep) {
+            const size_t nb = std::min(vrstep, MV - b0);
+            GemmDesc gp = gemm_nn(LL(R), LL(na), LL(nb), 1.0, aux_block(V, true, b0, nb, scrVr),
+                                  LL(R * N), T2 + a0 + MW * b0, LL(MW), b0 ? 1.0 : 0.0,
+                                  Hb.get() + N, LL(Rp * N));
+            gp.b_ncontig = true;
+            gp.nbo1 = LL(N);
+            gp.sAo1 = LL(R);
+            gp.sCo1 = LL(Rp);
+            gemm(gp);
+          }
           GemmDesc gf = gemm_nn(LL(N), LL(N), LL(Rp), -1.0, Lb.get(), LL(Rp), Hb.get(), LL(Rp),
                                 1.0, Fp[tdx_spins[q]].get(), LL(N));
           gf.a_kcontig = true;
@@ -778,7 +895,7 @@ void form_fock(const FockRequest& rq) {
         const size_t kc = tile_chunk(khi - klo, a,
                                      std::max<size_t>(1, std::min(khi - klo, budget / per_k)));
         DevBuf ZYV(Rp * a * N * kc), ZYW(Rp * a * N * kc), gpk(np * a * kc), Gao(N * N * a * kc),
-            gri(R * N * a * kc), Wk(Rp * N * a * kc);
+            gri(R * N * a * kc), Wk(Rp * N * a * kc), scrX, scrXr;
         for (size_t k0 = klo; k0 < khi; k0 += kc) {
           const size_t nk = std::min(kc, khi - k0);
           for (int term = 0; term < 2; ++term) {
@@ -794,11 +911,21 @@ void form_fock(const FockRequest& rq) {
                                   b1yl + N * k0, LL(No), 0.0, ZY, LL(Rp * a));
             gz.b_ncontig = true;
             gemm(gz);
-            gemm(gemm_nn(LL(np), LL(a * nk), LL(MXi), 1.0, Xi.J3_0.get(), LL(np),
-                         xh + MXi * a * k0, LL(MXi), 0.0, gpk.get(), LL(np)));
+            // gpk = J3_0 xh, gri = J3_ri_0 xh, accumulated over Xi's aux blocks
+            const size_t st_ao = aux_step(Xi, false, budget), st_ri = aux_step(Xi, true, budget);
+            for (size_t b0 = 0; b0 < MXi; b0 += st_ao) {
+              const size_t nb = std::min(st_ao, MXi - b0);
+              gemm(gemm_nn(LL(np), LL(a * nk), LL(nb), 1.0, aux_block(Xi, false, b0, nb, scrX),
+                           LL(np), xh + MXi * a * k0 + b0, LL(MXi), b0 ? 1.0 : 0.0, gpk.get(),
+                           LL(np)));
+            }
             unpack_sym(gpk.get(), LL(np), LL(N), LL(a * nk), Gao.get(), LL(N), LL(N * N));
-            gemm(gemm_nn(LL(R * N), LL(a * nk), LL(MXi), 1.0, Xi.J3_ri_0.get(), LL(R * N),
-                         xh + MXi * a * k0, LL(MXi), 0.0, gri.get(), LL(R * N)));
+            for (size_t b0 = 0; b0 < MXi; b0 += st_ri) {
+              const size_t nb = std::min(st_ri, MXi - b0);
+              gemm(gemm_nn(LL(R * N), LL(a * nk), LL(nb), 1.0, aux_block(Xi, true, b0, nb, scrXr),
+                           LL(R * N), xh + MXi * a * k0 + b0, LL(MXi), b0 ? 1.0 : 0.0, gri.get(),
+                           LL(R * N)));
+            }
             GemmDesc fa = gemm_nn(LL(N), LL(N), LL(N), s_ss, Gao.get(), LL(N), ZY, LL(Rp * a),
                                   1.0, Fp[s].get(), LL(N));
             fa.nbr1 = LL(a);
@@ -990,14 +1117,7 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
     DevBuf H(N * o_tot * M);
     transform_ao(X, Co.get(), o_tot, H.get(), budget / 2);
     DevBuf H2(R * a_tot * M);
-    if (a_tot) {
-      GemmDesc g = gemm_nn(LL(R), LL(a_tot), LL(N), 1.0, X.J3_ri_0.get(), LL(R), Ca.get(), LL(N),
-                           0.0, H2.get(), LL(R));
-      g.nbo1 = LL(M);
-      g.sAo1 = LL(R * N);
-      g.sCo1 = LL(R * a_tot);
-      gemm(g);
-    }
+    if (a_tot) ri_transform(X, Ca.get(), a_tot, H2.get(), budget);
     for (int s = 0; s < ns; ++s) {
       const size_t o = sd[s].o, a = sd[s].a, c = sd[s].c;
       if (!a) continue;
@@ -1219,12 +1339,9 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
     DevBuf dmat(np * ns), XDr(MX * ns), XD(MX * ns), XDb(MX * ns), vb(MX * ns);
     for (int s = 0; s < ns; ++s)
       pack_density(Ca_s(s), LL(N), LL(N), LL(sd[s].a), two, dmat.get() + np * s);
-    GemmDesc g = gemm_nn(LL(MX), ns, LL(np), 1.0, WV.J3_0.get(), LL(np), dmat.get(), LL(np), 0.0,
-                         XDr.get(), LL(MX));
-    g.a_kcontig = true;
-    gemm(g);
-    g = gemm_nn(LL(MX), ns, LL(MX), 0.5 * ns, WV.P2.get(), LL(MX), XDr.get(), LL(MX), 0.0,
-                XD.get(), LL(MX));
+    fitted_density_raw(WV, dmat.get(), ns, XDr.get(), budget);
+    GemmDesc g = gemm_nn(LL(MX), ns, LL(MX), 0.5 * ns, WV.P2.get(), LL(MX), XDr.get(), LL(MX),
+                         0.0, XD.get(), LL(MX));
     g.a_kcontig = true;
     gemm(g);
     double coef[4] = {0, 0, 0, 0};

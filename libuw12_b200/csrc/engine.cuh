@@ -2,6 +2,7 @@
 // pair-loop-free FP64 schedule of libuw12's form_fock (src/uw12.cpp:22-119).
 #pragma once
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -35,11 +36,21 @@ class DeviceArray {
 // J3_0 (Np x M, packed (mn|A)), J3_ri_0 ((R N) x M, row nu + R mu) and the
 // metric eigendecomposition P2 = Q pinv(Lambda), df_vals = Lambda
 // (base_integrals.cpp:155-166).
+//
+// Integral-direct mode (the store_ao / store_ri = false constructors,
+// base_integrals.hpp:52-72): a tensor that is not stored has a producer that
+// writes aux functions [first, first + count) as columns of `out` (device
+// memory, leading dimension ld) on `stream`; every use asks it for the aux
+// functions it needs.
+using AuxProducer =
+    std::function<void(size_t first, size_t count, double* out, size_t ld, cudaStream_t stream)>;
+
 struct IntegralsHandle {
   int device = 0;
   size_t n_ao = 0, n_df = 0, n_ri = 0;
   DeviceArray J3_0, J3_ri_0, P2, lam;
   std::vector<double> lam_host;
+  AuxProducer ao_fn, ri_fn;  // set when J3_0 / J3_ri_0 are not stored
 };
 
 // ABS+ projectors (ri_utils.hpp:45-74) stored as one (N+R) x (N+R) matrix
@@ -57,6 +68,14 @@ IntegralsHandle* integrals_create(const double* X3, const double* X2, const doub
 IntegralsHandle* integrals_create_eigenbasis(const double* J3, const double* df_vals, size_t n_ao,
                                              size_t n_df, bool device_mem);
 AbsHandle* abs_create(const double* S, size_t n_ao, size_t n_ri, bool device_mem);
+// BaseIntegrals(two_index_fn, three_index_fn, three_index_ri_fn, ..., store_ao,
+// store_ri) (base_integrals.hpp:52-72, base_integrals.cpp:40-186): the metric X2
+// (n_df x n_df) is given, the three-index tensors come from producers; a stored
+// tensor is produced once, here, an unstored one at every use.  ri_fn may be
+// empty (no RI).
+IntegralsHandle* integrals_create_producer(const double* X2, bool x2_device, AuxProducer ao_fn,
+                                           AuxProducer ri_fn, size_t n_ao, size_t n_df,
+                                           size_t n_ri, bool store_ao, bool store_ri);
 
 struct FockRequest {
   const IntegralsHandle* W = nullptr;

@@ -17,18 +17,22 @@ __host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long 
   return z ^ (z >> 31);
 }
 
-__global__ void k_synth(double* out, int kind, long long n_ao, long long n_ri, long long rows,
-                        long long total, unsigned long long key, double inv_decay) {
+// Columns [first, first + count) of the tensor (rows x n_df), written with
+// leading dimension ld; element e of the full tensor is e = r + rows * column.
+__global__ void k_synth(double* out, long long ld, int kind, long long n_ao, long long n_ri,
+                        long long rows, long long first, long long total,
+                        unsigned long long key, double inv_decay) {
   const double two_pi = 6.283185307179586476925286766559;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long r = idx % rows, col = idx / rows;
+    const long long e = r + rows * (first + col);
     const unsigned long long base = key + 2ULL * static_cast<unsigned long long>(e);
     const unsigned long long h0 = mix64(base);
     const unsigned long long h1 = mix64(base + 1ULL);
     const double u1 = (static_cast<double>(h0 >> 11) + 1.0) * 0x1.0p-53;
     const double u2 = static_cast<double>(h1 >> 11) * 0x1.0p-53;
     const double g = sqrt(-2.0 * log(u1)) * cos(two_pi * u2);
-    const long long r = e % rows;
     long long p, q;
     if (kind == 0) {
       long long i = static_cast<long long>((sqrt(8.0 * double(r) + 1.0) - 1.0) * 0.5);
@@ -41,25 +45,35 @@ __global__ void k_synth(double* out, int kind, long long n_ao, long long n_ri, l
       q = r / n_ri;
     }
     const long long d = p > q ? p - q : q - p;
-    out[e] = g * exp(-double(d) * inv_decay);
+    out[r + ld * col] = g * exp(-double(d) * inv_decay);
   }
 }
 
 }  // namespace
 
-void synth_three_index(double* out, int kind, size_t n_ao, size_t n_ri, size_t n_df,
-                       unsigned long long seed, unsigned long long tag, double decay) {
+void synth_three_index_block(double* out, size_t ld, int kind, size_t n_ao, size_t n_ri,
+                             size_t first, size_t count, unsigned long long seed,
+                             unsigned long long tag, double decay, cudaStream_t stream) {
   if (kind != 0 && kind != 1) throw Error(kErrInvalid, "synth: kind must be 0 (AO) or 1 (RI)");
   if (!(decay > 0.0)) throw Error(kErrInvalid, "synth: decay must be positive");
   const long long rows = kind == 0 ? static_cast<long long>(n_ao * (n_ao + 1) / 2)
                                    : static_cast<long long>(n_ri * n_ao);
-  const long long total = rows * static_cast<long long>(n_df);
+  if (ld < static_cast<size_t>(rows)) throw Error(kErrInvalid, "synth: ld smaller than the rows");
+  const long long total = rows * static_cast<long long>(count);
   if (total <= 0) return;
   const unsigned long long key = mix64(mix64(seed) ^ tag);
-  k_synth<<<148 * 32, 256, 0, current_stream()>>>(out, kind, static_cast<long long>(n_ao),
-                                                   static_cast<long long>(n_ri), rows, total, key,
-                                                   1.0 / decay);
+  k_synth<<<148 * 32, 256, 0, stream>>>(out, static_cast<long long>(ld), kind,
+                                         static_cast<long long>(n_ao),
+                                         static_cast<long long>(n_ri), rows,
+                                         static_cast<long long>(first), total, key, 1.0 / decay);
   UW12_LAUNCHED();
+}
+
+void synth_three_index(double* out, int kind, size_t n_ao, size_t n_ri, size_t n_df,
+                       unsigned long long seed, unsigned long long tag, double decay) {
+  const size_t rows = kind == 0 ? n_ao * (n_ao + 1) / 2 : n_ri * n_ao;
+  synth_three_index_block(out, rows, kind, n_ao, n_ri, 0, n_df, seed, tag, decay,
+                          current_stream());
 }
 
 }  // namespace uw12b
