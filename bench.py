@@ -25,6 +25,7 @@ bounded number of iterations and its time is extrapolated to the full count.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -141,9 +142,10 @@ def _tag(name: str) -> int:
     return int.from_bytes(hashlib.sha256(name.encode()).digest()[:8], "little")
 
 
-def make_device_inputs(cfg, seed, device):
-    """Three-index tensors generated on the device (library synth kernel);
-    metrics, overlap and orbitals generated with torch on the device."""
+def make_device_inputs(cfg, seed, device, three_index=True):
+    """Three-index tensors generated on the device (library synth kernel; left
+    out when three_index is false); metrics, overlap and orbitals generated with
+    torch on the device."""
     import torch
     import libuw12_b200 as L
     N, M, R, occ, L_decay = cfg
@@ -151,10 +153,10 @@ def make_device_inputs(cfg, seed, device):
     g = torch.Generator(device=device)
     g.manual_seed(seed)
     t = {}
-    for nm in ("W3", "V3", "WV3"):
+    for nm in ("W3", "V3", "WV3") if three_index else ():
         t[nm] = torch.empty(np_ * M, dtype=torch.float64, device=device)
         L.synth_three_index(t[nm].data_ptr(), 0, N, 0, M, seed, _tag(nm), L_decay)
-    for nm in ("W3_ri", "V3_ri"):
+    for nm in ("W3_ri", "V3_ri") if three_index else ():
         t[nm] = torch.empty(R * N * M, dtype=torch.float64, device=device)
         L.synth_three_index(t[nm].data_ptr(), 1, N, R, M, seed, _tag(nm), L_decay)
     for nm in ("W2", "V2", "WV2"):
@@ -351,7 +353,10 @@ def config_dict(args):
                         f"n_occ={list(occ)} ({'UHF' if len(occ) == 2 else 'closed shell'}), "
                         f"all-electron, scales (s_os, s_ss)=({args.s_os}, {args.s_ss})",
             "n_ao": N, "n_df": M, "n_ri": R, "n_occ": list(occ), "decay": Ld,
-            "precision": "fp64", "l2": "inputs (28.6 GB at c1) exceed the 126 MB L2"}
+            "precision": "fp64", "l2": "inputs (28.6 GB at c1) exceed the 126 MB L2",
+            "integrals": ("integral-direct: no three-index tensor stored, each regenerated "
+                          "on the device (library synthetic producer) in aux blocks at every use"
+                          if getattr(args, "direct", False) else "stored on the device")}
 
 
 # --------------------------------------------------------------------------
@@ -370,6 +375,10 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--direct", action="store_true",
+                    help="integral-direct three-index tensors: regenerated on the device by "
+                         "the library's synthetic producer at every use instead of stored (for "
+                         "workloads whose inputs exceed device memory, e.g. --config c2)")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched many-molecule report")
     ap.add_argument("--no-adjoint", action="store_true",
@@ -378,6 +387,8 @@ def main():
                     help="moduli counts of the split-precision runs reported beside the FP64 "
                          "headline ('' = none)")
     args = ap.parse_args()
+    if args.direct:  # the host-side arms need every tensor in memory
+        args.no_e2e = args.no_cpu_baseline = args.no_batched = True
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -403,15 +414,34 @@ def main():
     cfg = CONFIGS[args.config]
     N, M, R, occ, _ = cfg
     act = list(occ)
-    t, orbs, occs = make_device_inputs(cfg, 11, device)
+    t, orbs, occs = make_device_inputs(cfg, 11, device, three_index=not args.direct)
     peak = fp64_peak_tflops(device)
 
-    W = L.setup_base_integrals(t["W3"].data_ptr(), t["W2"].data_ptr(), t["W3_ri"].data_ptr(),
-                               n_ao=N, n_df=M, n_ri=R, device=True)
-    V = L.setup_base_integrals(t["V3"].data_ptr(), t["V2"].data_ptr(), t["V3_ri"].data_ptr(),
-                               n_ao=N, n_df=M, n_ri=R, device=True)
-    WV = L.setup_base_integrals(t["WV3"].data_ptr(), t["WV2"].data_ptr(), None, n_ao=N, n_df=M,
-                                device=True)
+    if args.direct:
+        # the same synthetic tensors from the library's device producer,
+        # nothing stored: every three-index tensor is regenerated in aux
+        # blocks at every use
+        decay = cfg[4]
+        specs = {nm: L.SynthSpec(kind, N, R, 11, _tag(nm), decay)
+                 for nm, kind in (("W3", 0), ("V3", 0), ("WV3", 0), ("W3_ri", 1), ("V3_ri", 1))}
+        fp = L.synth_producer()
+
+        def produced(ao, ri, met):
+            return L.setup_base_integrals_callback(
+                t[met].data_ptr(), fp, fp if ri else None, n_ao=N, n_df=M, n_ri=R if ri else 0,
+                store_ao=False, store_ri=False, device=True,
+                user=ctypes.addressof(specs[ao]), user_ri=ctypes.addressof(specs[ri]) if ri else 0)
+
+        W = produced("W3", "W3_ri", "W2")
+        V = produced("V3", "V3_ri", "V2")
+        WV = produced("WV3", None, "WV2")
+    else:
+        W = L.setup_base_integrals(t["W3"].data_ptr(), t["W2"].data_ptr(), t["W3_ri"].data_ptr(),
+                                   n_ao=N, n_df=M, n_ri=R, device=True)
+        V = L.setup_base_integrals(t["V3"].data_ptr(), t["V2"].data_ptr(), t["V3_ri"].data_ptr(),
+                                   n_ao=N, n_df=M, n_ri=R, device=True)
+        WV = L.setup_base_integrals(t["WV3"].data_ptr(), t["WV2"].data_ptr(), None, n_ao=N,
+                                    n_df=M, device=True)
     A = L.setup_abs_projectors(t["S"].data_ptr(), N, R, device=True)
     fock_dev = torch.empty(N * N * len(occ), dtype=torch.float64, device=device)
     indirect = abs(args.s_ss) > 4 * np.finfo(float).eps
@@ -449,6 +479,7 @@ def main():
         dist.barrier()
     launches = L.launch_count() - n0
     prof = L.profile_read()
+    producer = L.profile_read_kind("producer")
     phases = {k: v / args.steps for k, v in L.profile_phases().items()}
     L.profile_enable(False)
     clk = clocks.stop()
@@ -522,6 +553,13 @@ def main():
         shapes = {"W3": N * (N + 1) // 2 * M, "V3": N * (N + 1) // 2 * M,
                   "WV3": N * (N + 1) // 2 * M, "W3_ri": R * N * M, "V3_ri": R * N * M,
                   "W2": M * M, "V2": M * M, "WV2": M * M}
+        if args.direct:
+            # gradients that fit beside the evaluation's intermediates: W's
+            # three-index tensor (the full reverse chain of one potential)
+            # and the metrics; the RI gradients are as large as the unstored
+            # RI tensors
+            for k in ("W3_ri", "V3_ri", "V3", "WV3"):
+                del shapes[k]
         gbuf = {k: torch.empty(v, dtype=torch.float64, device=device) for k, v in shapes.items()}
         gptr = {k: b.data_ptr() for k, b in gbuf.items()}
 
@@ -554,23 +592,43 @@ def main():
             torch.cuda.synchronize(device)
             return a0.elapsed_time(a1) / 1e3 / n, val
 
+        def projection(a, chunk=1 << 26):
+            """<a, r> with r a seeded Gaussian vector generated in chunks."""
+            gen = torch.Generator(device=device)
+            gen.manual_seed(5)
+            acc = 0.0
+            for i in range(0, a.numel(), chunk):
+                n = min(chunk, a.numel() - i)
+                r = torch.randn(n, dtype=torch.float64, device=device, generator=gen)
+                acc += float(torch.dot(a[i:i + n], r))
+            return acc
+
         t_fwd, e_fwd = timed(fwd_direct, args.steps)
         t_bwd, e_bwd = timed(backward, args.steps)
-        ref_g = {k: b.clone() for k, b in gbuf.items()}
+        # large gradients of the integral-direct run are compared through a
+        # random projection (a full copy would not fit beside the inputs)
+        projected = {k for k, v in shapes.items() if args.direct and v > M * M}
+        ref_p = {k: projection(gbuf[k]) for k in projected}
+        ref_g = {k: b.clone() for k, b in gbuf.items() if k not in projected}
         adjoint = {"scales": [args.s_os, 0.0], "terms": "direct (indirect_term = 0)",
                    "fp64": {"forward_s": t_fwd, "forward_backward_s": t_bwd, "energy": e_bwd,
                             "energy_equals_forward": e_bwd == e_fwd},
+                   "gradients": sorted(shapes),
                    "gradient_bytes": int(sum(v for v in shapes.values()) * 8)}
         splits = []
         for Lm in moduli:
             L.set_precision(Lm)
             t_s, e_s = timed(backward, args.steps)
             L.set_precision(0)
-            errs = {k: max_rel_diff(gbuf[k], ref_g[k]) for k in gbuf}
-            splits.append({"n_moduli": Lm, "forward_backward_s": t_s,
-                           "speedup_vs_fp64_forward_backward": t_bwd / t_s,
-                           "energy_rel_err_vs_fp64": abs(e_s - e_bwd) / abs(e_bwd),
-                           "gradient_max_rel_err_vs_fp64": errs})
+            errs = {k: max_rel_diff(gbuf[k], ref_g[k]) for k in ref_g}
+            entry = {"n_moduli": Lm, "forward_backward_s": t_s,
+                     "speedup_vs_fp64_forward_backward": t_bwd / t_s,
+                     "energy_rel_err_vs_fp64": abs(e_s - e_bwd) / abs(e_bwd),
+                     "gradient_max_rel_err_vs_fp64": errs}
+            if projected:
+                entry["gradient_projection_rel_err_vs_fp64"] = {
+                    k: abs(projection(gbuf[k]) - ref_p[k]) / abs(ref_p[k]) for k in projected}
+            splits.append(entry)
         adjoint["split_precision"] = splits
         del gbuf, ref_g
         torch.cuda.empty_cache()
@@ -704,6 +762,12 @@ def main():
             "cpu_baseline": cpu,
             "e2e": e2e,
             "phases_ms_per_step": phases,
+            "producer": ({"ms_per_step": producer["ms"] / args.steps,
+                          "calls_per_step": producer["launches"] / args.steps,
+                          "gb_per_step": producer["work"] / args.steps / 1e9,
+                          "note": "integral generation, reported separately; it is inside "
+                                  "value (the timed evaluation)"}
+                         if args.direct else None),
             "gpu_launches": int(launches),
             "clocks": clk,
             "split_precision": split,

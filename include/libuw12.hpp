@@ -10,12 +10,16 @@
 #ifndef UW12_B200_LIBUW12_HPP
 #define UW12_B200_LIBUW12_HPP
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstddef>
+#include <cstring>
+#include <exception>
 #include <fstream>
 #include <functional>
 #include <memory>
+#include <mutex>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -158,45 +162,53 @@ class BaseIntegrals {
   }
 
   /// Integrals from callbacks, one df shell per three-index call
-  /// (base_integrals.hpp:52-62).  The shells are assembled on the host and
-  /// uploaded once.
+  /// (base_integrals.hpp:52-62).  A stored tensor is produced once and kept on
+  /// the device; an unstored one is produced again, shell by shell, in the aux
+  /// blocks each use needs (integral-direct mode), so the callbacks must stay
+  /// callable for the object's lifetime and may run on several host threads.
   BaseIntegrals(const TwoIndexFn& two_index_fn, const ThreeIndexFn& three_index_fn,
                 const ThreeIndexFn& three_index_ri_fn, const std::vector<size_t>& df_sizes,
-                size_t n_ao, size_t n_df, size_t n_ri, bool /*store_ao_integrals*/ = true,
-                bool /*store_ri_integrals*/ = true) {
+                size_t n_ao, size_t n_df, size_t n_ri, bool store_ao_integrals = true,
+                bool store_ri_integrals = true) {
     check_shells(df_sizes, n_ao, n_df);
     if (n_ri == 0)
       throw std::runtime_error(
           "Three index ri integrals requested but number of ri basis functions is zero");
     const linalg::Mat J2 = two_index_fn();
-    const linalg::Mat J3 = assemble(three_index_fn, df_sizes, n_ao * (n_ao + 1) / 2, n_df);
-    const linalg::Mat J3r = assemble(three_index_ri_fn, df_sizes, n_ao * n_ri, n_df);
-    create(J3.memptr(), J2.memptr(), J3r.memptr(), n_ao, n_df, n_ri, n_df, n_df);
+    auto ao = std::make_shared<ShellProducer>(three_index_fn, df_sizes, n_ao * (n_ao + 1) / 2);
+    auto ri = std::make_shared<ShellProducer>(three_index_ri_fn, df_sizes, n_ao * n_ri);
+    create_produced(J2, ao, ri, n_ao, n_df, n_ri, store_ao_integrals, store_ri_integrals);
   }
 
   /// Callback integrals without RI (base_integrals.hpp:65-72).
   BaseIntegrals(const TwoIndexFn& two_index_fn, const ThreeIndexFn& three_index_fn,
                 const std::vector<size_t>& df_sizes, size_t n_ao, size_t n_df,
-                bool /*store_ao_integrals*/ = true) {
+                bool store_ao_integrals = true) {
     check_shells(df_sizes, n_ao, n_df);
     const linalg::Mat J2 = two_index_fn();
-    const linalg::Mat J3 = assemble(three_index_fn, df_sizes, n_ao * (n_ao + 1) / 2, n_df);
-    create(J3.memptr(), J2.memptr(), nullptr, n_ao, n_df, 0, n_df, 0);
+    auto ao = std::make_shared<ShellProducer>(three_index_fn, df_sizes, n_ao * (n_ao + 1) / 2);
+    create_produced(J2, ao, nullptr, n_ao, n_df, 0, store_ao_integrals, true);
   }
 
-  /// Stored AO integrals with RI integrals from a callback (base_integrals.hpp:78-88).
+  /// Stored AO integrals with RI integrals from a callback (base_integrals.hpp:78-88);
+  /// unless store_ri_integrals, the RI shells are produced at every use.
   BaseIntegrals(const linalg::Mat& J3_0, const linalg::Mat& J2,
                 const ThreeIndexFn& three_index_ri, const std::vector<size_t>& df_sizes,
                 bool use_ri, size_t n_ao, size_t n_df, size_t n_ri,
-                bool /*store_ri_integrals*/ = false) {
+                bool store_ri_integrals = false) {
     if (!use_ri) {
       create(J3_0.memptr(), J2.memptr(), nullptr, n_ao_from_packed(J3_0.n_rows()), J2.n_rows(),
              0, J3_0.n_cols(), 0);
       return;
     }
     check_shells(df_sizes, n_ao, n_df);
-    const linalg::Mat J3r = assemble(three_index_ri, df_sizes, n_ao * n_ri, n_df);
-    create(J3_0.memptr(), J2.memptr(), J3r.memptr(), n_ao, n_df, n_ri, J3_0.n_cols(), n_df);
+    if (J3_0.n_rows() != n_ao * (n_ao + 1) / 2 || J3_0.n_cols() != n_df)
+      throw std::runtime_error("Number of density-fitting basis functions inconsistent");
+    // J3_0's columns, copied to the device during construction only
+    auto ao = std::make_shared<ShellProducer>(nullptr, std::vector<size_t>{n_df}, J3_0.n_rows());
+    ao->stored = J3_0.memptr();
+    auto ri = std::make_shared<ShellProducer>(three_index_ri, df_sizes, n_ao * n_ri);
+    create_produced(J2, ao, ri, n_ao, n_df, n_ri, true, store_ri_integrals);
   }
 
   /// From raw pointers in host or device memory (uw12c_integrals_create).
@@ -246,21 +258,78 @@ class BaseIntegrals {
       throw std::runtime_error("total df basis functions inconsistent with number in shells");
   }
 
-  // coulomb_3idx (integral_functions.hpp:33-55): shell A fills columns
-  // offset(A) .. offset(A) + n_A.
-  static linalg::Mat assemble(const ThreeIndexFn& fn, const std::vector<size_t>& df_sizes,
-                              size_t rows, size_t n_df) {
-    linalg::Mat out(rows, n_df);
-    size_t off = 0;
-    for (size_t A = 0; A < df_sizes.size(); ++A) {
-      const linalg::Mat shell = fn(A);
-      if (shell.n_rows() != rows || shell.n_cols() != df_sizes[A])
-        throw std::logic_error("three-index shell of unexpected size");
-      for (size_t j = 0; j < shell.n_cols(); ++j)
-        for (size_t i = 0; i < rows; ++i) out(i, off + j) = shell(i, j);
-      off += df_sizes[A];
+  // A ThreeIndexFn as a uw12c_block_fn: columns [first, first + count) of
+  // the tensor come from the shells that overlap them (coulomb_3idx,
+  // integral_functions.hpp:33-55: shell A holds columns offset(A) ..
+  // offset(A) + n_A).  The first exception a shell call throws is kept and
+  // rethrown on the calling thread once the library reports the failure.
+  struct ShellProducer {
+    ShellProducer(ThreeIndexFn f, const std::vector<size_t>& df_sizes, size_t n_rows)
+        : fn(std::move(f)), rows(n_rows) {
+      offsets.push_back(0);
+      for (size_t n : df_sizes) offsets.push_back(offsets.back() + n);
     }
-    return out;
+
+    static int call(void* user, size_t first, size_t count, double* out, size_t ld,
+                    void* /*stream*/) noexcept {
+      auto* p = static_cast<ShellProducer*>(user);
+      try {
+        if (p->stored) {
+          for (size_t c = 0; c < count; ++c)
+            std::memcpy(out + c * ld, p->stored + (first + c) * p->rows, p->rows * sizeof(double));
+          return 0;
+        }
+        const size_t end = first + count;
+        size_t A = static_cast<size_t>(
+            std::upper_bound(p->offsets.begin(), p->offsets.end(), first) - p->offsets.begin());
+        for (A = A - 1; A + 1 < p->offsets.size() && p->offsets[A] < end; ++A) {
+          const linalg::Mat shell = p->fn(A);
+          if (shell.n_rows() != p->rows || shell.n_cols() != p->offsets[A + 1] - p->offsets[A])
+            throw std::logic_error("three-index shell of unexpected size");
+          const size_t c0 = std::max(first, p->offsets[A]);
+          const size_t c1 = std::min(end, p->offsets[A + 1]);
+          for (size_t c = c0; c < c1; ++c)
+            std::memcpy(out + (c - first) * ld, shell.memptr() + (c - p->offsets[A]) * p->rows,
+                        p->rows * sizeof(double));
+        }
+        return 0;
+      } catch (...) {
+        std::lock_guard<std::mutex> lock(p->mu);
+        if (!p->error) p->error = std::current_exception();
+        return 1;
+      }
+    }
+
+    void rethrow() {
+      std::lock_guard<std::mutex> lock(mu);
+      if (error) std::rethrow_exception(error);
+    }
+
+    ThreeIndexFn fn;
+    std::vector<size_t> offsets;
+    size_t rows;
+    const double* stored = nullptr;  // a tensor in memory instead of fn
+    std::mutex mu;
+    std::exception_ptr error;
+  };
+
+  void create_produced(const linalg::Mat& J2, const std::shared_ptr<ShellProducer>& ao,
+                       const std::shared_ptr<ShellProducer>& ri, size_t n_ao, size_t n_df,
+                       size_t n_ri, bool store_ao, bool store_ri) {
+    if (J2.n_rows() != n_df || J2.n_cols() != n_df)
+      throw std::runtime_error("Number of density-fitting basis functions inconsistent");
+    uw12c_integrals* h = nullptr;
+    const int status = uw12c_integrals_create_callback(
+        J2.memptr(), UW12C_MEM_HOST, &ShellProducer::call, ao.get(),
+        ri ? &ShellProducer::call : nullptr, ri.get(), n_ao, n_df, ri ? n_ri : 0, store_ao,
+        store_ri, UW12C_MEM_HOST, &h);
+    if (status != UW12C_OK) {
+      ao->rethrow();
+      if (ri) ri->rethrow();
+      detail::check(status);
+    }
+    // the producers live as long as the handle that calls them
+    h_.reset(h, [ao, ri](uw12c_integrals* p) { uw12c_integrals_destroy(p); });
   }
 
   void create(const double* X3, const double* X2, const double* X3_ri, size_t n_ao, size_t n_df,

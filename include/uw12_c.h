@@ -279,7 +279,9 @@ int uw12c_dgemm_split(long long m, long long n, long long k, double alpha, const
 /* Timing of a kernel class while profiling is on: 0 FP64 DMMA GEMM (work =
  * FLOPs), 1 whole split-precision GEMMs (FP64-equivalent FLOPs), 2 their int8
  * tensor-core kernel (int8 operations), 3 their operand preparation and 4
- * their CRT reconstruction (bytes read + written). */
+ * their CRT reconstruction (bytes read + written), 5 the three-index producer
+ * calls of integral-direct handles (bytes produced; device time on the
+ * library's stream, host producers' staging included). */
 int uw12c_profile_read_kind(int kind, unsigned long long* launches, double* ms, double* work);
 
 /* Deterministic synthetic three-index tensors written on the device (no

@@ -651,7 +651,7 @@ def split_bits(n_moduli: int, k_total: int) -> int:
     return b.value
 
 
-PROFILE_KINDS = ("dgemm", "split_gemm", "i8_mma", "split_prep", "split_crt")
+PROFILE_KINDS = ("dgemm", "split_gemm", "i8_mma", "split_prep", "split_crt", "producer")
 
 
 def profile_read_kind(kind: str) -> dict:

@@ -85,14 +85,22 @@ void eigh(double* A, size_t n, double* w) {
   if (hinfo != 0) throw_runtime("eigen-decomposition failed");
 }
 
-size_t auto_budget_doubles(size_t requested_bytes) {
+// Chunk budget in doubles: the caller's, or `fraction` (45% by default) of
+// the device memory available now (free memory plus what the library's pool
+// holds unused).  The evaluations re-read it at the start of each chunked
+// phase, after the phase's persistent intermediates are allocated.
+size_t auto_budget_doubles(size_t requested_bytes, double fraction = 0.45) {
+  if (requested_bytes)  // an explicit budget may be small (many small chunks)
+    return std::max<size_t>(requested_bytes, size_t(64) << 10) / sizeof(double);
   size_t free_b = 0, total_b = 0;
   UW12_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  size_t b = requested_bytes ? requested_bytes : static_cast<size_t>(0.45 * double(free_b));
-  // an explicit budget may be small (many small chunks); the automatic one
-  // never drops below 64 MiB
-  b = std::max<size_t>(b, requested_bytes ? size_t(64) << 10 : size_t(64) << 20);
-  return b / sizeof(double);
+  unsigned long long reserved = 0, used = 0;  // 64-bit pool attributes
+  UW12_CUDA(cudaMemPoolGetAttribute(library_pool(), cudaMemPoolAttrReservedMemCurrent, &reserved));
+  UW12_CUDA(cudaMemPoolGetAttribute(library_pool(), cudaMemPoolAttrUsedMemCurrent, &used));
+  const double avail = double(free_b) + (reserved > used ? double(reserved - used) : 0.0);
+  // the automatic budget never drops below 64 MiB
+  return std::max<size_t>(static_cast<size_t>(fraction * avail), size_t(64) << 20) /
+         sizeof(double);
 }
 
 inline long long LL(size_t v) { return static_cast<long long>(v); }
@@ -126,7 +134,19 @@ const double* aux_block(const IntegralsHandle& X, bool ri, size_t a0, size_t na,
   const AuxProducer& fn = ri ? X.ri_fn : X.ao_fn;
   if (!fn) throw_runtime(ri ? "J3_ri_0 not stored" : "J3_0 not stored");
   if (scratch.size() < rows * na) scratch.alloc(rows * na);
-  fn(a0, na, scratch.get(), rows, current_stream());
+  cudaStream_t s = current_stream();
+  if (profile_enabled()) {
+    cudaEvent_t a, b;
+    UW12_CUDA(cudaEventCreate(&a));
+    UW12_CUDA(cudaEventCreate(&b));
+    UW12_CUDA(cudaEventRecord(a, s));
+    fn(a0, na, scratch.get(), rows, s);
+    UW12_CUDA(cudaEventRecord(b, s));
+    profile_record(kProfProducer, a, b, 8.0 * double(rows) * double(na),
+                   std::string(ri ? "produce ri " : "produce ao ") + std::to_string(na));
+  } else {
+    fn(a0, na, scratch.get(), rows, s);
+  }
   return scratch.get();
 }
 
@@ -494,7 +514,7 @@ void form_fock(const FockRequest& rq) {
   const double two = (ns == 1) ? 2.0 : 1.0;
   const double kap4 = 2.0 * half;
   cudaStream_t st = current_stream();
-  const size_t budget = auto_budget_doubles(rq.mem_budget);
+  size_t budget = auto_budget_doubles(rq.mem_budget);
   // Sharding: the chunk loops (t~ dX over aux functions, same-spin 3-el
   // energy and Fock over occupied k) run over a contiguous, balanced part of
   // their index range per shard; all other contributions come from shard 0
@@ -602,6 +622,7 @@ void form_fock(const FockRequest& rq) {
     const IntegralsHandle& X = which == 0 ? W : V;
     PerX& P = which == 0 ? XW : XV;
     const size_t M = X.n_df;
+    budget = auto_budget_doubles(rq.mem_budget);
     P.B1.resize(ns);
     P.B2.resize(ns);
     P.Wst.resize(ns);
@@ -681,6 +702,13 @@ void form_fock(const FockRequest& rq) {
         wdot(ttl[sp].get(), LL(MW), tab[s].get(), LL(MW), LL(MW), LL(MV), nullptr, nullptr,
              0.5 * f, acc.get(), kE4d);
     }
+  if (!do_ind)  // the stacked transforms serve only X_AB and the same-spin terms
+    for (int s = 0; s < ns; ++s) {
+      XW.Wst[s].release();
+      XW.SV[s].release();
+      XV.Wst[s].release();
+      XV.SV[s].release();
+    }
 
   // =====================================================================
   // direct Fock: 4-el (four_electron.cpp:11-77) + 3-el X dt~ (direct_utils.cpp:164-204)
@@ -712,6 +740,13 @@ void form_fock(const FockRequest& rq) {
       gf.b_ncontig = true;
       gemm(gf);
     }
+    if (!do_ind)  // B1 and B2 serve only the direct Fock and the same-spin terms
+      for (int s = 0; s < ns; ++s) {
+        XW.B1[s].release();
+        XW.B2[s].release();
+        XV.B1[s].release();
+        XV.B2[s].release();
+      }
     // t~ dX: F[sigma'] -= sum_ab T2[a,b] G_W[a]^T S^-1 G_V[b] with
     // T2 = P2_W Tc[sigma'] P2_V^T and G_X[a] = [sq(J3_0^X[:,a]); J3ri_0^X[:,a]]
     // (R' x N).  L[a] = S^-1 G_W[a] does not depend on sigma', so it is formed
@@ -741,34 +776,47 @@ void form_fock(const FockRequest& rq) {
       T2s.push_back(std::move(T2));
     }
     if (!tdx_spins.empty()) {
-      const size_t per_a = 3 * Rp * N + np;
+      // The chunk buffers are the only large allocations of this phase, so
+      // it takes 70% of the available memory.  Unstored V blocks are
+      // produced again for every chunk of W's aux functions: the chunk takes
+      // most of the budget and V's blocks at most an eighth each; unstored W
+      // blocks add to the chunk's share.
+      budget = auto_budget_doubles(rq.mem_budget, 0.7);
+      const size_t vstep = aux_step(V, false, budget / 2), vrstep = aux_step(V, true, budget / 2);
+      const size_t vscr = (V.J3_0.get() ? 0 : np * vstep) + (V.J3_ri_0.get() ? 0 : R * N * vrstep);
+      const size_t per_a = N * N + 2 * Rp * N + (W.J3_0.get() ? 0 : np) +
+                           (W.J3_ri_0.get() ? 0 : R * N);
+      const size_t avail = budget > vscr ? budget - vscr : 0;
       const auto [alo, ahi] = part(MW);
       const size_t ac = tile_chunk(ahi - alo, 1,
-                                   std::max<size_t>(1, std::min(ahi - alo, budget / per_a)));
-      DevBuf sbuf(np * ac), Gst(Rp * N * ac), Lb(Rp * N * ac), Hb(Rp * N * ac);
+                                   std::max<size_t>(1, std::min(ahi - alo, avail / per_a)));
+      // Ga holds sq(J3_0^W[:, a]) (N x N per a), then serves as the packed s
+      // columns (N(N+1)/2 per a) of each spin
+      DevBuf Ga(N * N * ac), Lb(Rp * N * ac), Hb(Rp * N * ac);
       DevBuf scrW, scrWr, scrV, scrVr;
-      const size_t vstep = aux_step(V, false, budget), vrstep = aux_step(V, true, budget);
+      double* sbuf = Ga.get();
       for (size_t a0 = alo; a0 < ahi; a0 += ac) {
         const size_t na = std::min(ac, ahi - a0);
-        // G_W chunk, AO rows then RI rows of each (R' x N) block
-        unpack_sym(aux_block(W, false, a0, na, scrW), LL(np), LL(N), LL(na), Gst.get(), LL(Rp),
-                   LL(Rp * N));
-        copy3d(aux_block(W, true, a0, na, scrWr), LL(R), LL(R * N), Gst.get() + N, LL(Rp),
-               LL(Rp * N), LL(R), LL(N), LL(na));
-        gemm(gemm_nn(LL(Rp), LL(N * na), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp), Gst.get(), LL(Rp),
-                     0.0, Lb.get(), LL(Rp)));
+        // L[a] = S^-1 G_W[a] = S^-1[:, AO] sq(J3_0^W[:, a]) + S^-1[:, RI] J3ri_0^W[:, a],
+        // the RI block read where it lies (R x N per a, leading dimension R)
+        unpack_sym(aux_block(W, false, a0, na, scrW), LL(np), LL(N), LL(na), Ga.get(), LL(N),
+                   LL(N * N));
+        gemm(gemm_nn(LL(Rp), LL(N * na), LL(N), 1.0, AB.Sinv.get(), LL(Rp), Ga.get(), LL(N), 0.0,
+                     Lb.get(), LL(Rp)));
+        gemm(gemm_nn(LL(Rp), LL(N * na), LL(R), 1.0, AB.Sinv.get() + Rp * N, LL(Rp),
+                     aux_block(W, true, a0, na, scrWr), LL(R), 1.0, Lb.get(), LL(Rp)));
         for (size_t q = 0; q < tdx_spins.size(); ++q) {
           const double* T2 = T2s[q].get();
           // s = J3_0^V T2^T and p = J3_ri_0^V T2^T, accumulated over V's aux blocks
           for (size_t b0 = 0; b0 < MV; b0 += vstep) {
             const size_t nb = std::min(vstep, MV - b0);
             GemmDesc gs = gemm_nn(LL(np), LL(na), LL(nb), 1.0, aux_block(V, false, b0, nb, scrV),
-                                  LL(np), T2 + a0 + MW * b0, LL(MW), b0 ? 1.0 : 0.0, sbuf.get(),
+                                  LL(np), T2 + a0 + MW * b0, LL(MW), b0 ? 1.0 : 0.0, sbuf,
                                   LL(np));
             gs.b_ncontig = true;
             gemm(gs);
           }
-          unpack_sym(sbuf.get(), LL(np), LL(N), LL(na), Hb.get(), LL(Rp), LL(Rp * N));
+          unpack_sym(sbuf, LL(np), LL(N), LL(na), Hb.get(), LL(Rp), LL(Rp * N));
           for (size_t b0 = 0; b0 < MV; b0 += vrstep) {
             const size_t nb = std::min(vrstep, MV - b0);
             GemmDesc gp = gemm_nn(LL(R), LL(na), LL(nb), 1.0, aux_block(V, true, b0, nb, scrVr),
@@ -820,6 +868,7 @@ void form_fock(const FockRequest& rq) {
       clock.mark("ss_3el_energy");
       // ---- 3-el indirect energy (indirect_utils.cpp:101-133), chunked over k
       {
+        budget = auto_budget_doubles(rq.mem_budget);
         const size_t per_k = 2 * Rp * a * a;
         const auto [klo, khi] = part(o);
         const size_t kc = tile_chunk(khi - klo, a,
@@ -890,10 +939,18 @@ void form_fock(const FockRequest& rq) {
                     xhV.get(), LL(MV));
         g.b_ncontig = true;
         gemm(g);
+        budget = auto_budget_doubles(rq.mem_budget);
+        // unstored W / V blocks (accumulated over, for every k chunk) take at
+        // most an eighth of the budget each
+        size_t xscr = 0;
+        for (const IntegralsHandle* Xi : {&W, &V})
+          xscr = std::max(xscr, (Xi->J3_0.get() ? 0 : np * aux_step(*Xi, false, budget / 2)) +
+                                    (Xi->J3_ri_0.get() ? 0 : R * N * aux_step(*Xi, true, budget / 2)));
         const size_t per_k = 3 * Rp * a * N + a * (N * N + R * N + np);
         const auto [klo, khi] = part(o);
+        const size_t kavail = budget > xscr ? budget - xscr : 0;
         const size_t kc = tile_chunk(khi - klo, a,
-                                     std::max<size_t>(1, std::min(khi - klo, budget / per_k)));
+                                     std::max<size_t>(1, std::min(khi - klo, kavail / per_k)));
         DevBuf ZYV(Rp * a * N * kc), ZYW(Rp * a * N * kc), gpk(np * a * kc), Gao(N * N * a * kc),
             gri(R * N * a * kc), Wk(Rp * N * a * kc), scrX, scrXr;
         for (size_t k0 = klo; k0 < khi; k0 += kc) {
@@ -912,7 +969,8 @@ void form_fock(const FockRequest& rq) {
             gz.b_ncontig = true;
             gemm(gz);
             // gpk = J3_0 xh, gri = J3_ri_0 xh, accumulated over Xi's aux blocks
-            const size_t st_ao = aux_step(Xi, false, budget), st_ri = aux_step(Xi, true, budget);
+            const size_t st_ao = aux_step(Xi, false, budget / 2);
+            const size_t st_ri = aux_step(Xi, true, budget / 2);
             for (size_t b0 = 0; b0 < MXi; b0 += st_ao) {
               const size_t nb = std::min(st_ao, MXi - b0);
               gemm(gemm_nn(LL(np), LL(a * nk), LL(nb), 1.0, aux_block(Xi, false, b0, nb, scrX),
@@ -1077,7 +1135,7 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
   const size_t R = W.n_ri, Rp = N + R;
   const double two = (ns == 1) ? 2.0 : 1.0;
   cudaStream_t st = current_stream();
-  const size_t budget = auto_budget_doubles(rq.mem_budget);
+  size_t budget = auto_budget_doubles(rq.mem_budget);
   double F[2][2] = {{0, 0}, {0, 0}};
   for (int s = 0; s < ns; ++s)
     for (int sp = 0; sp < ns; ++sp) F[s][sp] = spin_factor(ns, s, sp, rq.s_os, rq.s_ss);
@@ -1114,6 +1172,7 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
     P.B2.resize(ns);
     P.Wst.resize(ns);
     P.SW.resize(ns);
+    budget = auto_budget_doubles(rq.mem_budget);
     DevBuf H(N * o_tot * M);
     transform_ao(X, Co.get(), o_tot, H.get(), budget / 2);
     DevBuf H2(R * a_tot * M);
@@ -1197,6 +1256,7 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
     double* g3 = gJ3[which];
     double* g3ri = gJ3ri[which];
     if (!g3 && !g3ri) continue;
+    budget = auto_budget_doubles(rq.mem_budget);
     DevBuf Bb1(N * o_tot * M), Bbri(R * a_tot * M);
     Bb1.zero();
     for (int s = 0; s < ns; ++s) {

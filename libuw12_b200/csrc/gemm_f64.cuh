@@ -84,8 +84,17 @@ void profile_reset();
 // Kernel classes: the FP64 DMMA GEMM; whole split-precision GEMMs (work =
 // FP64-equivalent 2mnk FLOPs); their int8 tcgen05 product kernel (work = int8
 // operations 2 m n K per modulus); their operand preparation and CRT
-// reconstruction kernels (work = algorithmic bytes read + written).
-enum { kProfDgemm = 0, kProfSplitGemm, kProfI8Mma, kProfSplitPrep, kProfSplitCrt, kProfKinds };
+// reconstruction kernels (work = algorithmic bytes read + written); the
+// three-index producers of integral-direct handles (work = bytes produced).
+enum {
+  kProfDgemm = 0,
+  kProfSplitGemm,
+  kProfI8Mma,
+  kProfSplitPrep,
+  kProfSplitCrt,
+  kProfProducer,
+  kProfKinds
+};
 KernelStats profile_read_kind(int kind);
 // Adds one timed launch (the events are destroyed once read).
 void profile_record(int kind, cudaEvent_t a, cudaEvent_t b, double work, std::string shape);

@@ -3,6 +3,8 @@
 // uw12_fock / uw12_energy, the callback BaseIntegrals constructor and the
 // error behaviour.  Input and output are flat binary files written and read by
 // tests/test_gpu_cpp_drop_in.py.
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <fstream>
@@ -80,6 +82,26 @@ int main(int argc, char** argv) {
   const double e_cb = uw12::uw12_energy(W_cb, V, WV, abs, orbitals, occupations, n_active,
                                         scales[0], scales[1]);
 
+  // Integral-direct: nothing stored, the shells are produced at every use;
+  // a 64 KiB budget splits every loop over aux functions into many blocks,
+  // whose edges cut through shells
+  const uw12::BaseIntegrals W_direct(two, three, three_ri, shells, n_ao, n_df, n_ri, false, false);
+  const uw12::BaseIntegrals V_direct(uw12::linalg::Mat(V3.data(), np, n_df),
+                                     uw12::linalg::Mat(V2.data(), n_df, n_df),
+                                     [&](size_t A) {
+                                       return uw12::linalg::Mat(V3r.data() + n_ri * n_ao * offsets[A],
+                                                                n_ri * n_ao, shells[A]);
+                                     },
+                                     shells, true, n_ao, n_df, n_ri, false);
+  uw12c_set_memory_budget(64 << 10);
+  std::vector<double> fock_direct(n_ao * n_ao * n_spin);
+  const double e_direct = uw12::uw12_fock(fock_direct.data(), W_direct, V_direct, WV, abs,
+                                          orbitals, occupations, n_active, scales[0], scales[1]);
+  uw12c_set_memory_budget(0);
+  double fock_direct_diff = 0;
+  for (size_t i = 0; i < fock.size(); ++i)
+    fock_direct_diff = std::max(fock_direct_diff, std::abs(fock_direct[i] - fock[i]));
+
   // Error behaviour (libuw12.cpp:61-63, utils.hpp:235-253)
   double errors = 0;
   try {
@@ -94,13 +116,26 @@ int main(int argc, char** argv) {
   } catch (const std::logic_error&) {
     errors += 1;
   }
+  try {  // a shell of the wrong size, found while the stored tensor is produced
+    const uw12::integrals::ThreeIndexFn bad = [&](size_t) { return uw12::linalg::Mat(np, 1); };
+    const uw12::BaseIntegrals W_bad(two, bad, shells, n_ao, n_df);
+  } catch (const std::logic_error&) {
+    errors += 1;
+  }
+  try {  // the same shell, found at use in integral-direct mode
+    const uw12::integrals::ThreeIndexFn bad = [&](size_t) { return uw12::linalg::Mat(np, 1); };
+    const uw12::BaseIntegrals W_bad(two, bad, three_ri, shells, n_ao, n_df, n_ri, false, true);
+    uw12::uw12_energy(W_bad, V, WV, abs, orbitals, occupations, n_active, scales[0], scales[1]);
+  } catch (const std::runtime_error&) {
+    errors += 1;
+  }
 
   std::ofstream out(argv[2], std::ios::binary);
-  const double head[4] = {e_fock, e_only, e_cb, errors};
+  const double head[6] = {e_fock, e_only, e_cb, errors, e_direct, fock_direct_diff};
   out.write(reinterpret_cast<const char*>(head), sizeof(head));
   out.write(reinterpret_cast<const char*>(fock.data()),
             static_cast<std::streamsize>(fock.size() * sizeof(double)));
-  std::printf("drop_in_check: E=%.15e (energy-only %.15e, callback integrals %.15e)\n", e_fock,
-              e_only, e_cb);
+  std::printf("drop_in_check: E=%.15e (energy-only %.15e, callback integrals %.15e, "
+              "integral-direct %.15e)\n", e_fock, e_only, e_cb, e_direct);
   return 0;
 }
