@@ -265,9 +265,9 @@ int uw12c_dgemm_noalloc(long long m, long long n, long long k, double alpha, con
  * eigensolves, energy reductions and Fock symmetrisation stay FP64. */
 int uw12c_set_precision(int n_moduli);
 /* GEMMs below min_flops stay FP64 in split-precision mode (default 2e9), and
- * so do thin ones (2mn/(m+n) < 800) and short contractions (K < 512), whose
- * operand preparation or reconstruction would cost more than the FP64
- * product; 0 routes every GEMM through the split path. */
+ * so do those whose estimated operand preparation, int8 products and
+ * reconstruction would not beat the FP64 product (thin or short ones); 0
+ * routes every GEMM through the split path. */
 int uw12c_set_split_threshold(double min_flops);
 int uw12c_split_bits(int n_moduli, long long k_total, int* bits);
 /* uw12c_dgemm computed by the split-precision GEMM with n_moduli moduli. */

@@ -778,27 +778,39 @@ void form_fock(const FockRequest& rq) {
     if (!tdx_spins.empty()) {
       // The chunk buffers are the only large allocations of this phase, so
       // it takes 70% of the available memory.  Unstored V blocks are
-      // produced again for every chunk of W's aux functions: the chunk takes
-      // most of the budget and V's blocks at most an eighth each; unstored W
-      // blocks add to the chunk's share.
+      // produced again for every chunk of W's aux functions: V's RI blocks
+      // take up to a quarter of the budget (their aux functions are the
+      // contraction length of the p GEMM, whose output is large), its AO
+      // blocks up to a sixteenth, the chunk the rest; unstored W blocks add
+      // to the chunk's share.
       budget = auto_budget_doubles(rq.mem_budget, 0.7);
-      const size_t vstep = aux_step(V, false, budget / 2), vrstep = aux_step(V, true, budget / 2);
+      const size_t vstep = aux_step(V, false, budget / 4), vrstep = aux_step(V, true, budget);
       const size_t vscr = (V.J3_0.get() ? 0 : np * vstep) + (V.J3_ri_0.get() ? 0 : R * N * vrstep);
-      const size_t per_a = N * N + 2 * Rp * N + (W.J3_0.get() ? 0 : np) +
-                           (W.J3_ri_0.get() ? 0 : R * N);
+      const size_t per_a = 2 * N * N + Rp * N + R * N + (W.J3_0.get() ? 0 : np);
       const size_t avail = budget > vscr ? budget - vscr : 0;
       const auto [alo, ahi] = part(MW);
       const size_t ac = tile_chunk(ahi - alo, 1,
                                    std::max<size_t>(1, std::min(ahi - alo, avail / per_a)));
-      // Ga holds sq(J3_0^W[:, a]) (N x N per a), then serves as the packed s
-      // columns (N(N+1)/2 per a) of each spin
-      DevBuf Ga(N * N * ac), Lb(Rp * N * ac), Hb(Rp * N * ac);
-      DevBuf scrW, scrWr, scrV, scrVr;
+      // Per chunk of W's aux functions a: Ga = sq(J3_0^W[:, a]) (N x N per a;
+      // afterwards the packed s columns of each spin), L = S^-1 G_W (R' x N
+      // per a), Hao = sq(s_a) (N x N per a) and Hr = p_a (R x N per a, RI rows
+      // nu + R mu).  When W's RI tensor is produced, its block and Hr share
+      // one buffer: the block is consumed by L before p overwrites it.
+      DevBuf Ga(N * N * ac), Lb(Rp * N * ac), Hao(N * N * ac);
+      DevBuf scrW, scrWr, scrV, scrVr, HrBuf;
       double* sbuf = Ga.get();
+      double* Hr = nullptr;
+      if (W.J3_ri_0.get()) {
+        HrBuf.alloc(R * N * ac);
+        Hr = HrBuf.get();
+      } else {
+        scrWr.alloc(R * N * ac);
+        Hr = scrWr.get();
+      }
       for (size_t a0 = alo; a0 < ahi; a0 += ac) {
         const size_t na = std::min(ac, ahi - a0);
-        // L[a] = S^-1 G_W[a] = S^-1[:, AO] sq(J3_0^W[:, a]) + S^-1[:, RI] J3ri_0^W[:, a],
-        // the RI block read where it lies (R x N per a, leading dimension R)
+        // L[a] = S^-1[:, AO] sq(J3_0^W[:, a]) + S^-1[:, RI] J3ri_0^W[:, a], the RI
+        // block read where it lies (R x N per a, leading dimension R)
         unpack_sym(aux_block(W, false, a0, na, scrW), LL(np), LL(N), LL(na), Ga.get(), LL(N),
                    LL(N * N));
         gemm(gemm_nn(LL(Rp), LL(N * na), LL(N), 1.0, AB.Sinv.get(), LL(Rp), Ga.get(), LL(N), 0.0,
@@ -807,7 +819,8 @@ void form_fock(const FockRequest& rq) {
                      aux_block(W, true, a0, na, scrWr), LL(R), 1.0, Lb.get(), LL(Rp)));
         for (size_t q = 0; q < tdx_spins.size(); ++q) {
           const double* T2 = T2s[q].get();
-          // s = J3_0^V T2^T and p = J3_ri_0^V T2^T, accumulated over V's aux blocks
+          // s = J3_0^V T2^T and p = J3_ri_0^V T2^T, accumulated over V's aux
+          // blocks; p for all AO indices mu at once (rows nu + R mu)
           for (size_t b0 = 0; b0 < MV; b0 += vstep) {
             const size_t nb = std::min(vstep, MV - b0);
             GemmDesc gs = gemm_nn(LL(np), LL(na), LL(nb), 1.0, aux_block(V, false, b0, nb, scrV),
@@ -816,25 +829,31 @@ void form_fock(const FockRequest& rq) {
             gs.b_ncontig = true;
             gemm(gs);
           }
-          unpack_sym(sbuf, LL(np), LL(N), LL(na), Hb.get(), LL(Rp), LL(Rp * N));
+          unpack_sym(sbuf, LL(np), LL(N), LL(na), Hao.get(), LL(N), LL(N * N));
           for (size_t b0 = 0; b0 < MV; b0 += vrstep) {
             const size_t nb = std::min(vrstep, MV - b0);
-            GemmDesc gp = gemm_nn(LL(R), LL(na), LL(nb), 1.0, aux_block(V, true, b0, nb, scrVr),
-                                  LL(R * N), T2 + a0 + MW * b0, LL(MW), b0 ? 1.0 : 0.0,
-                                  Hb.get() + N, LL(Rp * N));
+            GemmDesc gp = gemm_nn(LL(R * N), LL(na), LL(nb), 1.0,
+                                  aux_block(V, true, b0, nb, scrVr), LL(R * N),
+                                  T2 + a0 + MW * b0, LL(MW), b0 ? 1.0 : 0.0, Hr, LL(R * N));
             gp.b_ncontig = true;
-            gp.nbo1 = LL(N);
-            gp.sAo1 = LL(R);
-            gp.sCo1 = LL(Rp);
             gemm(gp);
           }
-          GemmDesc gf = gemm_nn(LL(N), LL(N), LL(Rp), -1.0, Lb.get(), LL(Rp), Hb.get(), LL(Rp),
-                                1.0, Fp[tdx_spins[q]].get(), LL(N));
-          gf.a_kcontig = true;
-          gf.nbr1 = LL(na);
-          gf.sAr1 = LL(Rp * N);
-          gf.sBr1 = LL(Rp * N);
-          gemm(gf);
+          // F[sigma'] -= sum_a L[a]^T [Hao[a]; Hr[a]], AO rows then RI rows of L
+          double* F = Fp[tdx_spins[q]].get();
+          GemmDesc fa = gemm_nn(LL(N), LL(N), LL(N), -1.0, Lb.get(), LL(Rp), Hao.get(), LL(N),
+                                1.0, F, LL(N));
+          fa.a_kcontig = true;
+          fa.nbr1 = LL(na);
+          fa.sAr1 = LL(Rp * N);
+          fa.sBr1 = LL(N * N);
+          gemm(fa);
+          GemmDesc fr = gemm_nn(LL(N), LL(N), LL(R), -1.0, Lb.get() + N, LL(Rp), Hr, LL(R), 1.0,
+                                F, LL(N));
+          fr.a_kcontig = true;
+          fr.nbr1 = LL(na);
+          fr.sAr1 = LL(Rp * N);
+          fr.sBr1 = LL(R * N);
+          gemm(fr);
         }
       }
     }

@@ -545,7 +545,7 @@ void gemm(const GemmDesc& d) {
     const double flops = 2.0 * double(d.m) * double(d.n) * double(d.k) * double(d.nbo1) *
                          double(d.nbo2) * double(d.nbr1) * double(d.nbr2);
     const double min_flops = split_min_flops();
-    if (flops >= min_flops && (min_flops == 0.0 || ozaki_profitable(d)) && ozaki_supported(d)) {
+    if (flops >= min_flops && (min_flops == 0.0 || ozaki_profitable(d, L)) && ozaki_supported(d)) {
       gemm_ozaki(d, L);
       return;
     }

@@ -1153,11 +1153,60 @@ void run_slabs(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
       return;
     }
   }
-  // 2. rows i / columns j
   const long long nbatch = d.nbo1 * d.nbo2;
   const long long pa = (d.sAo1 && d.nbo1 > 1 ? d.nbo1 : 1) * (d.sAo2 && d.nbo2 > 1 ? d.nbo2 : 1);
   const long long pb = (d.sBo1 && d.nbo1 > 1 ? d.nbo1 : 1) * (d.sBo2 && d.nbo2 > 1 ? d.nbo2 : 1);
-  long long ms = round_up(d.m, kTileI), ns = round_up(d.n, kTileJ);
+  // 2. long contractions into a small output: when the operands' residues
+  // exceed half the budget but the output's fit in the other half, K is cut
+  // into consecutive ranges (reduction batches, else k) whose products are
+  // reconstructed one after another and accumulated in C (beta = 1 after the
+  // first); row / column slabs would prepare each operand once per slab of
+  // the other.  A large output is cut into row / column slabs instead (each
+  // K range would reconstruct all of it).
+  const long long m_pad = round_up(d.m, kTileI), n_pad = round_up(d.n, kTileJ);
+  const long long op_bytes = L * (pa * m_pad + pb * n_pad) * round_up(k_total, kTileK);
+  const long long out_bytes = 4 * L * nbatch * m_pad * n_pad;
+  if (op_bytes > kSlabBudget / 2 && out_bytes <= kSlabBudget / 2 && k_total > kTileK) {
+    const long long pieces = (2 * op_bytes + kSlabBudget - 1) / kSlabBudget;
+    const long long nred = d.nbr1 * d.nbr2;
+    if (nred > 1) {
+      // ranges of reduction batches (r1 fastest); one r2 at a time when nbr2 > 1
+      if (d.nbr2 > 1) {
+        for (long long r2 = 0; r2 < d.nbr2; ++r2) {
+          GemmDesc e = d;
+          e.nbr2 = 1;
+          e.A += r2 * d.sAr2; e.B += r2 * d.sBr2;
+          e.sAr2 = e.sBr2 = 0;
+          if (r2 > 0) e.beta = 1.0;
+          run_slabs(e, cs, beta, s);
+        }
+        return;
+      }
+      const long long per = std::max<long long>(1, (d.nbr1 + pieces - 1) / pieces);
+      for (long long r0 = 0; r0 < d.nbr1; r0 += per) {
+        GemmDesc e = d;
+        e.nbr1 = std::min(per, d.nbr1 - r0);
+        e.A += r0 * d.sAr1; e.B += r0 * d.sBr1;
+        if (r0 > 0) e.beta = 1.0;
+        run_slabs(e, cs, beta, s);
+      }
+      return;
+    }
+    const long long kc = round_up((d.k + pieces - 1) / pieces, kTileK);
+    if (kc < d.k) {
+      for (long long k0 = 0; k0 < d.k; k0 += kc) {
+        GemmDesc e = d;
+        e.k = std::min(kc, d.k - k0);
+        e.A += k0 * (d.a_kcontig ? 1 : d.lda);
+        e.B += k0 * (d.b_ncontig ? d.ldb : 1);
+        if (k0 > 0) e.beta = 1.0;
+        run_slabs(e, cs, beta, s);
+      }
+      return;
+    }
+  }
+  // 3. rows i / columns j
+  long long ms = m_pad, ns = n_pad;
   while (slab_bytes(L, ms, ns, k_total, nbatch, pa, pb) > kSlabBudget) {
     if (ms >= ns && ms > kTileI)
       ms = round_up(ms / 2, kTileI);
@@ -1202,15 +1251,26 @@ int ozaki_bits(int n_moduli, long long k_total) {
   return std::min(beta, 50);  // |A'| <= 2^50: the FP64 rounding tricks stay exact
 }
 
-bool ozaki_profitable(const GemmDesc& d) {
-  // The operand preparation streams A and B (twice in FP64, once as L bytes
-  // per element) and costs about as much as 2mn/(m+n) ~ 800 FP64 FLOPs per
-  // operand element; thinner GEMMs are faster on the FP64 path.  The CRT
-  // reconstruction costs about as much per output element as an FP64 dot
-  // product of a few hundred terms, so short contractions stay FP64 too.
+bool ozaki_profitable(const GemmDesc& d, int n_moduli) {
+  // Estimated times on a B200 (fitted to measured kernels): operand
+  // preparation streams each operand element twice in FP64 and writes L
+  // residue bytes (~3.2 TB/s); the CRT reads L residue bytes (and C when
+  // beta != 0) and writes C (~2 TB/s); the int8 products run at ~2.2 POPS;
+  // the FP64 DMMA GEMM at ~26 TFLOP/s.  Split when it is clearly faster.
+  const double L = double(n_moduli);
+  const double k_total = double(d.k) * double(d.nbr1) * double(d.nbr2);
+  const double nbatch = double(d.nbo1) * double(d.nbo2);
+  const double pa = double(d.sAo1 && d.nbo1 > 1 ? d.nbo1 : 1) *
+                    double(d.sAo2 && d.nbo2 > 1 ? d.nbo2 : 1);
+  const double pb = double(d.sBo1 && d.nbo1 > 1 ? d.nbo1 : 1) *
+                    double(d.sBo2 && d.nbo2 > 1 ? d.nbo2 : 1);
   const double m = double(d.m), n = double(d.n);
-  const long long k_total = d.k * d.nbr1 * d.nbr2;
-  return 2.0 * m * n >= 800.0 * (m + n) && k_total >= 512;
+  const double flops = 2.0 * m * n * k_total * nbatch;
+  const double t_fp64 = flops / 26e12;
+  const double t_prep = (pa * m + pb * n) * k_total * (16.0 + L) / 3.2e12;
+  const double t_crt = nbatch * m * n * (L + 8.0 + (d.beta != 0.0 ? 8.0 : 0.0)) / 2.0e12;
+  const double t_i8 = flops * L / 2.2e15;
+  return t_prep + t_crt + t_i8 + 30e-6 < 0.9 * t_fp64;
 }
 
 bool ozaki_supported(const GemmDesc& d) {

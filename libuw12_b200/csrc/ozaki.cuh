@@ -41,9 +41,10 @@ double split_min_flops();
 void gemm_ozaki(const GemmDesc& d, int n_moduli);
 // Shapes the split-precision kernels take (K <= 8.4M, m, n <= 2^30).
 bool ozaki_supported(const GemmDesc& d);
-// Whether the split path is expected to beat the FP64 path
-// (2mn/(m+n) >= 800 and a contraction of at least 512 terms).
-bool ozaki_profitable(const GemmDesc& d);
+// Whether the split path with n_moduli moduli is expected to beat the FP64
+// path (a cost model of operand preparation, int8 products and CRT against
+// the FP64 GEMM).
+bool ozaki_profitable(const GemmDesc& d, int n_moduli);
 
 // beta (bits kept per operand element) for n_moduli moduli and a contraction
 // of k_total terms.

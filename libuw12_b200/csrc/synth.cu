@@ -2,6 +2,7 @@
 // uw12c_synth_three_index).  Same counter-based formula as the Python test
 // generator: key = mix(mix(seed) ^ tag); h_k = mix(key + 2e + k);
 // g = sqrt(-2 ln u1) cos(2 pi u2); value = g * exp(-|p - q| / decay).
+#include <algorithm>
 #include <cmath>
 
 #include "common.cuh"
@@ -19,20 +20,15 @@ __host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long 
 
 // Columns [first, first + count) of the tensor (rows x n_df), written with
 // leading dimension ld; element e of the full tensor is e = r + rows * column.
-__global__ void k_synth(double* out, long long ld, int kind, long long n_ao, long long n_ri,
-                        long long rows, long long first, long long total,
-                        unsigned long long key, double inv_decay) {
+// One thread per row (grid-stride), looping over the columns: the row's index
+// pair and decay factor are computed once, and consecutive threads write
+// consecutive rows of each column.
+__global__ void k_synth(double* out, long long ld, int kind, long long n_ri, long long rows,
+                        long long first, long long count, unsigned long long key,
+                        double inv_decay) {
   const double two_pi = 6.283185307179586476925286766559;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long long)gridDim.x * blockDim.x) {
-    const long long r = idx % rows, col = idx / rows;
-    const long long e = r + rows * (first + col);
-    const unsigned long long base = key + 2ULL * static_cast<unsigned long long>(e);
-    const unsigned long long h0 = mix64(base);
-    const unsigned long long h1 = mix64(base + 1ULL);
-    const double u1 = (static_cast<double>(h0 >> 11) + 1.0) * 0x1.0p-53;
-    const double u2 = static_cast<double>(h1 >> 11) * 0x1.0p-53;
-    const double g = sqrt(-2.0 * log(u1)) * cos(two_pi * u2);
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < rows;
+       r += (long long)gridDim.x * blockDim.x) {
     long long p, q;
     if (kind == 0) {
       long long i = static_cast<long long>((sqrt(8.0 * double(r) + 1.0) - 1.0) * 0.5);
@@ -45,7 +41,17 @@ __global__ void k_synth(double* out, long long ld, int kind, long long n_ao, lon
       q = r / n_ri;
     }
     const long long d = p > q ? p - q : q - p;
-    out[r + ld * col] = g * exp(-double(d) * inv_decay);
+    const double w = exp(-double(d) * inv_decay);
+    for (long long col = 0; col < count; ++col) {
+      const long long e = r + rows * (first + col);
+      const unsigned long long base = key + 2ULL * static_cast<unsigned long long>(e);
+      const unsigned long long h0 = mix64(base);
+      const unsigned long long h1 = mix64(base + 1ULL);
+      const double u1 = (static_cast<double>(h0 >> 11) + 1.0) * 0x1.0p-53;
+      const double u2 = static_cast<double>(h1 >> 11) * 0x1.0p-53;
+      const double g = sqrt(-2.0 * log(u1)) * cos(two_pi * u2);
+      out[r + ld * col] = g * w;
+    }
   }
 }
 
@@ -59,13 +65,12 @@ void synth_three_index_block(double* out, size_t ld, int kind, size_t n_ao, size
   const long long rows = kind == 0 ? static_cast<long long>(n_ao * (n_ao + 1) / 2)
                                    : static_cast<long long>(n_ri * n_ao);
   if (ld < static_cast<size_t>(rows)) throw Error(kErrInvalid, "synth: ld smaller than the rows");
-  const long long total = rows * static_cast<long long>(count);
-  if (total <= 0) return;
+  if (rows <= 0 || count == 0) return;
   const unsigned long long key = mix64(mix64(seed) ^ tag);
-  k_synth<<<148 * 32, 256, 0, stream>>>(out, static_cast<long long>(ld), kind,
-                                         static_cast<long long>(n_ao),
-                                         static_cast<long long>(n_ri), rows,
-                                         static_cast<long long>(first), total, key, 1.0 / decay);
+  const long long blocks = std::min<long long>((rows + 255) / 256, 148LL * 32);
+  k_synth<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(
+      out, static_cast<long long>(ld), kind, static_cast<long long>(n_ri), rows,
+      static_cast<long long>(first), static_cast<long long>(count), key, 1.0 / decay);
   UW12_LAUNCHED();
 }
 

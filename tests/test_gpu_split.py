@@ -7,7 +7,8 @@ reconstruction) on the GPU.
   within the scheme's bound 2^-beta (max|a_i.| sum|b_.j| + sum|a_i.| max|b_.j|)
   plus FP64 rounding of the reference.
 * Output batches (operands shared or per batch), reduction batches,
-  alpha / beta, K beyond one 65536-byte accumulator chunk.
+  alpha / beta, K beyond one 65536-byte accumulator chunk, and contractions
+  long enough to run as several K ranges accumulated in C.
 * Whole evaluations with every GEMM routed through the split path: the
   same parity tolerances as the FP64 path against the oracle at 14 moduli,
   and 1e-6 relative at 8 moduli.
@@ -148,6 +149,41 @@ def test_long_contraction_uses_several_accumulator_chunks(uw12lib, cuda_device):
                         dC.data_ptr(), m, n_moduli=12)
     torch.cuda.synchronize()
     ref = A.reshape((m, k), order="F") @ B.reshape((k, n), order="F")
+    assert np.array_equal(dC.cpu().numpy().reshape((m, n), order="F"), ref)
+
+
+@pytest.mark.parametrize("nbr1,a_k,b_n", [(1, False, False), (100, True, True)])
+def test_contraction_cut_into_k_ranges(uw12lib, cuda_device, nbr1, a_k, b_n):
+    """K = 1.2e6 (one range, or 100 reduction batches of 12000): the operands'
+    residues (14 x (128 + 256) x K bytes) exceed the temporaries budget, so
+    the contraction runs as consecutive K ranges accumulated in C; small
+    integers keep every range exact, so the result equals the FP64 product."""
+    import torch
+    rng = np.random.default_rng(17)
+    m, n, k_total = 40, 24, 1_200_000
+    k = k_total // nbr1
+    Am = rng.integers(-8, 9, (m, k_total)).astype(np.float64)
+    Bm = rng.integers(-8, 9, (k_total, n)).astype(np.float64)
+    # reduction batch r holds columns [r k, (r + 1) k) of Am and rows of Bm
+    if a_k:  # A(i, kk) at A[kk + k i] within each batch of k m elements
+        A = np.concatenate([Am[:, r * k:(r + 1) * k].reshape(-1) for r in range(nbr1)])
+        lda, sAr1 = k, k * m
+    else:
+        A = Am.reshape(-1, order="F")
+        lda, sAr1 = m, m * k
+    if b_n:  # B(kk, j) at B[j + n kk]
+        B = Bm.reshape(-1)
+        ldb, sBr1 = n, n * k
+    else:
+        B = Bm.reshape(-1, order="F")
+        ldb, sBr1 = k_total, k
+    dA, dB = _dev(torch, A), _dev(torch, B)
+    dC = torch.full((m * n,), 3.0, dtype=torch.float64, device="cuda")
+    uw12lib.dgemm_split(m, n, k, 1.0, dA.data_ptr(), lda, a_k, dB.data_ptr(), ldb, b_n, 0.5,
+                        dC.data_ptr(), m, nbr1=nbr1, sr=(sAr1, 0, sBr1, 0) if nbr1 > 1
+                        else (0, 0, 0, 0), n_moduli=14)
+    torch.cuda.synchronize()
+    ref = Am @ Bm + 1.5
     assert np.array_equal(dC.cpu().numpy().reshape((m, n), order="F"), ref)
 
 
