@@ -694,14 +694,16 @@ struct CrtArgs {
   double w[kOzakiMaxModuli][kMaxChunks];
   double mc[kMaxChunks];
   double inv_m;
-  int cw;  // CRT chunk width in bits
+  int cw;          // CRT chunk width in bits
+  int c_aligned;   // C, ldc and the batch strides allow 16-byte accesses
 };
 
 // One thread = 4 consecutive rows i of a column j of one batch; grid (row
 // blocks of 1024, columns strided by gridDim.y, batches).  The L residue words
-// of a column are loaded before any is used (one load per modulus and K chunk
-// in flight per thread), the K-chunk sums of the 4 bytes are kept as pairs of
-// 16-bit lanes, and the CRT runs on NCH chunks of cw bits.
+// of a column (and the 4 elements of C when beta != 0) are loaded before any
+// is used (one load per modulus and K chunk in flight per thread), the K-chunk
+// sums of the 4 bytes are kept as pairs of 16-bit lanes, the CRT runs on NCH
+// chunks of cw bits, and C is read and written 16 bytes at a time when aligned.
 // x 2^e: one multiply by an exactly representable power of two when 2^e is a
 // normal double, ldexp otherwise.
 __device__ __forceinline__ double scale_pow2(double x, int e) {
@@ -773,13 +775,28 @@ __global__ void __launch_bounds__(256, 2) k_crt(const CrtArgs a) {
     sa[e] = i0 + e < a.m ? a.shift_a[pa * a.rows_a + i0 + e] : 0;
   const double chunk = __longlong_as_double(static_cast<long long>(a.cw + 1023) << 52);  // 2^cw
 
+  const bool vec = i0 + 3 < a.m && a.c_aligned;
   for (long long j = blockIdx.y; j < a.n; j += gridDim.y) {
     const uint8_t* base = a.R + (static_cast<long long>(b) * a.n_pad + j) * a.L * a.m_pad + i0;
-    // one residue word (4 rows) per modulus and K chunk, all loads issued first
+    double* Cb = a.C + b1 * a.sCo1 + b2 * a.sCo2 + j * a.ldc;
+    // one residue word (4 rows) per modulus and K chunk, and the 4 elements of
+    // C when they are accumulated into: all loads issued first
     uint32_t w0[kOzakiMaxModuli];
 #pragma unroll
     for (int l = 0; l < kOzakiMaxModuli; ++l)
       if (l < a.L) w0[l] = __ldg(reinterpret_cast<const uint32_t*>(base + l * lstride));
+    double cold[4] = {0.0, 0.0, 0.0, 0.0};
+    if (a.beta != 0.0) {
+      if (vec) {
+        const double2 c01 = *reinterpret_cast<const double2*>(Cb + i0);
+        const double2 c23 = *reinterpret_cast<const double2*>(Cb + i0 + 2);
+        cold[0] = c01.x; cold[1] = c01.y; cold[2] = c23.x; cold[3] = c23.y;
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (i0 + e < a.m) cold[e] = Cb[i0 + e];
+      }
+    }
     double S[4][NCH];
 #pragma unroll
     for (int e = 0; e < 4; ++e)
@@ -834,11 +851,9 @@ __global__ void __launch_bounds__(256, 2) k_crt(const CrtArgs a) {
       }
     }
     const int sb = a.shift_b[pb * a.rows_b + j];
-    double* Cb = a.C + b1 * a.sCo1 + b2 * a.sCo2 + j * a.ldc;
+    double out[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
-      const long long i = i0 + e;
-      if (i >= a.m) break;
       double approx = 0.0;
 #pragma unroll
       for (int c = NCH - 1; c >= 0; --c) approx = fma(approx, chunk, S[e][c]);
@@ -846,9 +861,16 @@ __global__ void __launch_bounds__(256, 2) k_crt(const CrtArgs a) {
       double dig[NCH];
 #pragma unroll
       for (int c = 0; c < NCH; ++c) dig[c] = fma(-q, a.mc[c], S[e][c]);  // exact
-      double out = a.alpha * scale_pow2(join_chunks<NCH>(dig, chunk), -(sa[e] + sb));
-      if (a.beta != 0.0) out = fma(a.beta, Cb[i], out);
-      Cb[i] = out;
+      out[e] = a.alpha * scale_pow2(join_chunks<NCH>(dig, chunk), -(sa[e] + sb));
+      if (a.beta != 0.0) out[e] = fma(a.beta, cold[e], out[e]);
+    }
+    if (vec) {
+      *reinterpret_cast<double2*>(Cb + i0) = make_double2(out[0], out[1]);
+      *reinterpret_cast<double2*>(Cb + i0 + 2) = make_double2(out[2], out[3]);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (i0 + e < a.m) Cb[i0 + e] = out[e];
     }
   }
 }
@@ -1085,6 +1107,8 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
     for (int c = 0; c < kMaxChunks; ++c) ca.mc[c] = cs.mc[c];
     ca.inv_m = cs.inv_m;
     ca.cw = cs.cw;
+    ca.c_aligned = (reinterpret_cast<std::uintptr_t>(d.C) % 16 == 0) && d.ldc % 2 == 0 &&
+                   d.sCo1 % 2 == 0 && d.sCo2 % 2 == 0;
     const double bytes = double(splits * L) * double(d.m * d.n * nbatch) +
                          8.0 * double(d.m * d.n * nbatch) * (d.beta != 0.0 ? 2.0 : 1.0);
     Timer tm(kProfSplitCrt, bytes, "crt", s);
