@@ -362,6 +362,59 @@ def config_dict(args):
 # --------------------------------------------------------------------------
 # main arm
 # --------------------------------------------------------------------------
+def gemm_probe(args):
+    """One GEMM shape on both paths: `--warmup` untimed and `--steps` timed calls
+    each, CUDA events on the library's stream, kernel-class times of the split
+    path (one JSON line)."""
+    import torch
+    import libuw12_b200 as L
+    dims = [int(x) for x in args.gemm.split(",")]
+    m, n, k = dims[:3]
+    beta = float(dims[3]) if len(dims) > 3 else 0.0
+    moduli = [int(x) for x in args.split_moduli.split(",") if x.strip()] or [14]
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    L.lib()
+    stream = torch.cuda.current_stream(device)
+    L.set_stream(stream.cuda_stream)
+    g = torch.Generator(device=device)
+    g.manual_seed(3)
+    A = torch.randn(m * k, dtype=torch.float64, device=device, generator=g)
+    B = torch.randn(k * n, dtype=torch.float64, device=device, generator=g)
+    C = torch.zeros(m * n, dtype=torch.float64, device=device)
+    gargs = (m, n, k, 1.0, A.data_ptr(), m, False, B.data_ptr(), k, False, beta, C.data_ptr(), m)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        return e0.elapsed_time(e1) / args.steps
+
+    flops = 2.0 * m * n * k
+    out = {"gemm": [m, n, k], "beta": beta, "fp64_ms": timed(lambda: L.dgemm(*gargs))}
+    out["fp64_tflops"] = flops / out["fp64_ms"] / 1e9
+    Lm = moduli[0]
+    for _ in range(args.warmup):
+        L.dgemm_split(*gargs, n_moduli=Lm)
+    torch.cuda.synchronize(device)
+    L.profile_enable(True)
+    out[f"split{Lm}_ms"] = timed(lambda: L.dgemm_split(*gargs, n_moduli=Lm))
+    n_calls = args.steps + args.warmup
+    for kind in ("i8_mma", "split_prep", "split_crt"):
+        r = L.profile_read_kind(kind)
+        out[f"split{Lm}_{kind}"] = {"ms_per_call": r["ms"] / n_calls,
+                                    "work_per_s": r["work"] / (r["ms"] / 1e3) if r["ms"] else None}
+    L.profile_enable(False)
+    out["speedup"] = out["fp64_ms"] / out[f"split{Lm}_ms"]
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -386,7 +439,15 @@ def main():
     ap.add_argument("--split-moduli", default="14,10",
                     help="moduli counts of the split-precision runs reported beside the FP64 "
                          "headline ('' = none)")
+    ap.add_argument("--gemm", default="",
+                    help="instead of the workload: time one GEMM shape 'm,n,k[,beta]' (A m x k "
+                         "m-contiguous, B k x n k-contiguous, FP64 N(0,1)) on the FP64 path and "
+                         "the split path with the first --split-moduli count (kernel profiling "
+                         "probe)")
     args = ap.parse_args()
+    if args.gemm:
+        gemm_probe(args)
+        return
     if args.direct:  # the host-side arms need every tensor in memory
         args.no_e2e = args.no_cpu_baseline = args.no_batched = True
 
@@ -653,22 +714,33 @@ def main():
             dist.barrier()
         torch.cuda.synchronize(device)
         t0 = time.perf_counter()
+        stages = {}
         for _ in range(args.e2e_steps):
+            ts = time.perf_counter()
             We = L.setup_base_integrals(hp["W3"].reshape((np_, M), order="F"),
                                         hp["W2"].reshape((M, M)),
                                         hp["W3_ri"].reshape((R * N, M), order="F"))
+            stages["setup_W_s"] = time.perf_counter() - ts
+            ts = time.perf_counter()
             Ve = L.setup_base_integrals(hp["V3"].reshape((np_, M), order="F"),
                                         hp["V2"].reshape((M, M)),
                                         hp["V3_ri"].reshape((R * N, M), order="F"))
+            stages["setup_V_s"] = time.perf_counter() - ts
+            ts = time.perf_counter()
             WVe = L.setup_base_integrals(hp["WV3"].reshape((np_, M), order="F"),
                                          hp["WV2"].reshape((M, M)))
+            stages["setup_WV_s"] = time.perf_counter() - ts
+            ts = time.perf_counter()
             Ae = L.setup_abs_projectors(hp["S"].reshape((N + R, N + R)), N, R)
+            stages["setup_abs_s"] = time.perf_counter() - ts
+            ts = time.perf_counter()
             if world > 1:
                 e_e2e = evaluate(We, Ve, WVe, Ae, fock_dev)
                 fock_host = fock_dev.cpu()
             else:
                 e_e2e, fock_host = L.uw12_fock(We, Ve, WVe, Ae, orbs, occs, act, args.s_os,
                                                args.s_ss)
+            stages["fock_s"] = time.perf_counter() - ts
             for h in (We, Ve, WVe, Ae):
                 h.close()
         torch.cuda.synchronize(device)
@@ -681,7 +753,8 @@ def main():
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "includes": "H2D of all integrals from pinned host memory, metric/overlap "
                            "eigensolves, evaluation, Fock D2H",
-               "energy_rel_diff_vs_value_arm": abs(e_e2e - energy) / abs(energy)}
+               "energy_rel_diff_vs_value_arm": abs(e_e2e - energy) / abs(energy),
+               "last_step_stages": stages}
 
     # ---- CPU baseline on a bounded sample (rank 0, N = 1)
     cpu = None

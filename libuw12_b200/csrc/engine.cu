@@ -59,12 +59,29 @@ void require_symmetric(const double* A, size_t n, const char* msg) {
   if (!(h[0] <= 1e-10 * std::max(1.0, h[1]))) throw_logic(msg);
 }
 
+// One cuSOLVER handle per host thread and device, created on first use.
+cusolverDnHandle_t solver_handle() {
+  struct Handles {
+    std::map<int, cusolverDnHandle_t> h;
+    ~Handles() {
+      for (auto& kv : h) cusolverDnDestroy(kv.second);
+    }
+  };
+  thread_local Handles handles;
+  int dev = 0;
+  UW12_CUDA(cudaGetDevice(&dev));
+  auto it = handles.h.find(dev);
+  if (it != handles.h.end()) return it->second;
+  cusolverDnHandle_t h = nullptr;
+  solver_check(cusolverDnCreate(&h), "cusolverDnCreate");
+  handles.h[dev] = h;
+  return h;
+}
+
 // Ascending eigenpairs of a symmetric n x n matrix, in place (A -> vectors).
 void eigh(double* A, size_t n, double* w) {
   cudaStream_t s = current_stream();
-  cusolverDnHandle_t h = nullptr;
-  solver_check(cusolverDnCreate(&h), "cusolverDnCreate");
-  struct Guard { cusolverDnHandle_t h; ~Guard() { cusolverDnDestroy(h); } } guard{h};
+  cusolverDnHandle_t h = solver_handle();
   solver_check(cusolverDnSetStream(h, s), "cusolverDnSetStream");
   int lwork = 0;
   solver_check(cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
@@ -107,6 +124,37 @@ inline long long LL(size_t v) { return static_cast<long long>(v); }
 
 // Metric eigendecomposition (base_integrals.cpp:155-166): P2 = Q pinv(Lambda),
 // df_vals = Lambda, after libuw12's symmetry check.
+// A non-blocking stream that starts after the work already on `parent`;
+// join() makes `parent` wait for it and waits for it on the host.  The
+// destructor (also on an error path) waits for it before destroying it, so
+// nothing it reads or writes is released while in flight.
+class SideStream {
+ public:
+  explicit SideStream(cudaStream_t parent) : parent_(parent) {
+    UW12_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
+    UW12_CUDA(cudaEventCreateWithFlags(&ev_, cudaEventDisableTiming));
+    UW12_CUDA(cudaEventRecord(ev_, parent_));
+    UW12_CUDA(cudaStreamWaitEvent(s_, ev_, 0));
+  }
+  SideStream(const SideStream&) = delete;
+  SideStream& operator=(const SideStream&) = delete;
+  ~SideStream() {
+    cudaStreamSynchronize(s_);
+    cudaEventDestroy(ev_);
+    cudaStreamDestroy(s_);
+  }
+  cudaStream_t get() const { return s_; }
+  void join() {
+    UW12_CUDA(cudaEventRecord(ev_, s_));
+    UW12_CUDA(cudaStreamWaitEvent(parent_, ev_, 0));
+    UW12_CUDA(cudaStreamSynchronize(s_));
+  }
+
+ private:
+  cudaStream_t parent_ = nullptr, s_ = nullptr;
+  cudaEvent_t ev_ = nullptr;
+};
+
 void setup_metric(IntegralsHandle* h, const double* X2, bool device_mem) {
   cudaStream_t s = current_stream();
   const size_t n_df = h->n_df;
@@ -180,12 +228,16 @@ IntegralsHandle* integrals_create(const double* X3, const double* X2, const doub
     h->n_ri = X3_ri ? n_ri : 0;
     const size_t np = packed_size(n_ao);
     h->J3_0.alloc(np * n_df);
-    upload(h->J3_0.get(), X3, np * n_df, device_mem, s);
-    if (X3_ri) {
-      h->J3_ri_0.alloc(n_ri * n_ao * n_df);
-      upload(h->J3_ri_0.get(), X3_ri, n_ri * n_ao * n_df, device_mem, s);
-    }
+    if (X3_ri) h->J3_ri_0.alloc(n_ri * n_ao * n_df);
+    // The three-index copies run on a side stream (after the caller's work on
+    // the current stream, which may have produced device inputs) while the
+    // metric is diagonalised on the current stream; both are complete when
+    // this returns.
+    SideStream side(s);
+    upload(h->J3_0.get(), X3, np * n_df, device_mem, side.get());
+    if (X3_ri) upload(h->J3_ri_0.get(), X3_ri, n_ri * n_ao * n_df, device_mem, side.get());
     setup_metric(h, X2, device_mem);
+    side.join();
   } catch (...) {
     delete h;
     throw;

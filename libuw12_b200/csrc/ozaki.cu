@@ -302,6 +302,13 @@ __global__ void __launch_bounds__(256) k_residues(OperandView v, const int* __re
   __syncthreads();
   const int tid = threadIdx.x;
   const int c4 = (tid & 31) * 4;
+  // Each lane takes its 4 consecutive k in an order rotated by rot = (lane /
+  // 4) mod 4, so that the warp's reads of tile[r][c4 + ...] fall in 16
+  // distinct 8-byte bank pairs (two wavefronts, the minimum for 256 bytes);
+  // the packed residue word is rotated back before the store.
+  const int rot = ((tid & 31) >> 2) & 3;
+  const int q0 = c4 + (rot & 3), q1 = c4 + ((rot + 1) & 3), q2 = c4 + ((rot + 2) & 3),
+            q3 = c4 + ((rot + 3) & 3);
   for (int it = 0; it < 4; ++it) {
     const int r = it * 8 + tid / 32;
     const long long row = row0 + r;
@@ -309,18 +316,18 @@ __global__ void __launch_bounds__(256) k_residues(OperandView v, const int* __re
     // row of modulus 0 in the residue layout ((plane * tiles + tile) * L + l) * tile_rows + r
     const long long tile_base =
         ((plane * (rows_pad / tile_rows) + row / tile_rows) * mods.L) * tile_rows + row % tile_rows;
-    double x0, x1, x2, x3;
+    double x0, x1, x2, x3;  // elements k0 + q0 .. q3
     if (sh > -1000 && sh < 1000) {  // 2^sh is a normal double: scale by one multiply
       const double sc = ldexp(1.0, sh);
-      x0 = round_int(tile[r][c4] * sc);
-      x1 = round_int(tile[r][c4 + 1] * sc);
-      x2 = round_int(tile[r][c4 + 2] * sc);
-      x3 = round_int(tile[r][c4 + 3] * sc);
+      x0 = round_int(tile[r][q0] * sc);
+      x1 = round_int(tile[r][q1] * sc);
+      x2 = round_int(tile[r][q2] * sc);
+      x3 = round_int(tile[r][q3] * sc);
     } else {
-      x0 = round_int(ldexp(tile[r][c4], sh));
-      x1 = round_int(ldexp(tile[r][c4 + 1], sh));
-      x2 = round_int(ldexp(tile[r][c4 + 2], sh));
-      x3 = round_int(ldexp(tile[r][c4 + 3], sh));
+      x0 = round_int(ldexp(tile[r][q0], sh));
+      x1 = round_int(ldexp(tile[r][q1], sh));
+      x2 = round_int(ldexp(tile[r][q2], sh));
+      x3 = round_int(ldexp(tile[r][q3], sh));
     }
     const int v0 = int_of(x0), v1 = int_of(x1), v2 = int_of(x2), v3 = int_of(x3);
     uint8_t* dst = out + tile_base * k_pad + k0 + c4;
@@ -333,7 +340,9 @@ __global__ void __launch_bounds__(256) k_residues(OperandView v, const int* __re
           __byte_perm(residue_low(v0, x0, ip, p), residue_low(v1, x1, ip, p), 0x0040);
       const uint32_t hi =
           __byte_perm(residue_low(v2, x2, ip, p), residue_low(v3, x3, ip, p), 0x0040);
-      *reinterpret_cast<uint32_t*>(dst) = __byte_perm(lo, hi, 0x5410);
+      // byte i holds element (i + rot) mod 4: rotate left by rot bytes
+      const uint32_t w = __byte_perm(lo, hi, 0x5410);
+      *reinterpret_cast<uint32_t*>(dst) = __funnelshift_l(w, w, 8 * rot);
       dst += lstep;
     }
   }
