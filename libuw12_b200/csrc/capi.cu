@@ -4,6 +4,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -465,57 +466,140 @@ namespace {
 // block is split into column groups) that is copied to the device; the buffer
 // is reused under a mutex, so producers may be called from several host
 // threads (batched evaluations) one at a time per tensor.
+// A user producer.  Device producers are called directly.  Host producers
+// write into pinned stages that are copied to the device on the caller's
+// stream; two stages and a read-ahead thread overlap the user's function
+// with the GPU: after block [first, first + count) is staged, the next
+// range (the same count after it, or from 0 again at the end of the aux
+// range, where loops restart) is produced in the background into the other
+// stage, and a request for exactly that range takes it from there.  A stage
+// is rewritten only after its last copy has completed (an event per stage);
+// the caller's stream is not synchronised.
 struct UserProducer {
-  static constexpr size_t kStageDoubles = size_t(1) << 25;  // 256 MiB
-  uw12c_block_fn fn;
-  void* user;
-  bool host;
-  size_t rows;
-  std::mutex mu;
-  double* stage = nullptr;
-  size_t stage_n = 0;
+  static constexpr size_t kStageDoubles = size_t(1) << 25;  // 256 MiB per stage
+  uw12c_block_fn fn = nullptr;
+  void* user = nullptr;
+  bool host = false;
+  size_t rows = 0, n_df = 0;
+  std::mutex mu;  // one request at a time (handles may be shared by host threads)
+  struct Stage {
+    double* p = nullptr;
+    size_t n = 0;
+    cudaEvent_t copied = nullptr;  // last copy out of this stage
+  } stage[2];
+  // read-ahead job: range, stage, and its completion / failure
+  std::thread ahead;
+  bool ahead_on = false;
+  size_t ahead_first = 0, ahead_count = 0;
+  int ahead_stage = 0;
+  int ahead_rc = 0;
+  std::exception_ptr ahead_err;
+
   ~UserProducer() {
-    if (stage) cudaFreeHost(stage);
+    if (ahead.joinable()) ahead.join();
+    for (auto& st : stage) {
+      if (st.copied) cudaEventDestroy(st.copied);
+      if (st.p) cudaFreeHost(st.p);
+    }
   }
+
+  void check(int rc) const {
+    if (rc != 0)
+      throw uw12b::Error(UW12C_ERR_RUNTIME,
+                         "three-index integral callback returned " + std::to_string(rc));
+  }
+
+  void ensure(Stage& st, size_t n) {
+    if (!st.copied) UW12_CUDA(cudaEventCreateWithFlags(&st.copied, cudaEventDisableTiming));
+    if (st.n >= n) return;
+    UW12_CUDA(cudaEventSynchronize(st.copied));
+    if (st.p) cudaFreeHost(st.p);
+    st.p = nullptr;
+    st.n = 0;
+    UW12_CUDA(cudaMallocHost(reinterpret_cast<void**>(&st.p), n * sizeof(double)));
+    st.n = n;
+  }
+
+  // Waits for the read-ahead job; true when it produced [first, first + count).
+  bool take_ahead(size_t first, size_t count, int* which) {
+    if (!ahead_on) return false;
+    ahead.join();
+    ahead_on = false;
+    if (ahead_err) {
+      auto e = ahead_err;
+      ahead_err = nullptr;
+      if (ahead_first == first && ahead_count == count) std::rethrow_exception(e);
+      return false;
+    }
+    if (ahead_first != first || ahead_count != count) return false;
+    check(ahead_rc);
+    *which = ahead_stage;
+    return true;
+  }
+
   void operator()(size_t first, size_t count, double* out, size_t ld, cudaStream_t s) {
-    auto call = [&](size_t f, size_t c, double* o, size_t l) {
-      const int rc = fn(user, f, c, o, l, static_cast<void*>(s));
-      if (rc != 0)
-        throw uw12b::Error(UW12C_ERR_RUNTIME,
-                           "three-index integral callback returned " + std::to_string(rc));
-    };
     if (!host) {
-      call(first, count, out, ld);
+      check(fn(user, first, count, out, ld, static_cast<void*>(s)));
       return;
     }
     std::lock_guard<std::mutex> lk(mu);
     const size_t per = std::max<size_t>(1, std::min(count, kStageDoubles / rows));
-    if (stage_n < rows * per) {
-      if (stage) cudaFreeHost(stage);
-      stage = nullptr;
-      stage_n = 0;
-      UW12_CUDA(cudaMallocHost(reinterpret_cast<void**>(&stage), rows * per * sizeof(double)));
-      stage_n = rows * per;
+    int which = 0;
+    if (take_ahead(first, count, &which)) {  // (always joins a pending read-ahead)
+      stage_out(which, count, out, ld, s);
+    } else {
+      // produced here, one stage-sized piece at a time
+      for (size_t c0 = 0; c0 < count; c0 += per) {
+        const size_t nc = std::min(per, count - c0);
+        which = 1 - which;
+        Stage& st = stage[which];
+        ensure(st, rows * per);
+        UW12_CUDA(cudaEventSynchronize(st.copied));  // its previous copy is done
+        check(fn(user, first + c0, nc, st.p, rows, static_cast<void*>(s)));
+        stage_out(which, nc, out + ld * c0, ld, s);
+      }
+      if (count > per) return;  // no read-ahead for blocks larger than a stage
     }
-    for (size_t c0 = 0; c0 < count; c0 += per) {
-      const size_t nc = std::min(per, count - c0);
-      UW12_CUDA(cudaStreamSynchronize(s));  // the previous copy out of the stage is done
-      call(first + c0, nc, stage, rows);
-      UW12_CUDA(cudaMemcpy2DAsync(out + ld * c0, ld * sizeof(double), stage,
-                                  rows * sizeof(double), rows * sizeof(double), nc,
-                                  cudaMemcpyHostToDevice, s));
-    }
-    UW12_CUDA(cudaStreamSynchronize(s));
+    // read ahead the next range into the other stage
+    size_t nf = first + count, nc = count;
+    if (nf >= n_df) nf = 0;
+    nc = std::min(nc, n_df - nf);
+    if (nc == 0) return;
+    const int other = 1 - which;
+    ensure(stage[other], rows * per);
+    ahead_first = nf;
+    ahead_count = nc;
+    ahead_stage = other;
+    ahead_rc = 0;
+    ahead_err = nullptr;
+    ahead_on = true;
+    ahead = std::thread([this, nf, nc, other, s] {
+      try {
+        UW12_CUDA(cudaEventSynchronize(stage[other].copied));
+        ahead_rc = fn(user, nf, nc, stage[other].p, rows, static_cast<void*>(s));
+      } catch (...) {
+        ahead_err = std::current_exception();
+      }
+    });
+  }
+
+  void stage_out(int which, size_t nc, double* out, size_t ld, cudaStream_t s) {
+    Stage& st = stage[which];
+    UW12_CUDA(cudaMemcpy2DAsync(out, ld * sizeof(double), st.p, rows * sizeof(double),
+                                rows * sizeof(double), nc, cudaMemcpyHostToDevice, s));
+    UW12_CUDA(cudaEventRecord(st.copied, s));
   }
 };
 
-uw12b::AuxProducer wrap_producer(uw12c_block_fn fn, void* user, bool host, size_t rows) {
+uw12b::AuxProducer wrap_producer(uw12c_block_fn fn, void* user, bool host, size_t rows,
+                                 size_t n_df) {
   if (!fn) return {};
   auto p = std::make_shared<UserProducer>();
   p->fn = fn;
   p->user = user;
   p->host = host;
   p->rows = rows;
+  p->n_df = n_df;
   return [p](size_t f, size_t c, double* o, size_t l, cudaStream_t s) { (*p)(f, c, o, l, s); };
 }
 
@@ -534,8 +618,8 @@ int uw12c_integrals_create_callback(const double* X2, int x2_mem_kind,
     need(three_index != nullptr, "null three-index callback");
     *out = nullptr;
     const bool host = block_mem_kind == UW12C_MEM_HOST;
-    auto ao = wrap_producer(three_index, user, host, n_ao * (n_ao + 1) / 2);
-    auto ri = wrap_producer(three_index_ri, user_ri, host, n_ri * n_ao);
+    auto ao = wrap_producer(three_index, user, host, n_ao * (n_ao + 1) / 2, n_df);
+    auto ri = wrap_producer(three_index_ri, user_ri, host, n_ri * n_ao, n_df);
     auto h = std::make_unique<uw12c_integrals>();
     h->h.reset(uw12b::integrals_create_producer(X2, x2_mem_kind == UW12C_MEM_DEVICE,
                                                 std::move(ao), std::move(ri), n_ao,

@@ -9,6 +9,7 @@ integral-direct.
   aux functions are summed block by block), forward and adjoint.
 * The library's native device producer (synthetic tensors) against the same
   tensors stored.
+* Host producers are read ahead on a background thread.
 * A failing producer is reported as a runtime error.
 """
 import ctypes
@@ -105,6 +106,44 @@ def test_producer_is_called_in_blocks(uw12lib, cuda_device):
         uw12lib.set_memory_budget(0)
     M = d.W2.shape[0]
     assert len(calls) > 1 and all(0 <= f and f + n <= M for f, n in calls)
+
+
+def test_host_producer_reads_ahead(uw12lib, cuda_device):
+    """Host producers are read ahead: after a block is staged, the next range
+    is produced on a background thread while the GPU works, and the request
+    for it takes the staged copy.  Results equal the stored evaluation."""
+    import threading
+    c = [x for x in CASES if x.name == "unit_tiles"][0]
+    d = make_case(c)
+    main = threading.get_ident()
+    threads, calls = [], []
+
+    def traced(T):
+        inner = _host_producer(T, calls)
+
+        def f(first, count, out, ld, stream):
+            threads.append(threading.get_ident())
+            inner(first, count, out, ld, stream)
+        return f
+
+    M = d.W2.shape[0]
+    W = uw12lib.setup_base_integrals_callback(d.W2, traced(d.W3), traced(d.W3_ri), n_ao=c.n_ao,
+                                              n_df=M, n_ri=c.n_ri, store_ao=False,
+                                              store_ri=False)
+    V, WV = _stored(uw12lib, d)[1:]
+    A = uw12lib.setup_abs_projectors(d.S, c.n_ao, c.n_ri)
+    uw12lib.set_memory_budget(64 << 10)
+    try:
+        got = uw12lib.form_fock(W, V, WV, A, d.orbitals, d.occ, c.n_active, True, True, 1.0, 0.5)
+        ref = uw12lib.form_fock(*_stored(uw12lib, d), A, d.orbitals, d.occ, c.n_active, True,
+                                True, 1.0, 0.5)
+    finally:
+        uw12lib.set_memory_budget(0)
+    assert abs(got[0] - ref[0]) <= 1e-12 * max(1.0, abs(ref[0]))
+    for s in range(len(ref[1])):
+        assert np.max(np.abs(got[1][s] - ref[1][s])) <= 1e-12 * max(1.0, np.max(np.abs(ref[1][s])))
+    assert any(t != main for t in threads)  # some blocks were produced ahead
+    assert all(0 <= f and f + n <= M for f, n in calls)
 
 
 def test_native_device_producer_matches_stored_synthetic(uw12lib, cuda_device):
