@@ -768,7 +768,7 @@ __device__ __forceinline__ double small_to_double(uint32_t r) {
 // REDUCE: several K chunks, whose residue sums are reduced mod p; with one K
 // chunk the stored residues (already in [0, p)) enter the CRT sum directly.
 template <int NCH, bool REDUCE>
-__global__ void __launch_bounds__(256, 2) k_crt(const CrtArgs a) {
+__global__ void __launch_bounds__(256, REDUCE ? 2 : 3) k_crt(const CrtArgs a) {
   const long long i0 = (static_cast<long long>(blockIdx.x) * 256 + threadIdx.x) * 4;
   if (i0 >= a.m) return;
   const int b = blockIdx.z;
