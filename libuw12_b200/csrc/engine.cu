@@ -22,6 +22,10 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <exception>
+#include <vector>
+#include <thread>
+#include <cstring>
 #include <cmath>
 #include <cstdio>
 #include <map>
@@ -41,8 +45,80 @@ void solver_check(cusolverStatus_t st, const char* what) {
     throw Error(kErrCuda, std::string(what) + ": cusolver status " + std::to_string(int(st)));
 }
 
+// Pinned chunks for host-to-device copies out of pageable memory: filled by
+// several host threads at once while the previous chunk's DMA runs (a
+// pageable cudaMemcpyAsync stages through the driver at ~10 GB/s).  One set
+// per process, used under a mutex; an event per chunk guards its reuse.
+struct Staging {
+  static constexpr size_t kChunkBytes = size_t(64) << 20;
+  static constexpr int kChunks = 4;
+  std::mutex mu;
+  char* buf[kChunks] = {};
+  cudaEvent_t done[kChunks] = {};
+  int device[kChunks] = {};
+};
+
+Staging& staging() {
+  static Staging* st = new Staging();  // lives to process exit (pinned memory freed by it)
+  return *st;
+}
+
+// memcpy of `bytes` split over up to `threads` host threads.
+void parallel_memcpy(char* dst, const char* src, size_t bytes, unsigned threads) {
+  const size_t per = (bytes + threads - 1) / threads;
+  std::vector<std::thread> pool;
+  for (unsigned t = 1; t < threads && t * per < bytes; ++t)
+    pool.emplace_back([=] { std::memcpy(dst + t * per, src + t * per, std::min(per, bytes - t * per)); });
+  std::memcpy(dst, src, std::min(per, bytes));
+  for (auto& th : pool) th.join();
+}
+
+void upload_pageable(double* dst, const double* src, size_t n, cudaStream_t s) {
+  Staging& st = staging();
+  std::lock_guard<std::mutex> lk(st.mu);
+  int dev = 0;
+  UW12_CUDA(cudaGetDevice(&dev));
+  for (int c = 0; c < Staging::kChunks; ++c) {
+    if (!st.buf[c]) {
+      UW12_CUDA(cudaMallocHost(reinterpret_cast<void**>(&st.buf[c]), Staging::kChunkBytes));
+    }
+    if (!st.done[c] || st.device[c] != dev) {
+      if (st.done[c]) {
+        UW12_CUDA(cudaEventSynchronize(st.done[c]));
+        cudaEventDestroy(st.done[c]);
+      }
+      UW12_CUDA(cudaEventCreateWithFlags(&st.done[c], cudaEventDisableTiming));
+      st.device[c] = dev;
+    }
+  }
+  const unsigned threads = std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2));
+  const char* from = reinterpret_cast<const char*>(src);
+  char* to = reinterpret_cast<char*>(dst);
+  const size_t bytes = n * sizeof(double);
+  int c = 0;
+  for (size_t off = 0; off < bytes; off += Staging::kChunkBytes, c = (c + 1) % Staging::kChunks) {
+    const size_t len = std::min(Staging::kChunkBytes, bytes - off);
+    UW12_CUDA(cudaEventSynchronize(st.done[c]));  // this chunk's previous copy is done
+    parallel_memcpy(st.buf[c], from + off, len, threads);
+    UW12_CUDA(cudaMemcpyAsync(to + off, st.buf[c], len, cudaMemcpyHostToDevice, s));
+    UW12_CUDA(cudaEventRecord(st.done[c], s));
+  }
+  // the caller's buffer has been read; the chunks' copies finish in stream order
+}
+
+// n doubles to the device: device-to-device, a direct copy from pinned host
+// memory, or the staged pipeline for large pageable host buffers.
 void upload(double* dst, const double* src, size_t n, bool device_mem, cudaStream_t s) {
   if (!n) return;
+  if (!device_mem && n * sizeof(double) >= (size_t(32) << 20)) {
+    cudaPointerAttributes at{};
+    const bool known = cudaPointerGetAttributes(&at, src) == cudaSuccess;
+    if (!known) cudaGetLastError();  // clear the query's error
+    if (!known || at.type == cudaMemoryTypeUnregistered) {
+      upload_pageable(dst, src, n, s);
+      return;
+    }
+  }
   UW12_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double),
                             device_mem ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
 }
@@ -234,9 +310,28 @@ IntegralsHandle* integrals_create(const double* X3, const double* X2, const doub
     // metric is diagonalised on the current stream; both are complete when
     // this returns.
     SideStream side(s);
-    upload(h->J3_0.get(), X3, np * n_df, device_mem, side.get());
-    if (X3_ri) upload(h->J3_ri_0.get(), X3_ri, n_ri * n_ao * n_df, device_mem, side.get());
-    setup_metric(h, X2, device_mem);
+    // host sources are read on a second host thread (a pageable source is
+    // copied through pinned chunks by host threads), so the eigensolve runs
+    // meanwhile
+    std::exception_ptr upload_err;
+    const int dev = h->device;
+    std::thread up([&] {
+      try {
+        UW12_CUDA(cudaSetDevice(dev));
+        upload(h->J3_0.get(), X3, np * n_df, device_mem, side.get());
+        if (X3_ri) upload(h->J3_ri_0.get(), X3_ri, n_ri * n_ao * n_df, device_mem, side.get());
+      } catch (...) {
+        upload_err = std::current_exception();
+      }
+    });
+    try {
+      setup_metric(h, X2, device_mem);
+    } catch (...) {
+      up.join();
+      throw;
+    }
+    up.join();
+    if (upload_err) std::rethrow_exception(upload_err);
     side.join();
   } catch (...) {
     delete h;
