@@ -168,6 +168,40 @@ int uw12c_fock_backward(const uw12c_integrals* W, const uw12c_integrals* V,
                         double* const* dE_dX3, double* const* dE_dX3_ri, double* const* dE_dX2,
                         int grad_mem_kind);
 
+/* A consumer of a three-index gradient in blocks (no counterpart in libuw12):
+ * receives aux functions [first, first + count) as the columns of `block`
+ * (leading dimension ld = the tensor's rows) and returns 0, or non-zero on
+ * failure.  Device blocks may be read by work the sink enqueues on the CUDA
+ * stream `stream` (a cudaStream_t) before it returns; later work on that
+ * stream may overwrite them.  Host blocks are valid until the sink returns. */
+typedef int (*uw12c_block_sink)(void* user, size_t first, size_t count, const double* block,
+                                size_t ld, void* stream);
+/* uw12c_fock_backward with the three-index gradients handed to sinks in aux
+ * blocks instead of written to whole buffers (no counterpart in libuw12): a
+ * gradient as large as an unstored (integral-direct) tensor is never held
+ * whole on the device.  sink3[3] (W, V, WV; packed rows) and sink3_ri[2] (W,
+ * V; RI rows), each with its user pointer, any entry NULL to skip that
+ * gradient; block_mem_kind UW12C_MEM_DEVICE passes device blocks,
+ * UW12C_MEM_HOST host blocks (staged through pinned memory, at most 256 MiB
+ * per call).  Every aux function of a requested gradient is delivered once,
+ * in increasing order.  The metric gradients go to dE_dX2 as in
+ * uw12c_fock_backward. */
+int uw12c_fock_backward_blocks(const uw12c_integrals* W, const uw12c_integrals* V,
+                               const uw12c_integrals* WV, const uw12c_abs* abs, size_t n_ao,
+                               size_t n_spin, const double* const* C, const size_t* ldc,
+                               const size_t* n_orb, const double* const* occ,
+                               const size_t* n_occ, const size_t* n_active,
+                               double scale_opp_spin, double scale_same_spin, double* energy,
+                               double* terms, double* fock, int fock_mem_kind,
+                               const uw12c_block_sink* sink3, void* const* user3,
+                               const uw12c_block_sink* sink3_ri, void* const* user3_ri,
+                               int block_mem_kind, double* const* dE_dX2, int grad_mem_kind);
+/* A device sink for uw12c_fock_backward_blocks that adds the sum of squares
+ * of every block it receives to the double at `user` (device memory, on the
+ * library's stream): the squared Frobenius norm of a streamed gradient. */
+int uw12c_sink_norm2(void* user, size_t first, size_t count, const double* block, size_t ld,
+                     void* stream);
+
 /* Replaces uw12::uw12_fock(double* fock, ...) (libuw12.hpp:157-169,
  * libuw12.cpp:184-214) in its raw-pointer form: C is the setup_orbitals
  * buffer (n_ao x n_orb*n_spin), occ the setup_occupations buffer

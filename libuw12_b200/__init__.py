@@ -95,6 +95,12 @@ def lib():
                                       ctypes.POINTER(P), PSZ, PSZ, c_d, c_d, PD, PD, P,
                                       ctypes.c_int, ctypes.POINTER(P), ctypes.POINTER(P),
                                       ctypes.POINTER(P), ctypes.c_int]
+    L.uw12c_fock_backward_blocks.argtypes = [P, P, P, P, c_sz, c_sz, ctypes.POINTER(P), PSZ,
+                                             PSZ, ctypes.POINTER(P), PSZ, PSZ, c_d, c_d, PD, PD,
+                                             P, ctypes.c_int, ctypes.POINTER(P),
+                                             ctypes.POINTER(P), ctypes.POINTER(P),
+                                             ctypes.POINTER(P), ctypes.c_int, ctypes.POINTER(P),
+                                             ctypes.c_int]
     L.uw12c_energy.argtypes = [P, P, P, P, P, c_sz, c_sz, c_sz, P, c_sz, c_sz, PSZ, c_d, c_d,
                                c_sz, PD]
     L.uw12c_set_stream.argtypes = [P]
@@ -553,6 +559,86 @@ def fock_backward(W: BaseIntegrals, V: BaseIntegrals, WV: BaseIntegrals, abs_p: 
                                      float(scale_same_spin), ctypes.byref(energy), terms,
                                      _fptr(fock) if fock is not None else P(0), MEM_HOST, d3,
                                      d3ri, d2, MEM_DEVICE if device_out is not None else MEM_HOST))
+    focks = None
+    if fock is not None:
+        focks = [np.array(fock[:, s * n_ao:(s + 1) * n_ao]) for s in range(n_spin)]
+    return energy.value, focks, (terms[0], terms[1], terms[2]), grads
+
+
+SINK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t,
+                           ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
+BLOCK_GRADIENT_NAMES = ("W3", "V3", "WV3", "W3_ri", "V3_ri")
+
+
+def sink_norm2() -> int:
+    """Address of ``uw12c_sink_norm2``, a native device sink (user = device
+    double that accumulates the squared norm of the blocks)."""
+    return ctypes.cast(lib().uw12c_sink_norm2, ctypes.c_void_p).value
+
+
+def fock_backward_blocks(W: BaseIntegrals, V: BaseIntegrals, WV: BaseIntegrals,
+                         abs_p: ABSProjectors, orbitals: Sequence[np.ndarray],
+                         occupations: Sequence[np.ndarray], n_active: Sequence[int],
+                         scale_opp_spin: float, scale_same_spin: float, sinks: dict,
+                         metric_gradients: Sequence[str] = ("W2", "V2", "WV2"),
+                         calculate_fock: bool = True, device: bool = False,
+                         users: Optional[dict] = None):
+    """``uw12c_fock_backward_blocks``: the three-index gradients delivered in aux
+    blocks.  ``sinks`` maps names of ``BLOCK_GRADIENT_NAMES`` to Python callables
+    ``f(first, count, block)`` (``block`` a host ``rows x count`` array, valid
+    during the call; ``device=False``) or to C function pointers (ints) with
+    ``users[name]`` as their user pointer (``device=True`` passes device
+    blocks).  Returns ``(energy, fock, (E2, E3, E4), metric_grads)``."""
+    n_spin = len(orbitals)
+    if n_spin < 1 or n_spin > 2 or len(occupations) != n_spin or len(n_active) != n_spin:
+        raise UW12LogicError("invalid number of spin channels")
+    n_ao = W.n_ao
+    Cs = [np.asfortranarray(np.asarray(c, dtype=np.float64)) for c in orbitals]
+    occs = [np.ascontiguousarray(np.asarray(o, dtype=np.float64).reshape(-1)) for o in occupations]
+    P = ctypes.c_void_p
+    c_ptrs = (P * n_spin)(*[_fptr(c) for c in Cs])
+    ldc = (ctypes.c_size_t * n_spin)(*[max(1, c.shape[0]) for c in Cs])
+    norb = (ctypes.c_size_t * n_spin)(*[c.shape[1] for c in Cs])
+    o_ptrs = (P * n_spin)(*[_fptr(o) for o in occs])
+    nocc = (ctypes.c_size_t * n_spin)(*[o.size for o in occs])
+    nact = (ctypes.c_size_t * n_spin)(*[int(a) for a in n_active])
+    users = users or {}
+    keep = []  # callbacks stay alive for the call
+
+    def as_sink(name):
+        f = sinks.get(name)
+        if f is None:
+            return P(0)
+        if isinstance(f, int):
+            return P(f)
+
+        def cb(user, first, count, block, ld, stream):
+            try:
+                view = np.ctypeslib.as_array(ctypes.cast(block, ctypes.POINTER(ctypes.c_double)),
+                                             shape=(ld * count,)).reshape((ld, count), order="F")
+                f(int(first), int(count), view)
+                return 0
+            except Exception:  # reported by the library as a runtime error
+                return 1
+        c = SINK_FN(cb)
+        keep.append(c)
+        return ctypes.cast(c, P)
+
+    s3 = (P * 3)(*[as_sink(n) for n in ("W3", "V3", "WV3")])
+    s3ri = (P * 2)(*[as_sink(n) for n in ("W3_ri", "V3_ri")])
+    u3 = (P * 3)(*[P(users.get(n, 0)) for n in ("W3", "V3", "WV3")])
+    u3ri = (P * 2)(*[P(users.get(n, 0)) for n in ("W3_ri", "V3_ri")])
+    shapes = {"W2": (W.n_df, W.n_df), "V2": (V.n_df, V.n_df), "WV2": (WV.n_df, WV.n_df)}
+    grads = {n: np.zeros(shapes[n], order="F") for n in metric_gradients}
+    d2 = (P * 3)(*[_fptr(grads[n]) if n in grads else P(0) for n in ("W2", "V2", "WV2")])
+    energy = ctypes.c_double()
+    terms = (ctypes.c_double * 3)()
+    fock = np.zeros((n_ao, n_ao * n_spin), order="F") if calculate_fock else None
+    _check(lib().uw12c_fock_backward_blocks(
+        W.handle, V.handle, WV.handle, abs_p.handle, n_ao, n_spin, c_ptrs, ldc, norb, o_ptrs,
+        nocc, nact, float(scale_opp_spin), float(scale_same_spin), ctypes.byref(energy), terms,
+        _fptr(fock) if fock is not None else P(0), MEM_HOST, s3, u3, s3ri, u3ri,
+        MEM_DEVICE if device else MEM_HOST, d2, MEM_HOST))
     focks = None
     if fock is not None:
         focks = [np.array(fock[:, s * n_ao:(s + 1) * n_ao]) for s in range(n_spin)]

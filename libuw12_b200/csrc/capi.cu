@@ -15,6 +15,7 @@
 #include "../../include/uw12_c.h"
 #include "engine.cuh"
 #include "gemm_f64.cuh"
+#include "kernels.cuh"
 #include "ozaki.cuh"
 
 namespace uw12b {
@@ -457,6 +458,104 @@ int uw12c_fock_backward(const uw12c_integrals* W, const uw12c_integrals* V,
                   fock != nullptr, scale_opp_spin, scale_same_spin, 0, energy, terms, fock,
                   fock_mem_kind, &ad);
   });
+}
+
+namespace {
+
+// A user gradient sink as an engine sink: device blocks are passed on; host
+// blocks are copied through a pinned stage (at most 256 MiB at a time, so one
+// engine block may reach the user as several).
+uw12b::GradSink wrap_sink(uw12c_block_sink fn, void* user, bool host, size_t rows) {
+  if (!fn) return {};
+  struct Stage {
+    double* p = nullptr;
+    size_t n = 0;
+    ~Stage() {
+      if (p) cudaFreeHost(p);
+    }
+  };
+  auto stage = std::make_shared<Stage>();
+  return [fn, user, host, rows, stage](size_t first, size_t count, const double* block,
+                                       size_t ld, cudaStream_t s) {
+    auto check = [](int rc) {
+      if (rc != 0)
+        throw uw12b::Error(UW12C_ERR_RUNTIME,
+                           "gradient block sink returned " + std::to_string(rc));
+    };
+    if (!host) {
+      check(fn(user, first, count, block, ld, static_cast<void*>(s)));
+      return;
+    }
+    const size_t per = std::max<size_t>(1, std::min(count, (size_t(1) << 25) / rows));
+    if (stage->n < rows * per) {
+      if (stage->p) cudaFreeHost(stage->p);
+      stage->p = nullptr;
+      stage->n = 0;
+      UW12_CUDA(cudaMallocHost(reinterpret_cast<void**>(&stage->p), rows * per * sizeof(double)));
+      stage->n = rows * per;
+    }
+    for (size_t c0 = 0; c0 < count; c0 += per) {
+      const size_t nc = std::min(per, count - c0);
+      UW12_CUDA(cudaMemcpy2DAsync(stage->p, rows * sizeof(double), block + ld * c0,
+                                  ld * sizeof(double), rows * sizeof(double), nc,
+                                  cudaMemcpyDeviceToHost, s));
+      UW12_CUDA(cudaStreamSynchronize(s));
+      check(fn(user, first + c0, nc, stage->p, rows, static_cast<void*>(s)));
+    }
+  };
+}
+
+}  // namespace
+
+int uw12c_fock_backward_blocks(const uw12c_integrals* W, const uw12c_integrals* V,
+                               const uw12c_integrals* WV, const uw12c_abs* abs, size_t n_ao,
+                               size_t n_spin, const double* const* C, const size_t* ldc,
+                               const size_t* n_orb, const double* const* occ,
+                               const size_t* n_occ, const size_t* n_active,
+                               double scale_opp_spin, double scale_same_spin, double* energy,
+                               double* terms, double* fock, int fock_mem_kind,
+                               const uw12c_block_sink* sink3, void* const* user3,
+                               const uw12c_block_sink* sink3_ri, void* const* user3_ri,
+                               int block_mem_kind, double* const* dE_dX2, int grad_mem_kind) {
+  return guarded([&] {
+    need(grad_mem_kind == UW12C_MEM_HOST || grad_mem_kind == UW12C_MEM_DEVICE,
+         "bad grad_mem_kind");
+    need(block_mem_kind == UW12C_MEM_HOST || block_mem_kind == UW12C_MEM_DEVICE,
+         "bad block_mem_kind");
+    need(W && V && WV, "null integral handle");
+    need(uw12b::g_n_shards == 1, "the adjoint evaluates unsharded (uw12c_set_shard(0, 1))");
+    const bool host = block_mem_kind == UW12C_MEM_HOST;
+    const uw12c_integrals* X[3] = {W, V, WV};
+    uw12b::AdjointOutputs ad;
+    for (int i = 0; i < 3; ++i) {
+      ad.dJ2[i] = dE_dX2 ? dE_dX2[i] : nullptr;
+      const size_t na = X[i]->h->n_ao;
+      if (sink3 && sink3[i])
+        ad.sink3[i] = wrap_sink(sink3[i], user3 ? user3[i] : nullptr, host, na * (na + 1) / 2);
+    }
+    for (int i = 0; i < 2; ++i)
+      if (sink3_ri && sink3_ri[i])
+        ad.sink3_ri[i] = wrap_sink(sink3_ri[i], user3_ri ? user3_ri[i] : nullptr, host,
+                                   X[i]->h->n_ri * X[i]->h->n_ao);
+    ad.device_mem = grad_mem_kind == UW12C_MEM_DEVICE;
+    run_form_fock(W, V, WV, abs, n_ao, n_spin, C, ldc, n_orb, occ, n_occ, n_active, 0,
+                  fock != nullptr, scale_opp_spin, scale_same_spin, 0, energy, terms, fock,
+                  fock_mem_kind, &ad);
+  });
+}
+
+int uw12c_sink_norm2(void* user, size_t first, size_t count, const double* block, size_t ld,
+                     void* stream) {
+  (void)first;
+  if (!user || !block) return 1;
+  try {
+    uw12b::sumsq_add(block, static_cast<long long>(ld), static_cast<long long>(ld),
+                     static_cast<long long>(count), static_cast<double*>(user),
+                     static_cast<cudaStream_t>(stream));
+  } catch (...) {
+    return 2;
+  }
+  return 0;
 }
 
 namespace {

@@ -1421,7 +1421,9 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
     const size_t M = X.n_df;
     double* g3 = gJ3[which];
     double* g3ri = gJ3ri[which];
-    if (!g3 && !g3ri) continue;
+    const GradSink& s3 = out.sink3[which];
+    const GradSink& s3ri = out.sink3_ri[which];
+    if (!g3 && !g3ri && !s3 && !s3ri) continue;
     budget = auto_budget_doubles(rq.mem_budget);
     DevBuf Bb1(N * o_tot * M), Bbri(R * a_tot * M);
     Bb1.zero();
@@ -1463,7 +1465,7 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
       copy3d(Wsb.get() + N, LL(Rp), LL(Rp * a), Bbri.get() + R * sd[s].aoff, LL(R),
              LL(R * a_tot), LL(R), LL(a), LL(M));
     }
-    if (g3) {
+    if (g3 || s3) {
       // B1bar_0 = B1bar P2^T, then per aux function the packed symmetric sum of B1bar_0 Co^T
       DevBuf Bb10(N * o_tot * M);
       GemmDesc gp = gemm_nn(LL(N * o_tot), LL(M), LL(M), 1.0, Bb1.get(), LL(N * o_tot),
@@ -1471,7 +1473,8 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
       gp.b_ncontig = true;
       gemm(gp);
       const size_t ac = std::max<size_t>(1, std::min(M, budget / (2 * N * N)));
-      DevBuf G(N * N * ac);
+      DevBuf G(N * N * ac), Pk;
+      if (!g3) Pk.alloc(np * ac);  // one streamed block
       for (size_t a0 = 0; a0 < M; a0 += ac) {
         const size_t na = std::min(ac, M - a0);
         GemmDesc g = gemm_nn(LL(N), LL(N), LL(o_tot), 1.0, Bb10.get() + N * o_tot * a0, LL(N),
@@ -1481,25 +1484,41 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
         g.sAo1 = LL(N * o_tot);
         g.sCo1 = LL(N * N);
         gemm(g);
-        pack_sym_sum(G.get(), LL(N), LL(na), g3 + np * a0, LL(np));
+        pack_sym_sum(G.get(), LL(N), LL(na), g3 ? g3 + np * a0 : Pk.get(), LL(np));
+        if (!g3) s3(a0, na, Pk.get(), np, st);
       }
     }
-    if (g3ri) {
+    if (g3ri || s3ri) {
+      // stored: one batched GEMM into the whole gradient; streamed: aux blocks
+      // of at most a quarter of the budget
+      const size_t rows = R * N;
+      const size_t step = g3ri ? M : std::max<size_t>(1, std::min(M, budget / (4 * rows)));
+      DevBuf Rk;
+      if (!g3ri) Rk.alloc(rows * step);
       if (a_tot == 0) {
-        UW12_CUDA(cudaMemsetAsync(g3ri, 0, R * N * M * sizeof(double), st));
+        if (g3ri) {
+          UW12_CUDA(cudaMemsetAsync(g3ri, 0, R * N * M * sizeof(double), st));
+        } else {
+          Rk.zero();
+          for (size_t b0 = 0; b0 < M; b0 += step) s3ri(b0, std::min(step, M - b0), Rk.get(), rows, st);
+        }
       } else {
         DevBuf Bbri0(R * a_tot * M);
         GemmDesc gp = gemm_nn(LL(R * a_tot), LL(M), LL(M), 1.0, Bbri.get(), LL(R * a_tot),
                               X.P2.get(), LL(M), 0.0, Bbri0.get(), LL(R * a_tot));
         gp.b_ncontig = true;
         gemm(gp);
-        GemmDesc g = gemm_nn(LL(R), LL(N), LL(a_tot), 1.0, Bbri0.get(), LL(R), Ca.get(), LL(N),
-                             0.0, g3ri, LL(R));
-        g.b_ncontig = true;
-        g.nbo1 = LL(M);
-        g.sAo1 = LL(R * a_tot);
-        g.sCo1 = LL(R * N);
-        gemm(g);
+        for (size_t b0 = 0; b0 < M; b0 += step) {
+          const size_t nb = std::min(step, M - b0);
+          GemmDesc g = gemm_nn(LL(R), LL(N), LL(a_tot), 1.0, Bbri0.get() + R * a_tot * b0, LL(R),
+                               Ca.get(), LL(N), 0.0, g3ri ? g3ri + rows * b0 : Rk.get(), LL(R));
+          g.b_ncontig = true;
+          g.nbo1 = LL(nb);
+          g.sAo1 = LL(R * a_tot);
+          g.sCo1 = LL(R * N);
+          gemm(g);
+          if (!g3ri) s3ri(b0, nb, Rk.get(), rows, st);
+        }
       }
     }
   }
@@ -1561,7 +1580,8 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
   }
 
   // ---- WV: dE/dJ3_0 and dE/dJ2 through the fitted density
-  if (gJ3[2] || gJ2[2]) {
+  const GradSink& s3x = out.sink3[2];
+  if (gJ3[2] || s3x || gJ2[2]) {
     DevBuf dmat(np * ns), XDr(MX * ns), XD(MX * ns), XDb(MX * ns), vb(MX * ns);
     for (int s = 0; s < ns; ++s)
       pack_density(Ca_s(s), LL(N), LL(N), LL(sd[s].a), two, dmat.get() + np * s);
@@ -1573,15 +1593,23 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
     double coef[4] = {0, 0, 0, 0};
     for (int s = 0; s < ns; ++s)
       for (int sp = 0; sp < ns; ++sp) coef[s * ns + sp] = F[s][sp];
-    if (gJ3[2]) {
+    if (gJ3[2] || s3x) {
       // Xbar_D[s] = L sum_s' f X_D[s'];  dJ3 = 1/2 n_spin dmat (P2 Xbar_D)^T
       combine_vecs(XD.get(), LL(MX), ns, coef, WV.lam.get(), XDb.get());
       gemm(gemm_nn(LL(MX), ns, LL(MX), 1.0, WV.P2.get(), LL(MX), XDb.get(), LL(MX), 0.0, vb.get(),
                    LL(MX)));
-      GemmDesc gd = gemm_nn(LL(np), LL(MX), ns, 0.5 * ns, dmat.get(), LL(np), vb.get(), LL(MX),
-                            0.0, gJ3[2], LL(np));
-      gd.b_ncontig = true;
-      gemm(gd);
+      // whole, or in aux blocks of at most a quarter of the budget when streamed
+      const size_t step = gJ3[2] ? MX : std::max<size_t>(1, std::min(MX, budget / (4 * np)));
+      DevBuf Xk;
+      if (!gJ3[2]) Xk.alloc(np * step);
+      for (size_t b0 = 0; b0 < MX; b0 += step) {
+        const size_t nb = std::min(step, MX - b0);
+        GemmDesc gd = gemm_nn(LL(np), LL(nb), ns, 0.5 * ns, dmat.get(), LL(np), vb.get() + b0,
+                              LL(MX), 0.0, gJ3[2] ? gJ3[2] + np * b0 : Xk.get(), LL(np));
+        gd.b_ncontig = true;
+        gemm(gd);
+        if (!gJ3[2]) s3x(b0, nb, Xk.get(), np, st);
+      }
     }
     if (gJ2[2]) {
       // U = Q X_D = P2 (L X_D); dJ2 = -1/2 U (U F)^T

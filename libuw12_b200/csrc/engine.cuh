@@ -113,11 +113,20 @@ void form_fock(const FockRequest& rq);
 // gradient is -J2^-1 G J2^-1 (no eigenvector derivatives), exact when no metric
 // eigenvalue falls below the pseudo-inverse cut-off (1e-10).  The energy and
 // Fock of rq (direct terms) are computed first.
+// A consumer of a three-index gradient in aux blocks: columns [first, first +
+// count) as a device block (leading dimension ld) on `stream`; the block may be
+// overwritten by later work on that stream once the call returns.
+using GradSink =
+    std::function<void(size_t first, size_t count, const double* block, size_t ld, cudaStream_t)>;
+
 struct AdjointOutputs {
   double* dJ3[3] = {nullptr, nullptr, nullptr};  // W, V, WV
   double* dJ3_ri[2] = {nullptr, nullptr};        // W, V
   double* dJ2[3] = {nullptr, nullptr, nullptr};  // W, V, WV
   bool device_mem = false;
+  // instead of dJ3 / dJ3_ri (which must then be null): the gradient in aux
+  // blocks, never held whole on the device
+  GradSink sink3[3], sink3_ri[2];
 };
 void form_fock_adjoint(const FockRequest& rq, const AdjointOutputs& out);
 

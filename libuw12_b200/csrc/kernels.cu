@@ -475,4 +475,37 @@ void gather_scale_cols(const double* src, long long rows, const int* idx, const 
   UW12_LAUNCHED();
 }
 
+// out += sum of squares of the rows x cols block A (leading dimension lda):
+// grid-stride partial sums, a warp-shuffle and shared-memory block reduction,
+// one atomic add per block (summation order not fixed).
+__global__ void k_sumsq_add(const double* __restrict__ A, long long lda, long long rows,
+                            long long cols, double* out) {
+  __shared__ double part[32];
+  const long long total = rows * cols;
+  double acc = 0.0;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long c = e / rows, r = e - c * rows;
+    const double x = A[r + lda * c];
+    acc = fma(x, x, acc);
+  }
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) part[warp] = acc;
+  __syncthreads();
+  if (warp == 0) {
+    acc = lane < (int)(blockDim.x >> 5) ? part[lane] : 0.0;
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) atomicAdd(out, acc);
+  }
+}
+
+void sumsq_add(const double* A, long long lda, long long rows, long long cols, double* out,
+               cudaStream_t s) {
+  const long long total = rows * cols;
+  if (total <= 0) return;
+  k_sumsq_add<<<grid_for(total, 4), kT, 0, s>>>(A, lda, rows, cols, out);
+  UW12_LAUNCHED();
+}
+
 }  // namespace uw12b

@@ -50,6 +50,9 @@ void symmetrise(const double* G, long long ldg, long long n, double* F, long lon
 
 // max |A - A^T| and max |A| into out[0], out[1] (device), n x n column-major.
 void symmetry_stats(const double* A, long long lda, long long n, double* out);
+// *out += sum of squares of the rows x cols block A (leading dimension lda), on s.
+void sumsq_add(const double* A, long long lda, long long rows, long long cols, double* out,
+               cudaStream_t s);
 
 // Y = sum_q coefT[q]*T[q] - r[i]*c[j]*sum_q coefX[q]*X[q], M x M, q < nq <= 2.
 void combine_y(double* Y, long long m, const double* const* T, const double* coefT,
