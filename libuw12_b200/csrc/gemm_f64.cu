@@ -16,8 +16,9 @@ namespace uw12b {
 
 namespace {
 
-// k tile 16 with 4 stages measured 1.5% faster on the c1 evaluation than 32
-// with 3 (and 16 with 5, 32 with 2); both are compile-time settings.
+// k tile 16 with 4 stages measured 1.5% faster than 32 with 3 (and than 16
+// with 5, 32 with 2) on a full evaluation with N = 500 AO, M = 1500 DF and
+// R = 2000 RI functions; both are compile-time settings.
 #ifndef UW12_DMMA_BK
 #define UW12_DMMA_BK 16
 #endif
