@@ -16,6 +16,15 @@ through the C-ABI from pinned host buffers: integral upload, on-device metric
 and overlap eigensolves, evaluation (and all-reduce) and Fock read-back per
 step.
 
+Beside the headline the JSON line reports the split-precision arms
+(``--split-moduli``), forward + backward (``adjoint``) and a 64-molecule batch
+(``batched``).  ``--config c2 --direct`` evaluates N=1200, M=3600, R=4800
+(closed shell, 100 occupied) integral-direct: no three-index tensor stored,
+each regenerated on the device by the library's synthetic producer at every
+use, the three-index gradients streamed in aux blocks to a squared-norm sink.
+``--gemm m,n,k[,beta]`` times one GEMM shape on the FP64 and split paths
+instead (a kernel profiling probe).
+
 ``--impl reference`` times the CPU restatement of libuw12's algorithm (the
 oracle; libuw12 itself cannot be built here) on the host cores for the same
 workload: every heavy loop of the reference (its parallel_for /
