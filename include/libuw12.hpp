@@ -11,6 +11,7 @@
 #define UW12_B200_LIBUW12_HPP
 
 #include <algorithm>
+#include <array>
 #include <cfloat>
 #include <cmath>
 #include <cstddef>
@@ -517,6 +518,163 @@ inline double uw12_fock(double* fock, const BaseIntegrals& W, const BaseIntegral
     for (size_t e = 0; e < n_ao * n_ao; ++e) fock[s * n_ao * n_ao + e] = res.fock[s][e];
   return res.energy;
 }
+
+/// Controls and entry points of the B200 library beyond libuw12's API (no
+/// counterpart in libuw12).
+namespace b200 {
+
+/// Split-precision GEMMs (int8 tensor cores, n_moduli moduli) in the following
+/// evaluations on this thread; 0 returns to FP64 (uw12c_set_precision).
+inline void set_precision(int n_moduli) { detail::check(uw12c_set_precision(n_moduli)); }
+
+/// Device-memory budget of the chunked loops in bytes; 0 restores the automatic
+/// one (uw12c_set_memory_budget).
+inline void set_memory_budget(size_t bytes) { detail::check(uw12c_set_memory_budget(bytes)); }
+
+/// Gradients of the direct-term energy with respect to the integrals.
+struct Gradients {
+  std::vector<linalg::Mat> dX3;     ///< W, V, WV: packed n_ao(n_ao+1)/2 x n_df
+  std::vector<linalg::Mat> dX3_ri;  ///< W, V: (n_ri n_ao) x n_df (empty when streamed)
+  std::vector<linalg::Mat> dX2;     ///< W, V, WV: n_df x n_df
+};
+
+struct BackwardResult {
+  utils::FockMatrixAndEnergy fock_energy;  ///< energy and Fock of form_fock without indirect term
+  double terms[3] = {0, 0, 0};             ///< two-, three-, four-electron energies
+  Gradients gradients;
+};
+
+/// A consumer of gradient blocks in host memory: aux functions [first, first +
+/// count) as the columns of `block` (leading dimension ld), valid during the call.
+using GradientSink =
+    std::function<void(size_t first, size_t count, const double* block, size_t ld)>;
+
+namespace detail_b200 {
+
+struct SpinArgs {
+  size_t n_ao = 0, n_spin = 0;
+  std::vector<const double*> C, occ;
+  std::vector<size_t> ldc, n_orb, n_occ;
+};
+
+inline SpinArgs spin_args(const Orbitals& orbitals, const Occupations& occupations,
+                          const std::vector<size_t>& n_active) {
+  SpinArgs a;
+  a.n_spin = orbitals.size();
+  if (a.n_spin < 1 || a.n_spin > 2 || occupations.size() != a.n_spin ||
+      n_active.size() != a.n_spin)
+    throw std::logic_error("invalid number of spin channels");
+  a.n_ao = orbitals[0].n_rows();
+  for (size_t s = 0; s < a.n_spin; ++s) {
+    if (orbitals[s].n_rows() != a.n_ao)
+      throw std::runtime_error("Inconsistent number of atomic orbitals");
+    a.C.push_back(orbitals[s].memptr());
+    a.ldc.push_back(a.n_ao);
+    a.n_orb.push_back(orbitals[s].n_cols());
+    a.occ.push_back(occupations[s].memptr());
+    a.n_occ.push_back(occupations[s].n_elem());
+  }
+  return a;
+}
+
+// A GradientSink as a uw12c_block_sink; the first exception a sink throws is
+// kept and rethrown once the library reports the failure.
+struct SinkState {
+  const GradientSink* fn = nullptr;
+  std::exception_ptr error;
+  static int call(void* user, size_t first, size_t count, const double* block, size_t ld,
+                  void* /*stream*/) noexcept {
+    auto* st = static_cast<SinkState*>(user);
+    try {
+      (*st->fn)(first, count, block, ld);
+      return 0;
+    } catch (...) {
+      if (!st->error) st->error = std::current_exception();
+      return 1;
+    }
+  }
+};
+
+}  // namespace detail_b200
+
+/// Reverse mode of the direct terms (uw12c_fock_backward): energy, terms and
+/// Fock plus every gradient, in host memory.
+inline BackwardResult fock_backward(const BaseIntegrals& W, const BaseIntegrals& V,
+                                    const BaseIntegrals& WV, const ABSProjectors& abs_projectors,
+                                    const Orbitals& orbitals, const Occupations& occupations,
+                                    const std::vector<size_t>& n_active, double scale_opp_spin,
+                                    double scale_same_spin) {
+  const auto a = detail_b200::spin_args(orbitals, occupations, n_active);
+  const BaseIntegrals* X[3] = {&W, &V, &WV};
+  BackwardResult r;
+  for (int i = 0; i < 3; ++i) {
+    const size_t n = X[i]->get_number_ao(), m = X[i]->get_number_df();
+    r.gradients.dX3.emplace_back(n * (n + 1) / 2, m);
+    r.gradients.dX2.emplace_back(m, m);
+    if (i < 2) r.gradients.dX3_ri.emplace_back(X[i]->get_number_ri() * n, m);
+  }
+  double* d3[3] = {r.gradients.dX3[0].memptr(), r.gradients.dX3[1].memptr(),
+                   r.gradients.dX3[2].memptr()};
+  double* d3ri[2] = {r.gradients.dX3_ri[0].memptr(), r.gradients.dX3_ri[1].memptr()};
+  double* d2[3] = {r.gradients.dX2[0].memptr(), r.gradients.dX2[1].memptr(),
+                   r.gradients.dX2[2].memptr()};
+  linalg::Mat fock(a.n_ao, a.n_ao * a.n_spin);
+  detail::check(uw12c_fock_backward(W.handle(), V.handle(), WV.handle(), abs_projectors.handle(),
+                                    a.n_ao, a.n_spin, a.C.data(), a.ldc.data(), a.n_orb.data(),
+                                    a.occ.data(), a.n_occ.data(), n_active.data(), scale_opp_spin,
+                                    scale_same_spin, &r.fock_energy.energy, r.terms,
+                                    fock.memptr(), UW12C_MEM_HOST, d3, d3ri, d2, UW12C_MEM_HOST));
+  for (size_t s = 0; s < a.n_spin; ++s)
+    r.fock_energy.fock.emplace_back(fock.memptr() + s * a.n_ao * a.n_ao, a.n_ao, a.n_ao);
+  return r;
+}
+
+/// uw12c_fock_backward_blocks: the three-index gradients of W, V, WV and the RI
+/// gradients of W, V (sinks[0..4]; an empty function skips that gradient)
+/// delivered to the sinks in aux blocks, host memory; the metric gradients
+/// are returned whole (gradients.dX3 and dX3_ri stay empty).
+inline BackwardResult fock_backward_blocks(const BaseIntegrals& W, const BaseIntegrals& V,
+                                           const BaseIntegrals& WV,
+                                           const ABSProjectors& abs_projectors,
+                                           const Orbitals& orbitals,
+                                           const Occupations& occupations,
+                                           const std::vector<size_t>& n_active,
+                                           double scale_opp_spin, double scale_same_spin,
+                                           const std::array<GradientSink, 5>& sinks) {
+  const auto a = detail_b200::spin_args(orbitals, occupations, n_active);
+  const BaseIntegrals* X[3] = {&W, &V, &WV};
+  BackwardResult r;
+  for (int i = 0; i < 3; ++i) {
+    const size_t m = X[i]->get_number_df();
+    r.gradients.dX2.emplace_back(m, m);
+  }
+  double* d2[3] = {r.gradients.dX2[0].memptr(), r.gradients.dX2[1].memptr(),
+                   r.gradients.dX2[2].memptr()};
+  detail_b200::SinkState st[5];
+  uw12c_block_sink fn[5];
+  void* users[5];
+  for (int i = 0; i < 5; ++i) {
+    st[i].fn = &sinks[i];
+    fn[i] = sinks[i] ? &detail_b200::SinkState::call : nullptr;
+    users[i] = &st[i];
+  }
+  linalg::Mat fock(a.n_ao, a.n_ao * a.n_spin);
+  const int status = uw12c_fock_backward_blocks(
+      W.handle(), V.handle(), WV.handle(), abs_projectors.handle(), a.n_ao, a.n_spin, a.C.data(),
+      a.ldc.data(), a.n_orb.data(), a.occ.data(), a.n_occ.data(), n_active.data(),
+      scale_opp_spin, scale_same_spin, &r.fock_energy.energy, r.terms, fock.memptr(),
+      UW12C_MEM_HOST, fn, users, fn + 3, users + 3, UW12C_MEM_HOST, d2, UW12C_MEM_HOST);
+  if (status != UW12C_OK) {
+    for (auto& s : st)
+      if (s.error) std::rethrow_exception(s.error);
+    detail::check(status);
+  }
+  for (size_t s = 0; s < a.n_spin; ++s)
+    r.fock_energy.fock.emplace_back(fock.memptr() + s * a.n_ao * a.n_ao, a.n_ao, a.n_ao);
+  return r;
+}
+
+}  // namespace b200
 
 }  // namespace uw12
 

@@ -4,6 +4,7 @@
 // error behaviour.  Input and output are flat binary files written and read by
 // tests/test_gpu_cpp_drop_in.py.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -130,8 +131,48 @@ int main(int argc, char** argv) {
     errors += 1;
   }
 
+  // B200 extensions: every gradient whole, then the three-index ones in blocks
+  // (under a 64 KiB budget, so in many blocks), put together again
+  const auto whole = uw12::b200::fock_backward(W, V, WV, abs, orbitals, occupations, n_active,
+                                               scales[0], 0.0);
+  std::vector<std::vector<double>> parts(5);
+  std::array<uw12::b200::GradientSink, 5> sinks;
+  for (int g = 0; g < 5; ++g)
+    sinks[g] = [&parts, g](size_t first, size_t count, const double* block, size_t ld) {
+      auto& v = parts[g];
+      if (v.size() != first * ld) throw std::logic_error("blocks out of order");
+      v.insert(v.end(), block, block + ld * count);
+    };
+  uw12c_set_memory_budget(64 << 10);
+  const auto blocks = uw12::b200::fock_backward_blocks(W, V, WV, abs, orbitals, occupations,
+                                                       n_active, scales[0], 0.0, sinks);
+  uw12c_set_memory_budget(0);
+  double grad_diff = std::abs(blocks.fock_energy.energy - whole.fock_energy.energy);
+  for (int g = 0; g < 5; ++g) {
+    const auto& ref = g < 3 ? whole.gradients.dX3[g] : whole.gradients.dX3_ri[g - 3];
+    double scale = 1e-300, diff = 0;
+    if (parts[g].size() != ref.n_elem()) diff = 1.0;
+    for (size_t e = 0; e < ref.n_elem() && e < parts[g].size(); ++e) {
+      scale = std::max(scale, std::abs(ref[e]));
+      diff = std::max(diff, std::abs(parts[g][e] - ref[e]));
+    }
+    grad_diff = std::max(grad_diff, diff / scale);
+  }
+  for (int g = 0; g < 3; ++g)
+    for (size_t e = 0; e < whole.gradients.dX2[g].n_elem(); ++e)
+      grad_diff = std::max(grad_diff, std::abs(blocks.gradients.dX2[g][e] -
+                                               whole.gradients.dX2[g][e]));
+  try {  // a sink that throws: its exception reaches the caller
+    std::array<uw12::b200::GradientSink, 5> bad;
+    bad[4] = [](size_t, size_t, const double*, size_t) { throw std::logic_error("sink full"); };
+    uw12::b200::fock_backward_blocks(W, V, WV, abs, orbitals, occupations, n_active, scales[0],
+                                     0.0, bad);
+  } catch (const std::logic_error&) {
+    errors += 1;
+  }
+
   std::ofstream out(argv[2], std::ios::binary);
-  const double head[6] = {e_fock, e_only, e_cb, errors, e_direct, fock_direct_diff};
+  const double head[7] = {e_fock, e_only, e_cb, errors, e_direct, fock_direct_diff, grad_diff};
   out.write(reinterpret_cast<const char*>(head), sizeof(head));
   out.write(reinterpret_cast<const char*>(fock.data()),
             static_cast<std::streamsize>(fock.size() * sizeof(double)));

@@ -1,8 +1,9 @@
 """The C++ drop-in header (include/libuw12.hpp) compiled into a small program
 that uses libuw12's API the way its callers do; its energy and Fock match the
 CPU oracle, the callback-built BaseIntegrals give the same energy, stored or
-integral-direct (shells produced at every use), and the error paths throw the
-reference's exception classes."""
+integral-direct (shells produced at every use), the error paths throw the
+reference's exception classes, and the uw12::b200 gradient extensions give
+the same gradients whole and in blocks."""
 import subprocess
 from pathlib import Path
 
@@ -53,8 +54,8 @@ def test_cpp_drop_in_matches_oracle(program, tmp_path, case):
     r = subprocess.run([str(program), str(inp), str(outp)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr + r.stdout
     raw = np.fromfile(outp, dtype=np.float64)
-    e_fock, e_only, e_cb, errors, e_direct, fock_direct_diff = raw[:6]
-    fock = raw[6:].reshape((case.n_ao, case.n_ao * n_spin), order="F")
+    e_fock, e_only, e_cb, errors, e_direct, fock_direct_diff, grad_diff = raw[:7]
+    fock = raw[7:].reshape((case.n_ao, case.n_ao * n_spin), order="F")
     e_ref, f_ref, _ = oracle_form_fock(d, True, True, 1.0, 0.5)
     fr = np.concatenate(f_ref, axis=1)
     assert abs(e_fock - e_ref) <= 1e-9 * abs(e_ref)
@@ -64,4 +65,6 @@ def test_cpp_drop_in_matches_oracle(program, tmp_path, case):
     # integral-direct W and V (shells produced in aux blocks at every use)
     assert abs(e_direct - e_fock) <= 1e-12 * abs(e_fock)
     assert fock_direct_diff <= 1e-12 * np.max(np.abs(fr))
-    assert errors == 4
+    # uw12::b200 extensions: gradients in blocks equal the whole gradients
+    assert grad_diff <= 1e-12
+    assert errors == 5
