@@ -798,7 +798,8 @@ def main():
         mols = batched_workload(device)
         batched = {"workload": "64 molecules, N ~ U[20,300], M = 3N, R = 4N, n_occ = round(N/10),"
                                " half closed shell, half UHF (n_beta = n_alpha - 1), scales "
-                               f"({args.s_os}, {args.s_ss}), energy + Fock, FP64",
+                               f"({args.s_os}, {args.s_ss}), energy + Fock, FP64 and split "
+                               "precision",
                    "n_ao_range": [min(m["n_ao"] for m in mols), max(m["n_ao"] for m in mols)]}
         for n_streams in (1, 8):
             L.fock_batched(mols, indirect, True, args.s_os, args.s_ss, n_streams=n_streams)
@@ -812,6 +813,25 @@ def main():
             batched[f"molecules_per_s_{n_streams}_streams"] = len(mols) / dt
         batched["speedup_8_vs_1_stream"] = (batched["s_per_batch_1_streams"] /
                                             batched["s_per_batch_8_streams"])
+        # the same batch in split precision (the calling thread's setting applies
+        # to every molecule), energies against the FP64 batch
+        ref = L.fock_batched(mols, indirect, True, args.s_os, args.s_ss, n_streams=1)
+        split_b = []
+        for Lm in moduli:
+            L.set_precision(Lm)
+            L.fock_batched(mols, indirect, True, args.s_os, args.s_ss, n_streams=1)
+            torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                res = L.fock_batched(mols, indirect, True, args.s_os, args.s_ss, n_streams=1)
+            torch.cuda.synchronize(device)
+            L.set_precision(0)
+            dt = (time.perf_counter() - t0) / args.steps
+            split_b.append({"n_moduli": Lm, "s_per_batch_1_stream": dt,
+                            "speedup_vs_fp64_1_stream": batched["s_per_batch_1_streams"] / dt,
+                            "max_energy_rel_err_vs_fp64": max(
+                                abs(r[0] - q[0]) / abs(q[0]) for r, q in zip(res, ref))})
+        batched["split_precision"] = split_b
         for m in mols:
             for k in ("W", "V", "WV", "abs"):
                 m[k].close()
