@@ -194,3 +194,71 @@ def form_fock(W, V, WV, Sfull_inv, orbitals, occ, n_active, indirect, calc_fock,
         E['4i'] = s_ss * e4i; E['3i'] = s_ss * e3i
     Ftot = [O.symmetrise(F[s] + Fsym[s]) for s in range(n_spin)]
     return sum(E.values()), Ftot, E
+
+
+# ---------------------------------------------------------------------------
+# Orbital-chunked form of the direct terms: the stacked intermediates (R' a x
+# M per spin and potential) are formed for at most `chunk` orbitals at a time,
+# so that their memory is bounded independently of the number of active
+# orbitals (the layout a device evaluation of N=2000, M=6000, R=8000 with 170
+# active orbitals per spin needs: whole, one stacked tensor is 82 GB).
+# ---------------------------------------------------------------------------
+
+def _stacked(Xi, Co_s, Ca_s, j0, j1, R):
+    """Rows of Wst for active orbitals j0..j1-1: per orbital, AO rows (B1 of
+    occupied column c + j) then RI rows (Bri of active column j)."""
+    N = Xi.n_ao
+    M = Xi.n_df
+    o, a = Co_s.shape[1], Ca_s.shape[1]
+    c = o - a
+    nj = j1 - j0
+    b1 = T1(Xi.J3_0, Co_s[:, c + j0:c + j1], Xi.P2)
+    bri = T2(Xi.J3_ri_0, Ca_s[:, j0:j1], Xi.P2, R)
+    st3 = np.zeros((N + R, nj, M))
+    st3[:N] = b1.reshape((N, nj, M), order='F')
+    st3[N:] = bri.reshape((R, nj, M), order='F')
+    return st3.reshape(((N + R) * nj, M), order='F')
+
+
+def chunked_xab_t(W, V, Sinv, Co_s, Ca_s, chunk):
+    """X_AB = Wst_W^T (I (x) S^-1) Wst_V accumulated over chunks of active
+    orbitals, and t = B2_W^T B2_V accumulated over chunks of occupied orbitals
+    (B2 rows i + a k: the k-chunk's rows are formed from its B1 columns)."""
+    N, R, M = W.n_ao, W.n_ri, W.n_df
+    Rp = N + R
+    o, a = Co_s.shape[1], Ca_s.shape[1]
+    X = np.zeros((M, M))
+    t = np.zeros((M, M))
+    for j0 in range(0, a, chunk):
+        j1 = min(a, j0 + chunk)
+        nj = j1 - j0
+        sw = _stacked(W, Co_s, Ca_s, j0, j1, R)
+        sv = _stacked(V, Co_s, Ca_s, j0, j1, R)
+        svs = (Sinv @ sv.reshape(Rp, nj * M, order='F')).reshape(Rp * nj, M, order='F')
+        X += sw.T @ svs
+    for k0 in range(0, o, chunk):
+        k1 = min(o, k0 + chunk)
+        b2w = T3(T1(W.J3_0, Co_s[:, k0:k1], W.P2), Ca_s)
+        b2v = T3(T1(V.J3_0, Co_s[:, k0:k1], V.P2), Ca_s)
+        t += b2w.T @ b2v
+    return X, t
+
+
+def chunked_direct_fock(W, V, Co_s, a, Y, chunk):
+    """Σ_k (B1_W Y)_k (B1_V)_k^T (active orbitals k >= c weighted 2), with B1 of
+    W and V formed for at most `chunk` occupied orbitals at a time."""
+    N = W.n_ao
+    o = Co_s.shape[1]
+    c = o - a
+    F = np.zeros((N, N))
+    for k0 in range(0, o, chunk):
+        k1 = min(o, k0 + chunk)
+        nk = k1 - k0
+        b1w = T1(W.J3_0, Co_s[:, k0:k1], W.P2)
+        b1v = T1(V.J3_0, Co_s[:, k0:k1], V.P2)
+        Z3 = (b1w @ Y).reshape((N, nk, -1), order='F').copy()
+        for idx in range(nk):
+            if a > 0 and k0 + idx >= c:
+                Z3[:, idx, :] *= 2.0
+        F += Z3.reshape(N, -1, order='F') @ b1v.reshape(N, -1, order='F').T
+    return F
