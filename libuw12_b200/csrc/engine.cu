@@ -765,7 +765,16 @@ void form_fock(const FockRequest& rq) {
   };
   PerX XW, XV;
   const bool need_sv_w = calc && do_ind;
-  for (int which = 0; which < 2; ++which) {
+  // Without same-spin terms the stacked transforms serve only X_AB, t and the
+  // direct Fock, which are sums over orbitals: when the whole intermediates
+  // (B1, B2, Wst of W and V, S^-1 Wst_V) exceed the chunk budget they are
+  // formed for a chunk of orbitals at a time instead (orbital_chunked).
+  budget = auto_budget_doubles(rq.mem_budget);
+  size_t whole = 0;
+  for (int s = 0; s < ns; ++s)
+    whole += 2 * (N * sd[s].o * MW + sd[s].a * sd[s].o * MW) + 3 * Rp * sd[s].a * MW;
+  const bool orbital_chunked = !do_ind && whole > budget;
+  for (int which = 0; which < 2 && !orbital_chunked; ++which) {
     const IntegralsHandle& X = which == 0 ? W : V;
     PerX& P = which == 0 ? XW : XV;
     const size_t M = X.n_df;
@@ -818,7 +827,95 @@ void form_fock(const FockRequest& rq) {
   // =====================================================================
   clock.mark("xab_t_energies");
   std::vector<DevBuf> Xab(ns), tab(ns), ttl(ns);
-  for (int s = 0; s < ns; ++s) {
+  // B1 (N*nk x M) of occupied orbitals [k0, k0 + nk) of spin s for potential X:
+  // sq(J3_0[:, A]) Co[:, k] P2.
+  auto b1_chunk = [&](const IntegralsHandle& X, int s, size_t k0, size_t nk, DevBuf& out) {
+    const size_t M = X.n_df;
+    DevBuf H(N * nk * M);
+    transform_ao(X, Co.get() + N * (sd[s].ooff + k0), nk, H.get(), budget / 2);
+    out.alloc(N * nk * M);
+    gemm(gemm_nn(LL(N * nk), LL(M), LL(M), 1.0, H.get(), LL(N * nk), X.P2.get(), LL(M), 0.0,
+                 out.get(), LL(N * nk)));
+  };
+  // occupied orbitals per chunk of the t and direct-Fock passes, active
+  // orbitals per chunk of the X_AB pass
+  // (per occupied orbital: B1 of W and V, the transform's output, Z or the two
+  // B2 rows of its a active orbitals)
+  auto per_k = [&](int s) { return (4 * N + 2 * sd[s].a) * MW; };
+  const size_t per_j = (N + R + 3 * Rp) * MW;
+  if (orbital_chunked) {
+    for (int s = 0; s < ns; ++s) {
+      const size_t o = sd[s].o, a = sd[s].a, c = sd[s].c;
+      Xab[s].alloc(MW * MV);
+      tab[s].alloc(MW * MV);
+      ttl[s].alloc(MW * MV);
+      Xab[s].zero();
+      tab[s].zero();
+      if (a == 0) {
+        ttl[s].zero();
+        continue;
+      }
+      // X_AB = sum over active-orbital chunks of Wst_W[j]^T S^-1 Wst_V[j]
+      const size_t jc = std::max<size_t>(1, std::min(a, budget / 2 / per_j));
+      for (size_t j0 = 0; j0 < a; j0 += jc) {
+        const size_t nj = std::min(jc, a - j0);
+        DevBuf St[2];
+        for (int which = 0; which < 2; ++which) {
+          const IntegralsHandle& X = which == 0 ? W : V;
+          const size_t M = X.n_df;
+          St[which].alloc(Rp * nj * M);
+          // AO rows of orbital j: sq(J3_0) Co[:, c + j] P2, into rows [0, N) of its block
+          DevBuf H(N * nj * M);
+          transform_ao(X, Co.get() + N * (sd[s].ooff + c + j0), nj, H.get(), budget / 2);
+          GemmDesc ga = gemm_nn(LL(N), LL(M), LL(M), 1.0, H.get(), LL(N * nj), X.P2.get(), LL(M),
+                                0.0, St[which].get(), LL(Rp * nj));
+          ga.nbo1 = LL(nj);
+          ga.sAo1 = LL(N);
+          ga.sCo1 = LL(Rp);
+          gemm(ga);
+          // RI rows: J3ri_0[:, A] Ca[:, j] P2, into rows [N, R') of its block
+          DevBuf H2(R * nj * M);
+          ri_transform(X, Ca_s(s) + N * j0, nj, H2.get(), budget);
+          GemmDesc gr = gemm_nn(LL(R), LL(M), LL(M), 1.0, H2.get(), LL(R * nj), X.P2.get(), LL(M),
+                                0.0, St[which].get() + N, LL(Rp * nj));
+          gr.nbo1 = LL(nj);
+          gr.sAo1 = LL(R);
+          gr.sCo1 = LL(Rp);
+          gemm(gr);
+        }
+        DevBuf SVj(Rp * nj * MV);
+        gemm(gemm_nn(LL(Rp), LL(nj * MV), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp), St[1].get(),
+                     LL(Rp), 0.0, SVj.get(), LL(Rp)));
+        GemmDesc gx = gemm_nn(LL(MW), LL(MV), LL(Rp * nj), 1.0, St[0].get(), LL(Rp * nj),
+                              SVj.get(), LL(Rp * nj), j0 ? 1.0 : 0.0, Xab[s].get(), LL(MW));
+        gx.a_kcontig = true;
+        gemm(gx);
+      }
+      // t = sum over occupied-orbital chunks of B2_W[k]^T B2_V[k], B2 = Ca^T B1
+      const size_t kc = std::max<size_t>(1, std::min(o, budget / 2 / per_k(s)));
+      for (size_t k0 = 0; k0 < o; k0 += kc) {
+        const size_t nk = std::min(kc, o - k0);
+        DevBuf B1w, B1v, B2w(a * nk * MW), B2v(a * nk * MV);
+        b1_chunk(W, s, k0, nk, B1w);
+        b1_chunk(V, s, k0, nk, B1v);
+        GemmDesc g3 = gemm_nn(LL(a), LL(nk * MW), LL(N), 1.0, Ca_s(s), LL(N), B1w.get(), LL(N),
+                              0.0, B2w.get(), LL(a));
+        g3.a_kcontig = true;
+        gemm(g3);
+        g3 = gemm_nn(LL(a), LL(nk * MV), LL(N), 1.0, Ca_s(s), LL(N), B1v.get(), LL(N), 0.0,
+                     B2v.get(), LL(a));
+        g3.a_kcontig = true;
+        gemm(g3);
+        GemmDesc gt = gemm_nn(LL(MW), LL(MV), LL(a * nk), 1.0, B2w.get(), LL(a * nk), B2v.get(),
+                              LL(a * nk), k0 ? 1.0 : 0.0, tab[s].get(), LL(MW));
+        gt.a_kcontig = true;
+        gemm(gt);
+      }
+      scale_rc(tab[s].get(), LL(MW), LL(MW), LL(MV), W.lam.get(), V.lam.get(), 1.0,
+               ttl[s].get(), LL(MW));
+    }
+  }
+  for (int s = 0; s < ns && !orbital_chunked; ++s) {
     const size_t o = sd[s].o, a = sd[s].a;
     Xab[s].alloc(MW * MV);
     tab[s].alloc(MW * MV);
@@ -849,7 +946,7 @@ void form_fock(const FockRequest& rq) {
         wdot(ttl[sp].get(), LL(MW), tab[s].get(), LL(MW), LL(MW), LL(MV), nullptr, nullptr,
              0.5 * f, acc.get(), kE4d);
     }
-  if (!do_ind)  // the stacked transforms serve only X_AB and the same-spin terms
+  if (!do_ind && !orbital_chunked)  // the stacked transforms serve only X_AB and the same-spin terms
     for (int s = 0; s < ns; ++s) {
       XW.Wst[s].release();
       XW.SV[s].release();
@@ -875,19 +972,34 @@ void form_fock(const FockRequest& rq) {
         cT[sp] = (f != 0.0) ? f * (a == 0 ? kap4 : 0.5 * kap4) : 0.0;
         cX[sp] = half * f;
       }
-      DevBuf Y(MW * MV), Z(N * o * MV);
+      DevBuf Y(MW * MV);
       combine_y(Y.get(), LL(MW), Tq, cT, Xq, cX, ns, W.lam.get(), V.lam.get());
-      gemm(gemm_nn(LL(N * o), LL(MV), LL(MW), 1.0, XW.B1[s].get(), LL(N * o), Y.get(), LL(MW),
-                   0.0, Z.get(), LL(N * o)));
-      if (a > 0)
-        copy3d(Z.get() + N * c, LL(N * o), 0, Z.get() + N * c, LL(N * o), 0, LL(N * a), LL(MV), 1,
-               2.0);
-      GemmDesc gf = gemm_nn(LL(N), LL(N), LL(o * MV), 1.0, Z.get(), LL(N), XV.B1[s].get(), LL(N),
-                            1.0, Fp[s].get(), LL(N));
-      gf.b_ncontig = true;
-      gemm(gf);
+      // whole B1, or B1 of W and V recomputed for a chunk of occupied orbitals
+      const size_t kc =
+          orbital_chunked ? std::max<size_t>(1, std::min(o, budget / 2 / per_k(s))) : o;
+      for (size_t k0 = 0; k0 < o; k0 += kc) {
+        const size_t nk = std::min(kc, o - k0);
+        DevBuf B1w, B1v, Z(N * nk * MV);
+        if (orbital_chunked) {
+          b1_chunk(W, s, k0, nk, B1w);
+          b1_chunk(V, s, k0, nk, B1v);
+        }
+        const double* bw = orbital_chunked ? B1w.get() : XW.B1[s].get();
+        const double* bv = orbital_chunked ? B1v.get() : XV.B1[s].get();
+        gemm(gemm_nn(LL(N * nk), LL(MV), LL(MW), 1.0, bw, LL(N * nk), Y.get(), LL(MW), 0.0,
+                     Z.get(), LL(N * nk)));
+        // active orbitals (k >= c) weighted 2
+        const size_t a0 = std::max(c, k0), a1 = k0 + nk;
+        if (a > 0 && a1 > a0)
+          copy3d(Z.get() + N * (a0 - k0), LL(N * nk), 0, Z.get() + N * (a0 - k0), LL(N * nk), 0,
+                 LL(N * (a1 - a0)), LL(MV), 1, 2.0);
+        GemmDesc gf = gemm_nn(LL(N), LL(N), LL(nk * MV), 1.0, Z.get(), LL(N), bv, LL(N), 1.0,
+                              Fp[s].get(), LL(N));
+        gf.b_ncontig = true;
+        gemm(gf);
+      }
     }
-    if (!do_ind)  // B1 and B2 serve only the direct Fock and the same-spin terms
+    if (!do_ind && !orbital_chunked)  // B1 and B2 serve only the direct Fock and the same-spin terms
       for (int s = 0; s < ns; ++s) {
         XW.B1[s].release();
         XW.B2[s].release();
