@@ -148,3 +148,79 @@ def direct_adjoint(Wb, Vb, WVb, abs_p, orbitals, occ, n_active, s_os, s_ss):
     gX2 = -sym(QX @ AX @ QX.T)
     return {"W3": gW3, "W3_ri": gW3ri, "W2": gW2, "V3": gV3, "V3_ri": gV3ri, "V2": gV2,
             "WV3": gWV3, "WV2": gX2}
+
+
+def chunked_three_index_adjoint(Wb, Vb, abs_p, orbitals, occ, n_active, s_os, s_ss, chunk):
+    """dE/dJ3_0 and dE/dJ3_ri_0 of W and V (as ``direct_adjoint``) with every
+    stacked intermediate formed for at most ``chunk`` orbitals at a time:
+    X and t accumulated over orbital chunks (schedule_model.chunked_xab_t); the
+    reverse sweep splits by linearity into a B2-bar path over chunks of
+    occupied orbitals k (B1bar_k = Ca (B2_other,k tbar^T)) and a Wst-bar path
+    over chunks of active orbitals j ((S^-1 Wst_other,j) Xbar^T, whose AO rows
+    add to B1bar of orbital c + j and whose RI rows are Bri-bar of j); both
+    reach dE/dJ3 through P2^T and the per-aux-function contractions with Co
+    (packed symmetric sum) and Ca."""
+    from tests import schedule_model as K
+    ns = len(orbitals)
+    Co = O.occupation_weighted_orbitals(orbitals, occ)
+    Ca = O.freeze_core(Co, n_active)
+    W = O.Integrals(Wb, Co, Ca)
+    V = O.Integrals(Vb, Co, Ca)
+    N, M, R = Wb.n_ao, Wb.n_df, Wb.n_ri
+    Rp = N + R
+    F = np.array([[spin_factor(ns, s, sp, s_os, s_ss) for sp in range(ns)] for s in range(ns)])
+    lw, lv = W.df_vals, V.df_vals
+    Sinv = np.block([[abs_p.s_inv_ao_ao, abs_p.s_inv_ao_ri], [abs_p.s_inv_ri_ao, abs_p.s_inv_ri_ri]])
+    X, t = [], []
+    for s in range(ns):
+        xs, ts = K.chunked_xab_t(Wb, Vb, Sinv, Co[s], Ca[s], chunk)
+        X.append(xs)
+        t.append(ts)
+    tt = [lw[:, None] * t[s] * lv[None, :] for s in range(ns)]
+    tbar, Xbar = [], []
+    for s in range(ns):
+        tb = sum(0.5 * F[s, sp] * tt[sp] for sp in range(ns))
+        ttb = sum(F[sp, s] * (0.5 * t[sp] - X[sp]) for sp in range(ns))
+        tbar.append(tb + lw[:, None] * ttb * lv[None, :])
+        Xbar.append(-sum(F[s, sp] * tt[sp] for sp in range(ns)))
+    out = {}
+    for which, (Xi, Yi) in enumerate(((Wb, Vb), (Vb, Wb))):
+        P2 = Xi.P2
+        g3 = np.zeros((N * (N + 1) // 2, M))
+        g3ri = np.zeros((R * N, M))
+        for s in range(ns):
+            o, a = Co[s].shape[1], Ca[s].shape[1]
+            c = o - a
+            if a == 0:
+                continue
+            tb = tbar[s].T if which == 0 else tbar[s]
+            xb = Xbar[s].T if which == 0 else Xbar[s]
+            # B2-bar path, chunks of occupied orbitals k
+            for k0 in range(0, o, chunk):
+                k1 = min(o, k0 + chunk)
+                nk = k1 - k0
+                b2o = K.T3(K.T1(Yi.J3_0, Co[s][:, k0:k1], Yi.P2), Ca[s])  # a nk x M
+                b2b = b2o @ tb
+                b1b = (Ca[s] @ b2b.reshape((a, nk * M), order="F")).reshape((N * nk, M),
+                                                                           order="F")
+                b10 = b1b @ P2.T
+                for A in range(M):
+                    G = b10[:, A].reshape((N, nk), order="F") @ Co[s][:, k0:k1].T
+                    g3[:, A] += _pack_sym_sum(G)
+            # Wst-bar path, chunks of active orbitals j
+            for j0 in range(0, a, chunk):
+                j1 = min(a, j0 + chunk)
+                nj = j1 - j0
+                sy = K._stacked(Yi, Co[s], Ca[s], j0, j1, R)
+                ssy = (Sinv @ sy.reshape(Rp, nj * M, order="F")).reshape(Rp * nj, M, order="F")
+                wsb = (ssy @ xb).reshape((Rp, nj, M), order="F")
+                ao = (wsb[:N].reshape((N * nj, M), order="F")) @ P2.T
+                ri = (wsb[N:].reshape((R * nj, M), order="F")) @ P2.T
+                for A in range(M):
+                    G = ao[:, A].reshape((N, nj), order="F") @ Co[s][:, c + j0:c + j1].T
+                    g3[:, A] += _pack_sym_sum(G)
+                    g3ri[:, A] += (ri[:, A].reshape((R, nj), order="F") @
+                                   Ca[s][:, j0:j1].T).reshape(-1, order="F")
+        out["W3" if which == 0 else "V3"] = g3
+        out["W3_ri" if which == 0 else "V3_ri"] = g3ri
+    return out

@@ -82,3 +82,24 @@ def test_stacked_x_matches_oracle_xab():
 
         x = st(Wi).T @ np.kron(np.eye(a), Sinv) @ st(Vi)
         assert np.allclose(x, x_ref[s], rtol=1e-12, atol=1e-12 * np.abs(x_ref[s]).max())
+
+
+@pytest.mark.parametrize("chunk", [1, 2])
+@pytest.mark.parametrize("name", ["closed", "frozen", "open"])
+def test_orbital_chunked_three_index_adjoint(name, chunk):
+    """The reverse sweep over orbital chunks (the memory layout of large
+    systems) equals the whole-intermediate adjoint (1e-12)."""
+    case = {"closed": Case("closed", 6, 10, 9, (3,), (3,), "baseline", 3, 4.0),
+            "frozen": Case("frozen", 6, 10, 9, (3,), (2,), "baseline", 3, 4.0),
+            "open": Case("open", 7, 11, 9, (4, 3), (3, 2), "baseline", 3, 4.0)}[name]
+    d = make_case(case)
+    Wb = O.BaseIntegrals(d.W3, d.W2, d.W3_ri)
+    Vb = O.BaseIntegrals(d.V3, d.V2, d.V3_ri)
+    WVb = O.BaseIntegrals(d.WV3, d.WV2)
+    absp = O.calculate_abs_projectors(d.S, case.n_ao, case.n_ri)
+    ref = AR.direct_adjoint(Wb, Vb, WVb, absp, d.orbitals, d.occ, list(case.n_active), 1.0, 0.5)
+    got = AR.chunked_three_index_adjoint(Wb, Vb, absp, d.orbitals, d.occ, list(case.n_active),
+                                         1.0, 0.5, chunk)
+    for key in ("W3", "W3_ri", "V3", "V3_ri"):
+        scale = max(np.max(np.abs(ref[key])), 1e-300)
+        assert np.max(np.abs(got[key] - ref[key])) <= 1e-12 * scale, key
