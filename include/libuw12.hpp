@@ -597,13 +597,14 @@ struct SinkState {
 
 }  // namespace detail_b200
 
-/// Reverse mode of the direct terms (uw12c_fock_backward): energy, terms and
-/// Fock plus every gradient, in host memory.
+/// Reverse mode of form_fock (uw12c_fock_backward): energy, terms and Fock
+/// plus every gradient, in host memory; the direct terms only unless
+/// indirect_term (then, with scale_same_spin != 0, the energy of uw12_energy).
 inline BackwardResult fock_backward(const BaseIntegrals& W, const BaseIntegrals& V,
                                     const BaseIntegrals& WV, const ABSProjectors& abs_projectors,
                                     const Orbitals& orbitals, const Occupations& occupations,
                                     const std::vector<size_t>& n_active, double scale_opp_spin,
-                                    double scale_same_spin) {
+                                    double scale_same_spin, bool indirect_term = false) {
   const auto a = detail_b200::spin_args(orbitals, occupations, n_active);
   const BaseIntegrals* X[3] = {&W, &V, &WV};
   BackwardResult r;
@@ -621,8 +622,9 @@ inline BackwardResult fock_backward(const BaseIntegrals& W, const BaseIntegrals&
   linalg::Mat fock(a.n_ao, a.n_ao * a.n_spin);
   detail::check(uw12c_fock_backward(W.handle(), V.handle(), WV.handle(), abs_projectors.handle(),
                                     a.n_ao, a.n_spin, a.C.data(), a.ldc.data(), a.n_orb.data(),
-                                    a.occ.data(), a.n_occ.data(), n_active.data(), scale_opp_spin,
-                                    scale_same_spin, &r.fock_energy.energy, r.terms,
+                                    a.occ.data(), a.n_occ.data(), n_active.data(),
+                                    indirect_term ? 1 : 0, scale_opp_spin, scale_same_spin,
+                                    &r.fock_energy.energy, r.terms,
                                     fock.memptr(), UW12C_MEM_HOST, d3, d3ri, d2, UW12C_MEM_HOST));
   for (size_t s = 0; s < a.n_spin; ++s)
     r.fock_energy.fock.emplace_back(fock.memptr() + s * a.n_ao * a.n_ao, a.n_ao, a.n_ao);
@@ -640,7 +642,8 @@ inline BackwardResult fock_backward_blocks(const BaseIntegrals& W, const BaseInt
                                            const Occupations& occupations,
                                            const std::vector<size_t>& n_active,
                                            double scale_opp_spin, double scale_same_spin,
-                                           const std::array<GradientSink, 5>& sinks) {
+                                           const std::array<GradientSink, 5>& sinks,
+                                           bool indirect_term = false) {
   const auto a = detail_b200::spin_args(orbitals, occupations, n_active);
   const BaseIntegrals* X[3] = {&W, &V, &WV};
   BackwardResult r;
@@ -662,7 +665,8 @@ inline BackwardResult fock_backward_blocks(const BaseIntegrals& W, const BaseInt
   const int status = uw12c_fock_backward_blocks(
       W.handle(), V.handle(), WV.handle(), abs_projectors.handle(), a.n_ao, a.n_spin, a.C.data(),
       a.ldc.data(), a.n_orb.data(), a.occ.data(), a.n_occ.data(), n_active.data(),
-      scale_opp_spin, scale_same_spin, &r.fock_energy.energy, r.terms, fock.memptr(),
+      indirect_term ? 1 : 0, scale_opp_spin, scale_same_spin, &r.fock_energy.energy, r.terms,
+      fock.memptr(),
       UW12C_MEM_HOST, fn, users, fn + 3, users + 3, UW12C_MEM_HOST, d2, UW12C_MEM_HOST);
   if (status != UW12C_OK) {
     for (auto& s : st)

@@ -146,11 +146,14 @@ int uw12c_fock_batched(const uw12c_molecule* mols, size_t n, int indirect_term,
                        int calculate_fock, double scale_opp_spin, double scale_same_spin,
                        size_t n_streams, int* statuses);
 
-/* Reverse mode of the direct terms (no counterpart in libuw12): with
- * indirect_term = 0 (the opposite-spin form of uw12_energy, scale_same_spin
- * entering only the direct same-spin pairs) the energy, terms and Fock
- * (dE/dD, as uw12c_form_fock) plus the gradient of the energy with respect to
- * the stored integrals:
+/* Reverse mode of uw12c_form_fock (no counterpart in libuw12): the energy,
+ * terms and Fock (dE/dD) of uw12c_form_fock with the same arguments plus the
+ * gradient of that energy with respect to the stored integrals.
+ * indirect_term = 0 differentiates the direct terms only (scale_same_spin
+ * entering the direct same-spin pairs); indirect_term = 1 with
+ * scale_same_spin != 0 adds the same-spin (exchange) energies of the two-,
+ * three- and four-electron terms, i.e. the energy of uw12c_fock /
+ * uw12_energy (libuw12.cpp:138 runs them when |scale_same_spin| > 4 eps).
  *   dE_dX3[3]    W, V, WV: packed n_ao(n_ao+1)/2 x n_df, entry (mn|P) of the
  *                packed storage (both triangle halves of sq(X3[:,P]) summed);
  *   dE_dX3_ri[2] W, V: (n_ri n_ao) x n_df, the X3_ri layout;
@@ -163,7 +166,8 @@ int uw12c_fock_backward(const uw12c_integrals* W, const uw12c_integrals* V,
                         const uw12c_integrals* WV, const uw12c_abs* abs, size_t n_ao,
                         size_t n_spin, const double* const* C, const size_t* ldc,
                         const size_t* n_orb, const double* const* occ, const size_t* n_occ,
-                        const size_t* n_active, double scale_opp_spin, double scale_same_spin,
+                        const size_t* n_active, int indirect_term, double scale_opp_spin,
+                        double scale_same_spin,
                         double* energy, double* terms, double* fock, int fock_mem_kind,
                         double* const* dE_dX3, double* const* dE_dX3_ri, double* const* dE_dX2,
                         int grad_mem_kind);
@@ -191,8 +195,9 @@ int uw12c_fock_backward_blocks(const uw12c_integrals* W, const uw12c_integrals* 
                                size_t n_spin, const double* const* C, const size_t* ldc,
                                const size_t* n_orb, const double* const* occ,
                                const size_t* n_occ, const size_t* n_active,
-                               double scale_opp_spin, double scale_same_spin, double* energy,
-                               double* terms, double* fock, int fock_mem_kind,
+                               int indirect_term, double scale_opp_spin,
+                               double scale_same_spin, double* energy, double* terms,
+                               double* fock, int fock_mem_kind,
                                const uw12c_block_sink* sink3, void* const* user3,
                                const uw12c_block_sink* sink3_ri, void* const* user3_ri,
                                int block_mem_kind, double* const* dE_dX2, int grad_mem_kind);

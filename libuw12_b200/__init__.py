@@ -92,11 +92,13 @@ def lib():
     L.uw12c_fock_batched.argtypes = [P, c_sz, ctypes.c_int, ctypes.c_int, c_d, c_d, c_sz,
                                      ctypes.POINTER(ctypes.c_int)]
     L.uw12c_fock_backward.argtypes = [P, P, P, P, c_sz, c_sz, ctypes.POINTER(P), PSZ, PSZ,
-                                      ctypes.POINTER(P), PSZ, PSZ, c_d, c_d, PD, PD, P,
+                                      ctypes.POINTER(P), PSZ, PSZ, ctypes.c_int, c_d, c_d, PD,
+                                      PD, P,
                                       ctypes.c_int, ctypes.POINTER(P), ctypes.POINTER(P),
                                       ctypes.POINTER(P), ctypes.c_int]
     L.uw12c_fock_backward_blocks.argtypes = [P, P, P, P, c_sz, c_sz, ctypes.POINTER(P), PSZ,
-                                             PSZ, ctypes.POINTER(P), PSZ, PSZ, c_d, c_d, PD, PD,
+                                             PSZ, ctypes.POINTER(P), PSZ, PSZ, ctypes.c_int, c_d,
+                                             c_d, PD, PD,
                                              P, ctypes.c_int, ctypes.POINTER(P),
                                              ctypes.POINTER(P), ctypes.POINTER(P),
                                              ctypes.POINTER(P), ctypes.c_int, ctypes.POINTER(P),
@@ -511,11 +513,13 @@ def fock_backward(W: BaseIntegrals, V: BaseIntegrals, WV: BaseIntegrals, abs_p: 
                   orbitals: Sequence[np.ndarray], occupations: Sequence[np.ndarray],
                   n_active: Sequence[int], scale_opp_spin: float, scale_same_spin: float,
                   gradients: Sequence[str] = GRADIENT_NAMES, calculate_fock: bool = True,
-                  device_out: Optional[dict] = None):
-    """Reverse mode of the direct terms (``uw12c_fock_backward``).
+                  device_out: Optional[dict] = None, indirect_term: bool = False):
+    """Reverse mode of ``form_fock`` (``uw12c_fock_backward``).
 
     Returns ``(energy, fock, (E2, E3, E4), grads)``: the energy, per-spin Fock
-    and terms of ``form_fock(..., indirect_term=False)`` and a dict of the
+    and terms of ``form_fock(..., indirect_term, ...)`` (the direct terms only
+    by default; with ``indirect_term`` and ``scale_same_spin != 0`` the
+    same-spin terms too, the energy of ``uw12_energy``) and a dict of the
     requested gradients of that energy with respect to the stored integrals
     ("W3", "V3", "WV3" packed n_ao(n_ao+1)/2 x n_df; "W3_ri", "V3_ri"
     (n_ri n_ao) x n_df; "W2", "V2", "WV2" n_df x n_df).  With ``device_out``
@@ -555,7 +559,8 @@ def fock_backward(W: BaseIntegrals, V: BaseIntegrals, WV: BaseIntegrals, abs_p: 
     terms = (ctypes.c_double * 3)()
     fock = np.zeros((n_ao, n_ao * n_spin), order="F") if calculate_fock else None
     _check(lib().uw12c_fock_backward(W.handle, V.handle, WV.handle, abs_p.handle, n_ao, n_spin,
-                                     c_ptrs, ldc, norb, o_ptrs, nocc, nact, float(scale_opp_spin),
+                                     c_ptrs, ldc, norb, o_ptrs, nocc, nact,
+                                     int(bool(indirect_term)), float(scale_opp_spin),
                                      float(scale_same_spin), ctypes.byref(energy), terms,
                                      _fptr(fock) if fock is not None else P(0), MEM_HOST, d3,
                                      d3ri, d2, MEM_DEVICE if device_out is not None else MEM_HOST))
@@ -582,9 +587,10 @@ def fock_backward_blocks(W: BaseIntegrals, V: BaseIntegrals, WV: BaseIntegrals,
                          scale_opp_spin: float, scale_same_spin: float, sinks: dict,
                          metric_gradients: Sequence[str] = ("W2", "V2", "WV2"),
                          calculate_fock: bool = True, device: bool = False,
-                         users: Optional[dict] = None):
+                         users: Optional[dict] = None, indirect_term: bool = False):
     """``uw12c_fock_backward_blocks``: the three-index gradients delivered in aux
-    blocks.  ``sinks`` maps names of ``BLOCK_GRADIENT_NAMES`` to Python callables
+    blocks (``indirect_term`` as for ``fock_backward``).  ``sinks`` maps names of
+    ``BLOCK_GRADIENT_NAMES`` to Python callables
     ``f(first, count, block)`` (``block`` a host ``rows x count`` array, valid
     during the call; ``device=False``) or to C function pointers (ints) with
     ``users[name]`` as their user pointer (``device=True`` passes device
@@ -636,8 +642,9 @@ def fock_backward_blocks(W: BaseIntegrals, V: BaseIntegrals, WV: BaseIntegrals,
     fock = np.zeros((n_ao, n_ao * n_spin), order="F") if calculate_fock else None
     _check(lib().uw12c_fock_backward_blocks(
         W.handle, V.handle, WV.handle, abs_p.handle, n_ao, n_spin, c_ptrs, ldc, norb, o_ptrs,
-        nocc, nact, float(scale_opp_spin), float(scale_same_spin), ctypes.byref(energy), terms,
-        _fptr(fock) if fock is not None else P(0), MEM_HOST, s3, u3, s3ri, u3ri,
+        nocc, nact, int(bool(indirect_term)), float(scale_opp_spin), float(scale_same_spin),
+        ctypes.byref(energy), terms, _fptr(fock) if fock is not None else P(0), MEM_HOST, s3, u3,
+        s3ri, u3ri,
         MEM_DEVICE if device else MEM_HOST, d2, MEM_HOST))
     focks = None
     if fock is not None:

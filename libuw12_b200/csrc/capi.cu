@@ -439,10 +439,10 @@ int uw12c_fock_backward(const uw12c_integrals* W, const uw12c_integrals* V,
                         const uw12c_integrals* WV, const uw12c_abs* abs, size_t n_ao,
                         size_t n_spin, const double* const* C, const size_t* ldc,
                         const size_t* n_orb, const double* const* occ, const size_t* n_occ,
-                        const size_t* n_active, double scale_opp_spin, double scale_same_spin,
-                        double* energy, double* terms, double* fock, int fock_mem_kind,
-                        double* const* dE_dX3, double* const* dE_dX3_ri, double* const* dE_dX2,
-                        int grad_mem_kind) {
+                        const size_t* n_active, int indirect_term, double scale_opp_spin,
+                        double scale_same_spin, double* energy, double* terms, double* fock,
+                        int fock_mem_kind, double* const* dE_dX3, double* const* dE_dX3_ri,
+                        double* const* dE_dX2, int grad_mem_kind) {
   return guarded([&] {
     need(grad_mem_kind == UW12C_MEM_HOST || grad_mem_kind == UW12C_MEM_DEVICE,
          "bad grad_mem_kind");
@@ -454,9 +454,9 @@ int uw12c_fock_backward(const uw12c_integrals* W, const uw12c_integrals* V,
     }
     for (int i = 0; i < 2; ++i) ad.dJ3_ri[i] = dE_dX3_ri ? dE_dX3_ri[i] : nullptr;
     ad.device_mem = grad_mem_kind == UW12C_MEM_DEVICE;
-    run_form_fock(W, V, WV, abs, n_ao, n_spin, C, ldc, n_orb, occ, n_occ, n_active, 0,
-                  fock != nullptr, scale_opp_spin, scale_same_spin, 0, energy, terms, fock,
-                  fock_mem_kind, &ad);
+    run_form_fock(W, V, WV, abs, n_ao, n_spin, C, ldc, n_orb, occ, n_occ, n_active,
+                  indirect_term, fock != nullptr, scale_opp_spin, scale_same_spin, 0, energy,
+                  terms, fock, fock_mem_kind, &ad);
   });
 }
 
@@ -512,8 +512,9 @@ int uw12c_fock_backward_blocks(const uw12c_integrals* W, const uw12c_integrals* 
                                size_t n_spin, const double* const* C, const size_t* ldc,
                                const size_t* n_orb, const double* const* occ,
                                const size_t* n_occ, const size_t* n_active,
-                               double scale_opp_spin, double scale_same_spin, double* energy,
-                               double* terms, double* fock, int fock_mem_kind,
+                               int indirect_term, double scale_opp_spin,
+                               double scale_same_spin, double* energy, double* terms,
+                               double* fock, int fock_mem_kind,
                                const uw12c_block_sink* sink3, void* const* user3,
                                const uw12c_block_sink* sink3_ri, void* const* user3_ri,
                                int block_mem_kind, double* const* dE_dX2, int grad_mem_kind) {
@@ -538,9 +539,9 @@ int uw12c_fock_backward_blocks(const uw12c_integrals* W, const uw12c_integrals* 
         ad.sink3_ri[i] = wrap_sink(sink3_ri[i], user3_ri ? user3_ri[i] : nullptr, host,
                                    X[i]->h->n_ri * X[i]->h->n_ao);
     ad.device_mem = grad_mem_kind == UW12C_MEM_DEVICE;
-    run_form_fock(W, V, WV, abs, n_ao, n_spin, C, ldc, n_orb, occ, n_occ, n_active, 0,
-                  fock != nullptr, scale_opp_spin, scale_same_spin, 0, energy, terms, fock,
-                  fock_mem_kind, &ad);
+    run_form_fock(W, V, WV, abs, n_ao, n_spin, C, ldc, n_orb, occ, n_occ, n_active,
+                  indirect_term, fock != nullptr, scale_opp_spin, scale_same_spin, 0, energy,
+                  terms, fock, fock_mem_kind, &ad);
   });
 }
 

@@ -1373,7 +1373,7 @@ void form_fock(const FockRequest& rq) {
 }
 
 // --------------------------------------------------------------------------
-// reverse mode of the direct terms
+// reverse mode (direct terms, and the same-spin terms with indirect_term)
 // --------------------------------------------------------------------------
 // Energy of the direct terms, with f = f(s, s') the spin factor
 // (four_electron_utils.cpp:9-30) and everything in the metric eigenbasis:
@@ -1396,10 +1396,11 @@ void form_fock(const FockRequest& rq) {
 //   dE/dJ2_W  = -sym(Q_W [sum_s 1/2 T_s L_V t[s]^T - X[s] L_V T_s^T] Q_W^T),
 //   dE/dJ2_V  = -sym(Q_V [sum_s 1/2 t[s]^T L_W T_s - T_s^T L_W X[s]] Q_V^T),
 //   dE/dJ2_WV = -1/2 sum_{s,s'} f (Q X_D[s]) (Q X_D[s'])^T,
-// with T_s = sum_s' f t[s'].
+// with T_s = sum_s' f t[s'].  With indirect_term the same-spin energies
+// (s_ss times E2-, E3-, E4-) add their own B2-bar, Wst-bar and metric terms
+// (comment at the same-spin section below).
 void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
   FockRequest rq = rq_in;
-  rq.indirect = false;
   if (rq.n_shards > 1) throw Error(kErrInvalid, "the adjoint evaluates unsharded");
   form_fock(rq);
 
@@ -1527,6 +1528,128 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
     lincomb(Xbar[s].get(), LL(MW), LL(MV), nt, mats, coefs, scaled, nullptr, nullptr);
   }
 
+  // ---- same-spin terms (indirect_term with s_ss != 0), energy s_ss E_ss:
+  //   E3- = esf <YW, P3(ZV)>, YW = Wst_W L_W B2_W^T, ZV = SW_V L_V B2_V^T
+  //   E4- = -1/2 esf <W4, P4(V4)>, W4 = B2_W L_W B2_W^T, V4 = B2_V L_V B2_V^T
+  //   E2- = -1/2 esf <B2_WV L_WV, B2_WV> (WV over the active orbitals, below)
+  // (esf = 2 closed shell, 1 open; P3, P4 the index exchanges of perm_3el,
+  // perm_4el). Their B2-bar and Wst-bar join the direct ones before the
+  // transforms are reversed; each L between eigenbasis factors adds
+  // (left factor)^T G (right factor) to the metric's A matrix:
+  //   G_Y = s esf P3(ZV), G_Z = s esf P3(YW) (chunks of occupied k),
+  //   Wst_W-bar = (sum_k G_Y B2_W,k) L_W, B2_W,k-bar = (G_Y^T Wst_W) L_W,
+  //   SW_V-bar = (sum_k G_Z B2_V,k) L_V -> Wst_V-bar = (I (x) S^-1) SW_V-bar,
+  //   B2_V,k-bar = (G_Z^T SW_V) L_V;  A_W += Wst_W^T T_Y, A_V += SW_V^T T_Z;
+  //   G_W4 = -1/2 s esf P4(V4): B2_W-bar += 2 (G_W4 B2_W) L_W,
+  //   A_W += B2_W^T G_W4 B2_W (and W <-> V with P4(W4)).
+  const bool same_spin = rq.indirect && rq.s_ss != 0.0;
+  std::vector<DevBuf> ssB2b[2], ssWsb[2];
+  DevBuf ssA[2];
+  if (same_spin) {
+    const double gs = two * rq.s_ss;
+    ssA[0].alloc(MW * MW);
+    ssA[0].zero();
+    ssA[1].alloc(MV * MV);
+    ssA[1].zero();
+    for (int which = 0; which < 2; ++which) {
+      ssB2b[which].resize(ns);
+      ssWsb[which].resize(ns);
+    }
+    for (int s = 0; s < ns; ++s) {
+      const size_t o = sd[s].o, a = sd[s].a;
+      if (a == 0 || o == 0) continue;
+      const size_t ao = a * o, Ra = Rp * a;
+      ssB2b[0][s].alloc(ao * MW);
+      ssB2b[1][s].alloc(ao * MV);
+      DevBuf b2wl(ao * MW), b2vl(ao * MV);
+      scale_rc(XW.B2[s].get(), LL(ao), LL(ao), LL(MW), nullptr, W.lam.get(), 1.0, b2wl.get(),
+               LL(ao));
+      scale_rc(XV.B2[s].get(), LL(ao), LL(ao), LL(MV), nullptr, V.lam.get(), 1.0, b2vl.get(),
+               LL(ao));
+      // three-electron, chunks of occupied orbitals k
+      {
+        budget = auto_budget_doubles(rq.mem_budget);
+        const size_t per_k = 3 * Ra * a + a * std::max(MW, MV);
+        const size_t kc = tile_chunk(o, a, std::max<size_t>(1, std::min(o, budget / per_k)));
+        DevBuf TY(Ra * MW), TZ(Ra * MV), Tmp(Ra * a * kc), GY(Ra * a * kc), GZ(Ra * a * kc),
+            Bt(a * kc * std::max(MW, MV));
+        for (size_t k0 = 0; k0 < o; k0 += kc) {
+          const size_t nk = std::min(kc, o - k0);
+          const double beta = k0 ? 1.0 : 0.0;
+          GemmDesc g = gemm_nn(LL(Ra), LL(a * nk), LL(MV), 1.0, XV.SW[s].get(), LL(Ra),
+                               b2vl.get() + a * k0, LL(ao), 0.0, Tmp.get(), LL(Ra));
+          g.b_ncontig = true;
+          gemm(g);
+          perm_3el(Tmp.get(), GY.get(), LL(Rp), LL(a), LL(nk), gs);
+          g = gemm_nn(LL(Ra), LL(a * nk), LL(MW), 1.0, XW.Wst[s].get(), LL(Ra),
+                      b2wl.get() + a * k0, LL(ao), 0.0, Tmp.get(), LL(Ra));
+          g.b_ncontig = true;
+          gemm(g);
+          perm_3el(Tmp.get(), GZ.get(), LL(Rp), LL(a), LL(nk), gs);
+          gemm(gemm_nn(LL(Ra), LL(MW), LL(a * nk), 1.0, GY.get(), LL(Ra),
+                       XW.B2[s].get() + a * k0, LL(ao), beta, TY.get(), LL(Ra)));
+          gemm(gemm_nn(LL(Ra), LL(MV), LL(a * nk), 1.0, GZ.get(), LL(Ra),
+                       XV.B2[s].get() + a * k0, LL(ao), beta, TZ.get(), LL(Ra)));
+          g = gemm_nn(LL(a * nk), LL(MW), LL(Ra), 1.0, GY.get(), LL(Ra), XW.Wst[s].get(),
+                      LL(Ra), 0.0, Bt.get(), LL(a * nk));
+          g.a_kcontig = true;
+          gemm(g);
+          scale_rc(Bt.get(), LL(a * nk), LL(a * nk), LL(MW), nullptr, W.lam.get(), 1.0,
+                   ssB2b[0][s].get() + a * k0, LL(ao));
+          g = gemm_nn(LL(a * nk), LL(MV), LL(Ra), 1.0, GZ.get(), LL(Ra), XV.SW[s].get(), LL(Ra),
+                      0.0, Bt.get(), LL(a * nk));
+          g.a_kcontig = true;
+          gemm(g);
+          scale_rc(Bt.get(), LL(a * nk), LL(a * nk), LL(MV), nullptr, V.lam.get(), 1.0,
+                   ssB2b[1][s].get() + a * k0, LL(ao));
+        }
+        GemmDesc g = gemm_nn(LL(MW), LL(MW), LL(Ra), 1.0, XW.Wst[s].get(), LL(Ra), TY.get(),
+                             LL(Ra), 1.0, ssA[0].get(), LL(MW));
+        g.a_kcontig = true;
+        gemm(g);
+        g = gemm_nn(LL(MV), LL(MV), LL(Ra), 1.0, XV.SW[s].get(), LL(Ra), TZ.get(), LL(Ra), 1.0,
+                    ssA[1].get(), LL(MV));
+        g.a_kcontig = true;
+        gemm(g);
+        ssWsb[0][s].alloc(Ra * MW);
+        scale_rc(TY.get(), LL(Ra), LL(Ra), LL(MW), nullptr, W.lam.get(), 1.0,
+                 ssWsb[0][s].get(), LL(Ra));
+        scale_rc(TZ.get(), LL(Ra), LL(Ra), LL(MV), nullptr, V.lam.get(), 1.0, TZ.get(), LL(Ra));
+        ssWsb[1][s].alloc(Ra * MV);
+        gemm(gemm_nn(LL(Rp), LL(a * MV), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp), TZ.get(), LL(Rp),
+                     0.0, ssWsb[1][s].get(), LL(Rp)));
+      }
+      // four-electron
+      {
+        DevBuf W4(ao * ao), V4(ao * ao), G4(ao * ao), T4(ao * std::max(MW, MV));
+        GemmDesc g = gemm_nn(LL(ao), LL(ao), LL(MW), 1.0, b2wl.get(), LL(ao), XW.B2[s].get(),
+                             LL(ao), 0.0, W4.get(), LL(ao));
+        g.b_ncontig = true;
+        gemm(g);
+        g = gemm_nn(LL(ao), LL(ao), LL(MV), 1.0, b2vl.get(), LL(ao), XV.B2[s].get(), LL(ao), 0.0,
+                    V4.get(), LL(ao));
+        g.b_ncontig = true;
+        gemm(g);
+        for (int which = 0; which < 2; ++which) {
+          const size_t M = which == 0 ? MW : MV;
+          const DevBuf& B2 = which == 0 ? XW.B2[s] : XV.B2[s];
+          const double* lam = which == 0 ? W.lam.get() : V.lam.get();
+          perm_4el(which == 0 ? V4.get() : W4.get(), G4.get(), LL(a), LL(o), -0.5 * gs);
+          gemm(gemm_nn(LL(ao), LL(M), LL(ao), 1.0, G4.get(), LL(ao), B2.get(), LL(ao), 0.0,
+                       T4.get(), LL(ao)));
+          GemmDesc ga = gemm_nn(LL(M), LL(M), LL(ao), 1.0, B2.get(), LL(ao), T4.get(), LL(ao),
+                                1.0, ssA[which].get(), LL(M));
+          ga.a_kcontig = true;
+          gemm(ga);
+          const double* mats[2] = {ssB2b[which][s].get(), T4.get()};
+          const double coefs[2] = {1.0, 2.0};
+          const int scaled[2] = {0, 1};
+          lincomb(ssB2b[which][s].get(), LL(ao), LL(M), 2, mats, coefs, scaled, nullptr, lam);
+        }
+      }
+    }
+  }
+
   // ---- dE/dJ3_0 and dE/dJ3_ri_0 of W and V
   for (int which = 0; which < 2; ++which) {
     const IntegralsHandle& X = which == 0 ? W : V;
@@ -1553,6 +1676,11 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
         gemm(gemm_nn(LL(a * o), LL(MV), LL(MW), 1.0, XW.B2[s].get(), LL(a * o), tbar[s].get(),
                      LL(MW), 0.0, B2b.get(), LL(a * o)));
       }
+      if (same_spin && ssB2b[which][s].size()) {
+        const double* mats[2] = {B2b.get(), ssB2b[which][s].get()};
+        const double coefs[2] = {1.0, 1.0};
+        lincomb(B2b.get(), LL(a * o), LL(M), 2, mats, coefs, nullptr, nullptr, nullptr);
+      }
       // B1bar_A (N x o) = Ca_s B2bar_A, into the spin block of Bb1
       GemmDesc g1 = gemm_nn(LL(N), LL(o), LL(a), 1.0, Ca_s(s), LL(N), B2b.get(), LL(a), 0.0,
                             Bb1.get() + N * sd[s].ooff, LL(N));
@@ -1570,6 +1698,11 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
       } else {
         gemm(gemm_nn(LL(Rp * a), LL(MV), LL(MW), 1.0, XW.SW[s].get(), LL(Rp * a), Xbar[s].get(),
                      LL(MW), 0.0, Wsb.get(), LL(Rp * a)));
+      }
+      if (same_spin && ssWsb[which][s].size()) {
+        const double* mats[2] = {Wsb.get(), ssWsb[which][s].get()};
+        const double coefs[2] = {1.0, 1.0};
+        lincomb(Wsb.get(), LL(Rp * a), LL(M), 2, mats, coefs, nullptr, nullptr, nullptr);
       }
       // AO rows -> active orbitals of B1bar; RI rows -> Bribar
       copy3d(Wsb.get(), LL(Rp), LL(Rp * a), Bb1.get() + N * (sd[s].ooff + c), LL(N),
@@ -1680,6 +1813,11 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
         gemm(g);
       }
     }
+    if (same_spin) {
+      const double* mats[2] = {Amat.get(), ssA[which].get()};
+      const double coefs[2] = {1.0, 1.0};
+      lincomb(Amat.get(), LL(M), LL(M), 2, mats, coefs, nullptr, nullptr, nullptr);
+    }
     DevBuf Q(M * M), QA(M * M);
     scale_rc(X.P2.get(), LL(M), LL(M), LL(M), nullptr, X.lam.get(), 1.0, Q.get(), LL(M));
     gemm(gemm_nn(LL(M), LL(M), LL(M), 1.0, Q.get(), LL(M), Amat.get(), LL(M), 0.0, QA.get(),
@@ -1691,8 +1829,72 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
     symmetrise(tmp.get(), LL(M), LL(M), g2, LL(M));
   }
 
-  // ---- WV: dE/dJ3_0 and dE/dJ2 through the fitted density
+  // ---- WV: dE/dJ3_0 and dE/dJ2 through the fitted density, and through the
+  // same-spin exchange E2- = -1/2 esf <B2 L, B2> (B2 = Ca^T B1, B1 of the
+  // active orbitals, two_electron.cpp:87-132): B2-bar = -s esf B2 L,
+  // B1-bar = Ca B2-bar, then P2^T and the packed symmetric sum per aux
+  // function with Ca; A_WV = -1/2 s esf B2^T B2
   const GradSink& s3x = out.sink3[2];
+  std::vector<DevBuf> ssX10(ns);  // B1-bar_0 of WV per spin (N a x MX)
+  DevBuf ssAX;
+  if (same_spin && (gJ3[2] || s3x || gJ2[2])) {
+    const double gs = two * rq.s_ss;
+    ssAX.alloc(MX * MX);
+    ssAX.zero();
+    budget = auto_budget_doubles(rq.mem_budget);
+    DevBuf H(N * a_tot * MX);
+    transform_ao(WV, Ca.get(), a_tot, H.get(), budget / 2);
+    for (int s = 0; s < ns; ++s) {
+      const size_t a = sd[s].a;
+      if (!a) continue;
+      DevBuf B1(N * a * MX), B2(a * a * MX), B2b(a * a * MX), B1b(N * a * MX);
+      gemm(gemm_nn(LL(N * a), LL(MX), LL(MX), 1.0, H.get() + N * sd[s].aoff, LL(N * a_tot),
+                   WV.P2.get(), LL(MX), 0.0, B1.get(), LL(N * a)));
+      GemmDesc g2 = gemm_nn(LL(a), LL(a * MX), LL(N), 1.0, Ca_s(s), LL(N), B1.get(), LL(N), 0.0,
+                            B2.get(), LL(a));
+      g2.a_kcontig = true;
+      gemm(g2);
+      GemmDesc ga = gemm_nn(LL(MX), LL(MX), LL(a * a), -0.5 * gs, B2.get(), LL(a * a), B2.get(),
+                            LL(a * a), 1.0, ssAX.get(), LL(MX));
+      ga.a_kcontig = true;
+      gemm(ga);
+      scale_rc(B2.get(), LL(a * a), LL(a * a), LL(MX), nullptr, WV.lam.get(), -gs, B2b.get(),
+               LL(a * a));
+      GemmDesc g1 = gemm_nn(LL(N), LL(a), LL(a), 1.0, Ca_s(s), LL(N), B2b.get(), LL(a), 0.0,
+                            B1b.get(), LL(N));
+      g1.nbo1 = LL(MX);
+      g1.sBo1 = LL(a * a);
+      g1.sCo1 = LL(N * a);
+      gemm(g1);
+      ssX10[s].alloc(N * a * MX);
+      GemmDesc gp = gemm_nn(LL(N * a), LL(MX), LL(MX), 1.0, B1b.get(), LL(N * a), WV.P2.get(),
+                            LL(MX), 0.0, ssX10[s].get(), LL(N * a));
+      gp.b_ncontig = true;
+      gemm(gp);
+    }
+  }
+  // adds the same-spin part of dE/dJ3_0^WV for aux functions [b0, b0 + nb)
+  // to dst (packed rows, leading dimension np)
+  auto add_ss_wv = [&](size_t b0, size_t nb, double* dst) {
+    if (!same_spin) return;
+    const size_t ac = std::max<size_t>(1, std::min(nb, budget / (4 * N * N)));
+    DevBuf G(N * N * ac);
+    for (int s = 0; s < ns; ++s) {
+      const size_t a = sd[s].a;
+      if (!a) continue;
+      for (size_t c0 = 0; c0 < nb; c0 += ac) {
+        const size_t nc = std::min(ac, nb - c0);
+        GemmDesc g = gemm_nn(LL(N), LL(N), LL(a), 1.0, ssX10[s].get() + N * a * (b0 + c0), LL(N),
+                             Ca_s(s), LL(N), 0.0, G.get(), LL(N));
+        g.b_ncontig = true;
+        g.nbo1 = LL(nc);
+        g.sAo1 = LL(N * a);
+        g.sCo1 = LL(N * N);
+        gemm(g);
+        pack_sym_sum(G.get(), LL(N), LL(nc), dst + np * c0, LL(np), 1.0);
+      }
+    }
+  };
   if (gJ3[2] || s3x || gJ2[2]) {
     DevBuf dmat(np * ns), XDr(MX * ns), XD(MX * ns), XDb(MX * ns), vb(MX * ns);
     for (int s = 0; s < ns; ++s)
@@ -1716,10 +1918,12 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
       if (!gJ3[2]) Xk.alloc(np * step);
       for (size_t b0 = 0; b0 < MX; b0 += step) {
         const size_t nb = std::min(step, MX - b0);
+        double* dst = gJ3[2] ? gJ3[2] + np * b0 : Xk.get();
         GemmDesc gd = gemm_nn(LL(np), LL(nb), ns, 0.5 * ns, dmat.get(), LL(np), vb.get() + b0,
-                              LL(MX), 0.0, gJ3[2] ? gJ3[2] + np * b0 : Xk.get(), LL(np));
+                              LL(MX), 0.0, dst, LL(np));
         gd.b_ncontig = true;
         gemm(gd);
+        add_ss_wv(b0, nb, dst);
         if (!gJ3[2]) s3x(b0, nb, Xk.get(), np, st);
       }
     }
@@ -1738,6 +1942,18 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
                             gJ2[2], LL(MX));
       gd.b_ncontig = true;
       gemm(gd);
+      if (same_spin) {
+        // += -Q A_WV Q^T (A_WV symmetric), Q = P2 L
+        DevBuf Q(MX * MX), QA(MX * MX);
+        scale_rc(WV.P2.get(), LL(MX), LL(MX), LL(MX), nullptr, WV.lam.get(), 1.0, Q.get(),
+                 LL(MX));
+        gemm(gemm_nn(LL(MX), LL(MX), LL(MX), 1.0, Q.get(), LL(MX), ssAX.get(), LL(MX), 0.0,
+                     QA.get(), LL(MX)));
+        GemmDesc gq = gemm_nn(LL(MX), LL(MX), LL(MX), -1.0, QA.get(), LL(MX), Q.get(), LL(MX),
+                              1.0, gJ2[2], LL(MX));
+        gq.b_ncontig = true;
+        gemm(gq);
+      }
     }
   }
 

@@ -104,15 +104,16 @@ struct FockRequest {
 
 void form_fock(const FockRequest& rq);
 
-// Reverse mode of the direct terms (form_fock with indirect_term = false):
-// the gradient of their energy with respect to the stored integrals.  Any
+// Reverse mode of form_fock: the gradient of its energy (the direct terms, and
+// with rq.indirect the same-spin terms too) with respect to the stored
+// integrals.  Any
 // pointer may be null (that gradient is skipped); device or host memory per
 // device_mem.  Layouts are those of the inputs: dJ3 packed
 // n_ao(n_ao+1)/2 x n_df (both triangle halves of (mn|P) summed into the packed
 // entry), dJ3_ri (n_ri n_ao) x n_df, dJ2 n_df x n_df symmetric.  The metric
 // gradient is -J2^-1 G J2^-1 (no eigenvector derivatives), exact when no metric
 // eigenvalue falls below the pseudo-inverse cut-off (1e-10).  The energy and
-// Fock of rq (direct terms) are computed first.
+// Fock of rq are computed first.
 // A consumer of a three-index gradient in aux blocks: columns [first, first +
 // count) as a device block (leading dimension ld) on `stream`; the block may be
 // overwritten by later work on that stream once the call returns.

@@ -268,7 +268,7 @@ __global__ void k_lincomb(double* Y, long long m, long long n, int nt, LincombAr
 // out[i(i+1)/2 + j, a] = G[i, j, a] + G[j, i, a] (j < i), G[i, i, a] (j = i):
 // the gradient of a function of sq(x) with respect to the packed x.
 __global__ void k_pack_sym_sum(const double* __restrict__ G, long long n, long long na,
-                               double* out, long long ldo) {
+                               double* out, long long ldo, double beta) {
   const long long np = n * (n + 1) / 2;
   const long long total = np * na;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
@@ -280,7 +280,44 @@ __global__ void k_pack_sym_sum(const double* __restrict__ G, long long n, long l
     while ((i + 1) * (i + 2) / 2 <= p) ++i;
     const long long j = p - i * (i + 1) / 2;
     const double* g = G + n * n * a;
-    out[p + ldo * a] = (i == j) ? g[i + n * i] : g[i + n * j] + g[j + n * i];
+    const double v = (i == j) ? g[i + n * i] : g[i + n * j] + g[j + n * i];
+    double* o = out + p + ldo * a;
+    *o = beta != 0.0 ? beta * *o + v : v;
+  }
+}
+
+// out[p + rp*i + rp*a*(j + a*kk)] = alpha * Z[p + rp*j + rp*a*(i + a*kk)]:
+// the two active-orbital indices of the same-spin three-electron products
+// exchanged (the permutation under which YW and ZV are contracted).
+__global__ void k_perm_3el(const double* __restrict__ Z, double* __restrict__ out,
+                           long long rp, long long a, long long kc, double alpha) {
+  const long long total = rp * a * a * kc;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long p = idx % rp;
+    long long t = idx / rp;
+    const long long i = t % a;
+    t /= a;
+    const long long j = t % a;
+    const long long kk = t / a;
+    out[idx] = alpha * Z[p + rp * (j + a * (i + a * kk))];
+  }
+}
+
+// out[i + a*l + ao*(j + a*k)] = alpha * V[i + a*k + ao*(j + a*l)], ao = a*o:
+// the occupied indices of rows and columns of (ik|jl) exchanged.
+__global__ void k_perm_4el(const double* __restrict__ V, double* __restrict__ out,
+                           long long a, long long o, double alpha) {
+  const long long ao = a * o, total = ao * ao;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long i = idx % a;
+    long long t = idx / a;
+    const long long l = t % o;
+    t /= o;
+    const long long j = t % a;
+    const long long k = t / a;
+    out[idx] = alpha * V[i + a * k + ao * (j + a * l)];
   }
 }
 
@@ -448,10 +485,26 @@ void lincomb(double* Y, long long m, long long n, int nt, const double* const* m
   UW12_LAUNCHED();
 }
 
-void pack_sym_sum(const double* G, long long n, long long na, double* out, long long ldo) {
+void pack_sym_sum(const double* G, long long n, long long na, double* out, long long ldo,
+                  double beta) {
   const long long total = n * (n + 1) / 2 * na;
   if (total <= 0) return;
-  k_pack_sym_sum<<<grid_for(total), kT, 0, current_stream()>>>(G, n, na, out, ldo);
+  k_pack_sym_sum<<<grid_for(total), kT, 0, current_stream()>>>(G, n, na, out, ldo, beta);
+  UW12_LAUNCHED();
+}
+
+void perm_3el(const double* Z, double* out, long long rp, long long a, long long kc,
+              double alpha) {
+  const long long total = rp * a * a * kc;
+  if (total <= 0) return;
+  k_perm_3el<<<grid_for(total), kT, 0, current_stream()>>>(Z, out, rp, a, kc, alpha);
+  UW12_LAUNCHED();
+}
+
+void perm_4el(const double* V, double* out, long long a, long long o, double alpha) {
+  const long long total = a * o * a * o;
+  if (total <= 0) return;
+  k_perm_4el<<<grid_for(total), kT, 0, current_stream()>>>(V, out, a, o, alpha);
   UW12_LAUNCHED();
 }
 

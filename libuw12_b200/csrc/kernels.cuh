@@ -71,9 +71,21 @@ constexpr int kMaxLincomb = 8;
 void lincomb(double* Y, long long m, long long n, int nt, const double* const* mats,
              const double* coefs, const int* scaled, const double* r, const double* c);
 // Gradient with respect to packed symmetric storage: out[:, a] (ldo >= n(n+1)/2)
-// from the n x n matrices G[:, :, a] (consecutive, n*n apart), G_ij + G_ji off
-// the diagonal.
-void pack_sym_sum(const double* G, long long n, long long na, double* out, long long ldo);
+// = beta * out[:, a] + the packed sum of the n x n matrix G[:, :, a]
+// (consecutive, n*n apart), G_ij + G_ji off the diagonal, G_ii on it.
+void pack_sym_sum(const double* G, long long n, long long na, double* out, long long ldo,
+                  double beta = 0.0);
+
+// out[p + rp*i + rp*a*(j + a*k)] = alpha * Z[p + rp*j + rp*a*(i + a*k)] for
+// p < rp, i, j < a, k < kc: the active-orbital pair of a same-spin
+// three-electron product (YW or ZV, rp*a x a*kc) exchanged; out and Z distinct.
+void perm_3el(const double* Z, double* out, long long rp, long long a, long long kc,
+              double alpha);
+
+// out[i + a*l + ao*(j + a*k)] = alpha * V[i + a*k + ao*(j + a*l)], ao = a*o:
+// the occupied indices of an (ik|jl) matrix (ao x ao) exchanged between rows
+// and columns; out and V distinct.
+void perm_4el(const double* V, double* out, long long a, long long o, double alpha);
 
 // A = I (n x n, column-major).
 void set_identity(double* A, long long n);

@@ -9,7 +9,11 @@
 # symbols prefixed "scipy_"). libuw12's CMake-generated config.hpp
 # (src/config.hpp.in: LINALG_KEY, PARALLEL_KEY, source_dir) is written here
 # with USE_ARMA and USE_OMP, the reference's OpenMP build.
-# Output: oracle/_ref/libuw12_ref.so (git-ignored).
+# Outputs (git-ignored):
+#   oracle/_ref/libuw12_ref.so         parity build, libuw12's own parallel.hpp
+#   oracle/_ref/libuw12_ref_timing.so  timing build: the same sources with the
+#       loop dispatcher oracle/refshim/timing/utils/parallel.hpp first on the
+#       include path (full or sampled loops, for the CPU baseline)
 
 REF ?= /root/reference
 HERE := $(patsubst %/,%,$(dir $(abspath $(lastword $(MAKEFILE_LIST)))))
@@ -30,10 +34,13 @@ SRCS := $(REF)/src/integrals/base_integrals.cpp \
         $(REF)/src/uw12.cpp \
         $(REF)/libuw12.cpp
 OBJS := $(patsubst $(REF)/%.cpp,$(OUT)/obj/%.o,$(SRCS)) $(OUT)/obj/ref_capi.o
+TOBJS := $(patsubst $(REF)/%.cpp,$(OUT)/tobj/%.o,$(SRCS)) $(OUT)/tobj/ref_capi.o
 
 CXXFLAGS := -std=c++17 -O3 -DNDEBUG -fPIC -fopenmp -w \
             -DUW12REF_BLAS_PREFIX=scipy_ \
             -I$(HERE)/refshim -I$(OUT)/gen -I$(REF)/src -I$(REF)
+
+all: $(OUT)/libuw12_ref.so $(OUT)/libuw12_ref_timing.so
 
 $(OUT)/libuw12_ref.so: $(OBJS)
 	@test -n "$(BLAS_LIB)" || (echo "scipy's OpenBLAS not found under $(BLAS_DIR)" && false)
@@ -51,6 +58,18 @@ $(OUT)/obj/ref_capi.o: $(HERE)/refshim/ref_capi.cpp $(OUT)/gen/config.hpp $(HERE
 	@mkdir -p $(dir $@)
 	$(REFCXX) $(CXXFLAGS) -c $< -o $@
 
-.PHONY: clean
+$(OUT)/libuw12_ref_timing.so: $(TOBJS)
+	@test -n "$(BLAS_LIB)" || (echo "scipy's OpenBLAS not found under $(BLAS_DIR)" && false)
+	$(REFCXX) -shared -fopenmp -o $@ $(TOBJS) $(BLAS_LIB) -Wl,-rpath,$(BLAS_DIR)
+
+$(OUT)/tobj/%.o: $(REF)/%.cpp $(OUT)/gen/config.hpp $(HERE)/refshim/armadillo $(HERE)/refshim/timing/utils/parallel.hpp
+	@mkdir -p $(dir $@)
+	$(REFCXX) -I$(HERE)/refshim/timing -DUW12REF_TIMING_BUILD $(CXXFLAGS) -c $< -o $@
+
+$(OUT)/tobj/ref_capi.o: $(HERE)/refshim/ref_capi.cpp $(OUT)/gen/config.hpp $(HERE)/refshim/armadillo $(HERE)/refshim/timing/utils/parallel.hpp
+	@mkdir -p $(dir $@)
+	$(REFCXX) -I$(HERE)/refshim/timing -DUW12REF_TIMING_BUILD $(CXXFLAGS) -c $< -o $@
+
+.PHONY: all clean
 clean:
 	rm -rf $(OUT)

@@ -20,9 +20,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libuw12_ref.so")
+TIMING_LIB_PATH = os.path.join(HERE, "_ref", "libuw12_ref_timing.so")
 REFERENCE_TREE = os.environ.get("UW12_REFERENCE_TREE", "/root/reference")
 
-_lib = None
+_libs = {}
 _dp = C.POINTER(C.c_double)
 _sp = C.POINTER(C.c_size_t)
 
@@ -40,7 +41,7 @@ def build(quiet: bool = True) -> bool:
     library exists afterwards."""
     if os.path.isdir(REFERENCE_TREE):
         out = subprocess.run(
-            ["make", "-f", os.path.join(HERE, "ref.mk"), f"REF={REFERENCE_TREE}", "-j8"],
+            ["make", "-f", os.path.join(HERE, "ref.mk"), f"REF={REFERENCE_TREE}", "-j8", "all"],
             capture_output=True, text=True)
         if out.returncode != 0:
             raise RuntimeError("reference build failed:\n" + out.stdout[-2000:] + out.stderr[-4000:])
@@ -49,16 +50,18 @@ def build(quiet: bool = True) -> bool:
     return os.path.exists(LIB_PATH)
 
 
-def available() -> bool:
-    return os.path.exists(LIB_PATH)
+def available(timing: bool = False) -> bool:
+    return os.path.exists(TIMING_LIB_PATH if timing else LIB_PATH)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            raise FileNotFoundError(f"{LIB_PATH} is not built (make -f oracle/ref.mk)")
-        L = C.CDLL(LIB_PATH)
+def lib(timing: bool = False):
+    """The parity build (libuw12's own loop dispatcher) or, with ``timing``,
+    the timing build (same sources, loops run in full or sampled)."""
+    path = TIMING_LIB_PATH if timing else LIB_PATH
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built (make -f oracle/ref.mk)")
+        L = C.CDLL(path)
         L.uw12ref_last_error.argtypes = [C.c_char_p, C.c_size_t]
         L.uw12ref_set_threads.argtypes = [C.c_int, C.c_int]
         L.uw12ref_max_threads.restype = C.c_int
@@ -67,15 +70,18 @@ def lib():
         L.uw12ref_evaluate.argtypes = [C.c_void_p, _dp, C.c_size_t, C.c_size_t, _dp, _sp, _sp,
                                        C.c_size_t, C.c_double, C.c_double, _dp, _dp, _dp, _dp]
         L.uw12ref_abs_blocks.argtypes = [_dp, C.c_size_t, C.c_size_t, _dp, _dp, _dp, _dp, _sp]
-        _lib = L
-    return _lib
+        if timing:
+            L.uw12ref_timing_set.argtypes = [C.c_int]
+            L.uw12ref_timing_read.argtypes = [_dp, C.POINTER(C.c_long), C.POINTER(C.c_long)]
+        _libs[path] = L
+    return _libs[path]
 
 
-def _check(status: int):
+def _check(status: int, timing: bool = False):
     if status == 0:
         return
     buf = C.create_string_buffer(4096)
-    lib().uw12ref_last_error(buf, 4096)
+    lib(timing).uw12ref_last_error(buf, 4096)
     msg = buf.value.decode()
     if status == 1:
         raise RefRuntimeError(msg)
@@ -96,37 +102,40 @@ def _f64(a: Optional[np.ndarray]) -> Optional[np.ndarray]:
     return np.asfortranarray(np.asarray(a, dtype=np.float64))
 
 
-def set_threads(omp_threads: int, blas_threads: int = 1) -> None:
-    lib().uw12ref_set_threads(int(omp_threads), int(blas_threads))
+def set_threads(omp_threads: int, blas_threads: int = 1, timing: bool = False) -> None:
+    lib(timing).uw12ref_set_threads(int(omp_threads), int(blas_threads))
 
 
-def max_threads() -> int:
-    return int(lib().uw12ref_max_threads())
+def max_threads(timing: bool = False) -> int:
+    return int(lib(timing).uw12ref_max_threads())
 
 
 class RefProblem:
     """libuw12's ``BaseIntegrals`` W, V, WV and ``ABSProjectors`` built by its own
     setup calls (deep copies; the arrays may be dropped afterwards)."""
 
-    def __init__(self, W3, W2, W3_ri, V3, V2, V3_ri, WV3, WV2, S, n_ao, n_df, n_ri):
+    def __init__(self, W3, W2, W3_ri, V3, V2, V3_ri, WV3, WV2, S, n_ao, n_df, n_ri,
+                 timing: bool = False):
+        self.timing = timing
+        self._L = lib(timing)
         arrs = [_f64(x) for x in (W3, W2, W3_ri, V3, V2, V3_ri, WV3, WV2, S)]
         h = C.c_void_p()
         t = C.c_double(0.0)
-        _check(lib().uw12ref_create(*[_ptr(a) for a in arrs], n_ao, n_df, n_ri, C.byref(h),
-                                    C.byref(t)))
+        _check(self._L.uw12ref_create(*[_ptr(a) for a in arrs], n_ao, n_df, n_ri, C.byref(h),
+                                      C.byref(t)), timing)
         self._h = h
         self.n_ao = n_ao
         self.setup_seconds = t.value
 
     @classmethod
-    def from_inputs(cls, inp):
+    def from_inputs(cls, inp, timing: bool = False):
         cfg = inp.cfg
         return cls(inp.W3, inp.W2, inp.W3_ri, inp.V3, inp.V2, inp.V3_ri, inp.WV3, inp.WV2,
-                   inp.S, cfg.n_ao, cfg.n_df, cfg.n_ri)
+                   inp.S, cfg.n_ao, cfg.n_df, cfg.n_ri, timing=timing)
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
-            lib().uw12ref_destroy(self._h)
+            self._L.uw12ref_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):
@@ -148,10 +157,24 @@ class RefProblem:
         T = np.zeros(3) if terms else None
         e = C.c_double(0.0)
         sec = C.c_double(0.0)
-        _check(lib().uw12ref_evaluate(self._h, _ptr(Cm), n_orb, n_spin, _ptr(occ), no, na,
-                                      len(n_active), float(s_os), float(s_ss), _ptr(F),
-                                      C.byref(e), _ptr(T), C.byref(sec)))
+        _check(self._L.uw12ref_evaluate(self._h, _ptr(Cm), n_orb, n_spin, _ptr(occ), no, na,
+                                        len(n_active), float(s_os), float(s_ss), _ptr(F),
+                                        C.byref(e), _ptr(T), C.byref(sec)), self.timing)
         return e.value, F, T, sec.value
+
+    def timed_evaluate(self, rounds: int, *args, **kw):
+        """Timing build only: one evaluation with every top-level loop sampled
+        at ``rounds`` iterations per thread (0 = every iteration). Returns
+        (estimated seconds, measured seconds, sampled loops, full loops)."""
+        if not self.timing:
+            raise ValueError("timed_evaluate needs the timing build")
+        self._L.uw12ref_timing_set(int(rounds))
+        _, _, _, sec = self.evaluate(*args, **kw)
+        extra = C.c_double(0.0)
+        ns, nf = C.c_long(0), C.c_long(0)
+        self._L.uw12ref_timing_read(C.byref(extra), C.byref(ns), C.byref(nf))
+        self._L.uw12ref_timing_set(0)
+        return sec + extra.value, sec, int(ns.value), int(nf.value)
 
 
 def abs_blocks(S: np.ndarray, n_ao: int, n_ri: int):

@@ -14,6 +14,8 @@
 //                              as uw12::form_fock (src/uw12.cpp:22-119)
 //   * uw12ref_abs_blocks    -> three_el::ri::calculate_abs_projectors
 //                              (src/three_electron/ri_utils.hpp:45-74)
+//   * uw12ref_timing_*      (timing build only) the loop dispatcher's mode and
+//                              the extrapolated time of skipped iterations
 // Errors: status 1 = std::runtime_error, 2 = std::logic_error, 3 = other; the
 // message is kept per thread for uw12ref_last_error.
 #include <omp.h>
@@ -26,6 +28,7 @@
 #include <vector>
 
 #include "four_electron/four_electron.hpp"
+#include "utils/parallel.hpp"
 #include "integrals/base_integrals.hpp"
 #include "integrals/integrals.hpp"
 #include "libuw12.hpp"
@@ -207,5 +210,24 @@ int uw12ref_abs_blocks(const double* S, size_t n_ao, size_t n_ri,
     }
   });
 }
+
+#ifdef UW12REF_TIMING_BUILD
+// Sampled loops (rounds > 0) or every iteration (0); resets the counters.
+void uw12ref_timing_set(int rounds) {
+  uw12ref_timing::sample_rounds = rounds;
+  uw12ref_timing::extra_seconds = 0.0;
+  uw12ref_timing::sampled_loops = 0;
+  uw12ref_timing::full_loops = 0;
+}
+
+// Extrapolated seconds of the iterations skipped since the last set, and the
+// numbers of sampled and fully run top-level loops.
+void uw12ref_timing_read(double* extra_seconds, long* sampled_loops,
+                         long* full_loops) {
+  *extra_seconds = uw12ref_timing::extra_seconds;
+  *sampled_loops = uw12ref_timing::sampled_loops;
+  *full_loops = uw12ref_timing::full_loops;
+}
+#endif
 
 }  // extern "C"

@@ -1,0 +1,182 @@
+// Loop dispatcher of the TIMING build of the libuw12 reference -- TEST
+// INFRASTRUCTURE ONLY (the CPU baseline of bench.py).
+//
+// oracle/ref.mk compiles libuw12's unmodified sources twice. The parity build
+// (libuw12_ref.so) uses the reference's own src/utils/parallel.hpp. The timing
+// build (libuw12_ref_timing.so) puts this directory first on the include path,
+// so that src/integrals/{integral_functions,transformations}.hpp, the only
+// files that include "utils/parallel.hpp", get this dispatcher instead. It has
+// the interface of the reference's parallel.hpp:31-183 (parallel_for,
+// parallel_sum, parallel_sum_2d, isolate) and two modes:
+//
+//   * full (sample_rounds == 0): every iteration runs, OpenMP-parallel at the
+//     top level and serially inside an active parallel region, as in the
+//     reference's OpenMP build;
+//   * sampled (sample_rounds = r > 0): a top-level loop with more than r x T
+//     iterations (T = OpenMP threads) runs r x T evenly spaced iterations,
+//     r per thread, all threads at once, and adds the extrapolated time of the
+//     rest to extra_seconds. The reference's OpenMP schedule gives each thread
+//     a contiguous block of ceil(n / T) iterations (two-index loops: ceil(n1 /
+//     T) outer iterations of n2 inner ones each), so the whole loop takes
+//     ceil(n / T) (resp. ceil(n1 / T) * n2) iteration times with every thread
+//     busy; the sample measures r such iteration times under the same memory
+//     contention. Loop results are then partial sums; only the time is used.
+//
+// The sampled estimate is checked against full evaluations of the parity
+// build (bench.py --validate-reference-sampler).
+#ifndef UW12_PARALLEL_HPP
+#define UW12_PARALLEL_HPP
+
+#include <omp.h>
+
+#include <functional>
+#include <vector>
+
+namespace uw12ref_timing {
+inline int sample_rounds = 0;       // 0: every iteration runs
+inline double extra_seconds = 0.0;  // extrapolated time of skipped iterations
+inline long sampled_loops = 0;      // top-level loops that were sampled
+inline long full_loops = 0;         // top-level loops that ran every iteration
+
+inline size_t ceil_div(size_t a, size_t b) { return (a + b - 1) / b; }
+
+inline bool sampling_applies(size_t n, bool parallel) {
+  return sample_rounds > 0 && parallel && !omp_in_parallel() &&
+         n > static_cast<size_t>(sample_rounds) *
+                 static_cast<size_t>(omp_get_max_threads());
+}
+
+// k evenly spaced indices of [0, n).
+inline std::vector<size_t> spaced(size_t n, size_t k) {
+  std::vector<size_t> idx(k);
+  for (size_t t = 0; t < k; ++t)
+    idx[t] = static_cast<size_t>((static_cast<double>(t) + 0.5) *
+                                 static_cast<double>(n) /
+                                 static_cast<double>(k));
+  return idx;
+}
+
+// Runs body(slot, item) for every sampled item, r per thread, and books the
+// extrapolated remainder: the full loop takes `rounds_full` iteration times,
+// the sample took r of them.
+template <typename Body>
+void run_sample(const std::vector<size_t>& items, size_t r, double rounds_full,
+                Body&& body) {
+  const double t0 = omp_get_wtime();
+#pragma omp parallel for schedule(static, 1)
+  for (long q = 0; q < static_cast<long>(items.size()); ++q)
+    body(static_cast<size_t>(q), items[static_cast<size_t>(q)]);
+  const double dt = omp_get_wtime() - t0;
+  extra_seconds += dt * (rounds_full / static_cast<double>(r) - 1.0);
+  ++sampled_loops;
+}
+}  // namespace uw12ref_timing
+
+namespace uw12::parallel {
+
+inline void parallel_for(size_t start, size_t stop,
+                         const std::function<void(size_t)>& func,
+                         bool parallel = true) {
+  namespace ts = uw12ref_timing;
+  const size_t n = stop > start ? stop - start : 0;
+  if (ts::sampling_applies(n, parallel)) {
+    const size_t T = static_cast<size_t>(omp_get_max_threads());
+    const size_t r = static_cast<size_t>(ts::sample_rounds);
+    ts::run_sample(ts::spaced(n, r * T), r,
+                   static_cast<double>(ts::ceil_div(n, T)),
+                   [&](size_t, size_t i) { func(start + i); });
+    return;
+  }
+  if (!omp_in_parallel()) ++ts::full_loops;
+  if (parallel) {
+#pragma omp parallel for
+    for (long i = static_cast<long>(start); i < static_cast<long>(stop); ++i)
+      func(static_cast<size_t>(i));
+  } else {
+    for (size_t i = start; i < stop; ++i) func(i);
+  }
+}
+
+// Sum over every iteration with one partial result per thread, added up at
+// the end (the reference's OpenMP reduction).
+template <typename ReturnType, typename Fn>
+ReturnType full_sum(size_t start, size_t stop, const ReturnType& identity,
+                    const Fn& func, bool parallel) {
+  if (!parallel) {
+    ReturnType result(identity);
+    for (size_t i = start; i < stop; ++i) result += func(i);
+    return result;
+  }
+  std::vector<ReturnType> part;
+#pragma omp parallel
+  {
+#pragma omp single
+    part.assign(static_cast<size_t>(omp_get_num_threads()), identity);
+    ReturnType& mine = part[static_cast<size_t>(omp_get_thread_num())];
+#pragma omp for
+    for (long i = static_cast<long>(start); i < static_cast<long>(stop); ++i)
+      mine += func(static_cast<size_t>(i));
+  }
+  ReturnType result(identity);
+  for (auto& p : part) result += p;
+  return result;
+}
+
+template <typename ReturnType>
+ReturnType parallel_sum(const size_t start, const size_t stop,
+                        const ReturnType& identity,
+                        const std::function<ReturnType(size_t)>& func,
+                        const bool parallel = true) {
+  namespace ts = uw12ref_timing;
+  const size_t n = stop > start ? stop - start : 0;
+  if (ts::sampling_applies(n, parallel)) {
+    const size_t T = static_cast<size_t>(omp_get_max_threads());
+    const size_t r = static_cast<size_t>(ts::sample_rounds);
+    const auto items = ts::spaced(n, r * T);
+    std::vector<ReturnType> part(items.size(), identity);
+    ts::run_sample(items, r, static_cast<double>(ts::ceil_div(n, T)),
+                   [&](size_t q, size_t i) { part[q] += func(start + i); });
+    return part[0];
+  }
+  if (!omp_in_parallel()) ++ts::full_loops;
+  return full_sum(start, stop, identity, func, parallel);
+}
+
+template <typename ReturnType>
+ReturnType parallel_sum_2d(
+    const size_t start1, const size_t stop1, const size_t start2,
+    const size_t stop2, const ReturnType& identity,
+    const std::function<ReturnType(size_t, size_t)>& func,
+    const bool parallel = true) {
+  namespace ts = uw12ref_timing;
+  const size_t n1 = stop1 > start1 ? stop1 - start1 : 0;
+  const size_t n2 = stop2 > start2 ? stop2 - start2 : 0;
+  if (ts::sampling_applies(n1 * n2, parallel)) {
+    const size_t T = static_cast<size_t>(omp_get_max_threads());
+    const size_t r = static_cast<size_t>(ts::sample_rounds);
+    const auto items = ts::spaced(n1 * n2, r * T);
+    std::vector<ReturnType> part(items.size(), identity);
+    ts::run_sample(items, r, static_cast<double>(ts::ceil_div(n1, T) * n2),
+                   [&](size_t q, size_t p) {
+                     part[q] += func(start1 + p / n2, start2 + p % n2);
+                   });
+    return part[0];
+  }
+  if (!omp_in_parallel()) ++ts::full_loops;
+  // outer iterations in parallel, the inner loop serial within each
+  const auto outer = [&](size_t i) -> ReturnType {
+    ReturnType result(identity);
+    for (size_t j = start2; j < stop2; ++j) result += func(i, j);
+    return result;
+  };
+  return full_sum(start1, stop1, identity, outer, parallel);
+}
+
+template <typename Func>
+void isolate(Func&& func) {
+  func();
+}
+
+}  // namespace uw12::parallel
+
+#endif  // UW12_PARALLEL_HPP

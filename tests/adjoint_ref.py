@@ -224,3 +224,149 @@ def chunked_three_index_adjoint(Wb, Vb, abs_p, orbitals, occ, n_active, s_os, s_
         out["W3" if which == 0 else "V3"] = g3
         out["W3_ri" if which == 0 else "V3_ri"] = g3ri
     return out
+
+
+def full_energy(W, V, WV, abs_p, orbitals, occ, n_active, s_os, s_ss):
+    """Energy with the same-spin (indirect) terms, as uw12_energy with s_ss != 0."""
+    return O.form_fock(W, V, WV, abs_p, orbitals, occ, n_active, True, False, s_os,
+                       s_ss).energy
+
+
+def perm_3el(Z, Rp, a, o):
+    """P3(Z)[p + Rp i, j + a k] = Z[p + Rp j, i + a k] for Z of shape (Rp a) x (a o)."""
+    T = Z.reshape((Rp, a, a, o), order="F")         # (p, row-orbital, col-orbital, k)
+    return np.transpose(T, (0, 2, 1, 3)).reshape((Rp * a, a * o), order="F")
+
+
+def perm_4el(Vm, a, o):
+    """P4(V)[i + a l, j + a k] = V[i + a k, j + a l] for V of shape (a o) x (a o)."""
+    T = Vm.reshape((a, o, a, o), order="F")          # (i, k_row, j, l_col)
+    return np.transpose(T, (0, 3, 2, 1)).reshape((a * o, a * o), order="F")
+
+
+def indirect_adjoint(Wb, Vb, WVb, abs_p, orbitals, occ, n_active):
+    """Gradients of the same-spin energy E_ss with respect to every stored
+    integral; uw12_energy's energy is E_direct(s_os, s_ss) + s_ss E_ss, so the
+    full gradient is direct_adjoint(...) + s_ss * indirect_adjoint(...).
+
+    With esf = 2 (closed shell) or 1, per spin, all in the metric eigenbasis:
+      E2- = -1/2 esf <B2_WV L_WV, B2_WV>              (two_electron.cpp:87-132;
+            B2_WV of the active orbitals only)
+      E4- = -1/2 esf <W4, P4(V4)>, W4 = B2_W L_W B2_W^T, V4 likewise
+                                                      (four_electron.cpp:143-179)
+      E3- = esf <YW, P3(ZV)>, YW = Wst_W L_W B2_W^T, ZV = SV_V L_V B2_V^T
+            (SV = (I (x) S^-1) Wst)                   (indirect_utils.cpp:101-133)
+    Reverse sweep: G_Y = esf P3(ZV), G_Z = esf P3(YW); Wst_W-bar = G_Y B2_W L_W,
+    B2_W-bar = G_Y^T Wst_W L_W, SV_V-bar = G_Z B2_V L_V -> Wst_V-bar = (I (x) S^-1)
+    SV_V-bar, B2_V-bar = G_Z^T SV_V L_V; G_W4 = -1/2 esf P4(V4): B2_W-bar +=
+    2 G_W4 B2_W L_W (and W <-> V); B2_WV-bar = -esf B2_WV L_WV; the transforms
+    are then reversed as in direct_adjoint.  Metric: each L between eigenbasis
+    factors contributes A += (left factor)^T G (right factor) to
+    dE/dJ2 = -sym(Q A Q^T), Q = P2 L."""
+    ns = len(orbitals)
+    esf = 2.0 if ns == 1 else 1.0
+    Co = O.occupation_weighted_orbitals(orbitals, occ)
+    Ca = O.freeze_core(Co, n_active)
+    W = O.Integrals(Wb, Co, Ca)
+    V = O.Integrals(Vb, Co, Ca)
+    WVa = O.Integrals(WVb, Ca, Ca)
+    N = Co[0].shape[0]
+    R = abs_p.s_inv_ri_ri.shape[0]
+    Rp = N + R
+    Sinv = np.block([[abs_p.s_inv_ao_ao, abs_p.s_inv_ao_ri], [abs_p.s_inv_ri_ao, abs_p.s_inv_ri_ri]])
+    lw, lv, lx = W.df_vals, V.df_vals, WVa.df_vals
+
+    def stacked(X, s):
+        B1 = X.get_X3idx_one_trans()[s]
+        Bri = X.get_X3idx_one_trans_ri()[s]
+        o, a = Co[s].shape[1], Ca[s].shape[1]
+        c = o - a
+        out = np.zeros((Rp * a, B1.shape[1]))
+        for j in range(a):
+            out[Rp * j:Rp * j + N] = B1[N * (c + j):N * (c + j + 1)]
+            out[Rp * j + N:Rp * (j + 1)] = Bri[R * j:R * (j + 1)]
+        return out
+
+    def unstack(Wsb, s, M):
+        """Wst-bar rows back to (B1-bar rows of the active orbitals, Bri-bar)."""
+        o, a = Co[s].shape[1], Ca[s].shape[1]
+        c = o - a
+        b1 = np.zeros((N * o, M))
+        br = np.zeros((R * a, M))
+        for j in range(a):
+            b1[N * (c + j):N * (c + j + 1)] = Wsb[Rp * j:Rp * j + N]
+            br[R * j:R * (j + 1)] = Wsb[Rp * j + N:Rp * (j + 1)]
+        return b1, br
+
+    def reverse(Xi, b1bar, brbar, C_occ, C_act, g3, g3ri):
+        """B1-bar (N o x M, orbitals C_occ) and Bri-bar (R a x M) to dE/dJ3_0, dE/dJ3_ri_0."""
+        P2 = Xi.P2
+        M = P2.shape[0]
+        o = C_occ.shape[1]
+        b10 = b1bar @ P2.T
+        for A in range(M):
+            G = b10[:, A].reshape((N, o), order="F") @ C_occ.T
+            g3[:, A] += _pack_sym_sum(G)
+        if brbar is not None and g3ri is not None:
+            br0 = brbar @ P2.T
+            a = C_act.shape[1]
+            for A in range(M):
+                g3ri[:, A] += (br0[:, A].reshape((R, a), order="F") @ C_act.T).reshape(-1, order="F")
+
+    MW, MV, MX = lw.size, lv.size, lx.size
+    out = {"W3": np.zeros((N * (N + 1) // 2, MW)), "W3_ri": np.zeros((R * N, MW)),
+           "V3": np.zeros((N * (N + 1) // 2, MV)), "V3_ri": np.zeros((R * N, MV)),
+           "WV3": np.zeros((N * (N + 1) // 2, MX))}
+    AW = np.zeros((MW, MW))
+    AV = np.zeros((MV, MV))
+    AX = np.zeros((MX, MX))
+    for s in range(ns):
+        o, a = Co[s].shape[1], Ca[s].shape[1]
+        if a == 0 or o == 0:
+            continue
+        B2W = W.get_X3idx_two_trans()[s]
+        B2V = V.get_X3idx_two_trans()[s]
+        WstW = stacked(W, s)
+        SVV = np.kron(np.eye(a), Sinv) @ stacked(V, s)
+        # three-electron
+        YW = (WstW * lw[None, :]) @ B2W.T
+        ZV = (SVV * lv[None, :]) @ B2V.T
+        GY = esf * perm_3el(ZV, Rp, a, o)
+        GZ = esf * perm_3el(YW, Rp, a, o)
+        TY = GY @ B2W
+        TZ = GZ @ B2V
+        WsbW = TY * lw[None, :]
+        WsbV = np.kron(np.eye(a), Sinv) @ (TZ * lv[None, :])
+        B2bW = GY.T @ (WstW * lw[None, :])
+        B2bV = GZ.T @ (SVV * lv[None, :])
+        AW += WstW.T @ TY
+        AV += SVV.T @ TZ
+        # four-electron
+        W4 = (B2W * lw[None, :]) @ B2W.T
+        V4 = (B2V * lv[None, :]) @ B2V.T
+        GW4 = -0.5 * esf * perm_4el(V4, a, o)
+        GV4 = -0.5 * esf * perm_4el(W4, a, o)
+        B2bW += 2.0 * (GW4 @ B2W) * lw[None, :]
+        B2bV += 2.0 * (GV4 @ B2V) * lv[None, :]
+        AW += B2W.T @ GW4 @ B2W
+        AV += B2V.T @ GV4 @ B2V
+        # back through the transforms of W and V
+        for Xi, B2b, Wsb, M, g3, g3ri in ((W, B2bW, WsbW, MW, out["W3"], out["W3_ri"]),
+                                          (V, B2bV, WsbV, MV, out["V3"], out["V3_ri"])):
+            b1, br = unstack(Wsb, s, M)
+            b1 += (Ca[s] @ B2b.reshape((a, o * M), order="F")).reshape((N * o, M), order="F")
+            reverse(Xi, b1, br, Co[s], Ca[s], g3, g3ri)
+        # two-electron (WV over the active orbitals)
+        B2X = WVa.get_X3idx_two_trans()[s]
+        B2bX = -esf * B2X * lx[None, :]
+        AX += -0.5 * esf * B2X.T @ B2X
+        b1 = (Ca[s] @ B2bX.reshape((a, a * MX), order="F")).reshape((N * a, MX), order="F")
+        reverse(WVa, b1, None, Ca[s], Ca[s], out["WV3"], None)
+
+    def sym(A):
+        return 0.5 * (A + A.T)
+
+    for key, Xi, lam, A in (("W2", W, lw, AW), ("V2", V, lv, AV), ("WV2", WVa, lx, AX)):
+        Q = Xi.P2 * lam[None, :]
+        out[key] = -sym(Q @ A @ Q.T)
+    return out

@@ -103,3 +103,47 @@ def test_orbital_chunked_three_index_adjoint(name, chunk):
     for key in ("W3", "W3_ri", "V3", "V3_ri"):
         scale = max(np.max(np.abs(ref[key])), 1e-300)
         assert np.max(np.abs(got[key] - ref[key])) <= 1e-12 * scale, key
+
+
+def _full_energy(d, c, ints, s_os, s_ss):
+    W = O.BaseIntegrals(ints["W3"], ints["W2"], ints["W3_ri"])
+    V = O.BaseIntegrals(ints["V3"], ints["V2"], ints["V3_ri"])
+    WV = O.BaseIntegrals(ints["WV3"], ints["WV2"])
+    absp = O.calculate_abs_projectors(d.S, c.n_ao, c.n_ri)
+    return AR.full_energy(W, V, WV, absp, d.orbitals, d.occ, list(c.n_active), s_os, s_ss)
+
+
+@pytest.mark.parametrize("case", CASES + [Case("base_open_frozen", 7, 10, 9, (4, 3), (3, 2),
+                                               "baseline", 21, 4.0)], ids=lambda c: c.name)
+@pytest.mark.parametrize("scales", [(1.0, 0.5), (0.0, 1.0)])
+def test_same_spin_adjoint_matches_finite_differences(case, scales):
+    """dE/d(integrals) of the full energy (same-spin terms included) =
+    direct_adjoint + s_ss indirect_adjoint, against central differences."""
+    s_os, s_ss = scales
+    d = make_case(case)
+    ints = {"W3": d.W3, "W2": d.W2, "W3_ri": d.W3_ri, "V3": d.V3, "V2": d.V2,
+            "V3_ri": d.V3_ri, "WV3": d.WV3, "WV2": d.WV2}
+    W = O.BaseIntegrals(d.W3, d.W2, d.W3_ri)
+    V = O.BaseIntegrals(d.V3, d.V2, d.V3_ri)
+    WV = O.BaseIntegrals(d.WV3, d.WV2)
+    absp = O.calculate_abs_projectors(d.S, case.n_ao, case.n_ri)
+    act = list(case.n_active)
+    gd = AR.direct_adjoint(W, V, WV, absp, d.orbitals, d.occ, act, s_os, s_ss)
+    gi = AR.indirect_adjoint(W, V, WV, absp, d.orbitals, d.occ, act)
+    e0 = _full_energy(d, case, ints, s_os, s_ss)
+    rng = np.random.default_rng(11)
+    for key in ("W3", "W3_ri", "W2", "V3", "V3_ri", "V2", "WV3", "WV2"):
+        base = ints[key]
+        dirn = rng.standard_normal(base.shape)
+        # the baseline metrics have eigenvalues down to ~1e-6: their step must
+        # stay well below that for the central difference to be accurate
+        h = 1e-5 if (case.family == "unit" or not key.endswith("2")) else 1e-9
+        if key.endswith("2"):
+            dirn = 0.5 * (dirn + dirn.T)
+        plus = dict(ints, **{key: base + h * dirn})
+        minus = dict(ints, **{key: base - h * dirn})
+        fd = (_full_energy(d, case, plus, s_os, s_ss) -
+              _full_energy(d, case, minus, s_os, s_ss)) / (2 * h)
+        an = float(np.sum((gd[key] + s_ss * gi[key]) * dirn))
+        scale = max(abs(fd), 1e-3 * max(1.0, abs(e0)))
+        assert abs(an - fd) <= 1e-6 * scale, (key, an, fd)
