@@ -282,7 +282,12 @@ int uw12c_dgemm(long long m, long long n, long long k, double alpha, const doubl
  * scratch).  All calls share the array, so calls that overlap on the GPU
  * race; the partial tiles are fully overwritten by each call, so nothing has
  * to start at zero.  The first call on a device looks up the array's device
- * address (once per device); make that first call before any stream capture. */
+ * address (once per device); make that first call before any stream capture.
+ * With lazy module loading (the CUDA default since 12.2) that first call also
+ * loads the library's device code and the array, which takes device memory:
+ * make it before the host program reserves the heap for its pool.  This entry
+ * point always computes in FP64 (the DMMA kernel): the split-precision mode of
+ * uw12c_set_precision does not apply to it. */
 #define UW12C_NOALLOC_SCRATCH_DOUBLES (1LL << 21)
 int uw12c_dgemm_noalloc(long long m, long long n, long long k, double alpha, const double* A,
                         long long lda, int a_kcontig, const double* B, long long ldb,

@@ -513,7 +513,8 @@ def fock_backward(W: BaseIntegrals, V: BaseIntegrals, WV: BaseIntegrals, abs_p: 
                   orbitals: Sequence[np.ndarray], occupations: Sequence[np.ndarray],
                   n_active: Sequence[int], scale_opp_spin: float, scale_same_spin: float,
                   gradients: Sequence[str] = GRADIENT_NAMES, calculate_fock: bool = True,
-                  device_out: Optional[dict] = None, indirect_term: bool = False):
+                  device_out: Optional[dict] = None, indirect_term: bool = False,
+                  host_out: Optional[dict] = None):
     """Reverse mode of ``form_fock`` (``uw12c_fock_backward``).
 
     Returns ``(energy, fock, (E2, E3, E4), grads)``: the energy, per-spin Fock
@@ -524,7 +525,9 @@ def fock_backward(W: BaseIntegrals, V: BaseIntegrals, WV: BaseIntegrals, abs_p: 
     ("W3", "V3", "WV3" packed n_ao(n_ao+1)/2 x n_df; "W3_ri", "V3_ri"
     (n_ri n_ao) x n_df; "W2", "V2", "WV2" n_df x n_df).  With ``device_out``
     (name -> device pointer) the gradients are written to device memory and
-    the dict is empty.
+    the dict is empty; with ``host_out`` (name -> Fortran-ordered float64 host
+    array of the gradient's shape, e.g. a view of pinned memory) those arrays
+    are filled and returned instead of new ones.
     """
     n_spin = len(orbitals)
     if n_spin < 1 or n_spin > 2 or len(occupations) != n_spin or len(n_active) != n_spin:
@@ -547,6 +550,13 @@ def fock_backward(W: BaseIntegrals, V: BaseIntegrals, WV: BaseIntegrals, abs_p: 
     for name in GRADIENT_NAMES:
         if device_out is not None:
             ptr[name] = P(device_out[name]) if name in device_out else P(0)
+        elif host_out is not None and name in host_out:
+            arr = host_out[name]
+            if (arr.shape != shapes[name] or arr.dtype != np.float64
+                    or not arr.flags.f_contiguous):
+                raise UW12LogicError(f"host_out[{name!r}] must be float64 F-ordered {shapes[name]}")
+            grads[name] = arr
+            ptr[name] = _fptr(arr)
         elif name in gradients:
             grads[name] = np.zeros(shapes[name], order="F")
             ptr[name] = _fptr(grads[name])

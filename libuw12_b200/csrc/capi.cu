@@ -747,7 +747,9 @@ int uw12c_fock_batched(const uw12c_molecule* mols, size_t n, int indirect_term,
   return guarded([&] {
     need(mols != nullptr || n == 0, "null molecule array");
     if (n == 0) return;
-    const size_t workers = std::min(n, n_streams ? n_streams : size_t(8));
+    // at most kOzakiErrorSlots workers: each owns one split-precision error flag
+    const size_t workers = std::min({n, n_streams ? n_streams : size_t(8),
+                                     static_cast<size_t>(uw12b::kOzakiErrorSlots)});
     // largest molecules first, so that the tail of the batch is short
     std::vector<size_t> order(n);
     for (size_t i = 0; i < n; ++i) order[i] = i;
@@ -768,7 +770,8 @@ int uw12c_fock_batched(const uw12c_molecule* mols, size_t n, int indirect_term,
     std::atomic<size_t> next{0};
     std::vector<int> st(n, UW12C_OK);
     std::vector<std::string> msg(n);
-    auto work = [&] {
+    auto work = [&](int slot) {
+      const int prev_slot = uw12b::set_error_slot(slot);
       cudaStream_t stream = nullptr;
       int dev = -1;
       uw12b::set_split_moduli(moduli);
@@ -798,15 +801,16 @@ int uw12c_fock_batched(const uw12c_molecule* mols, size_t n, int indirect_term,
       }
       uw12b::g_stream = nullptr;
       uw12b::g_budget_override = 0;
+      uw12b::set_error_slot(prev_slot);
     };
     std::vector<std::thread> pool;
-    for (size_t w = 1; w < workers; ++w) pool.emplace_back(work);
+    for (size_t w = 1; w < workers; ++w) pool.emplace_back(work, static_cast<int>(w));
     {
       // the calling thread works too; its stream and device are restored afterwards
       const cudaStream_t saved = uw12b::g_stream;
       int saved_dev = 0;
       cudaGetDevice(&saved_dev);
-      work();
+      work(0);
       uw12b::g_stream = saved;
       cudaSetDevice(saved_dev);
     }

@@ -841,8 +841,10 @@ void form_fock(const FockRequest& rq) {
   // orbitals per chunk of the X_AB pass
   // (per occupied orbital: B1 of W and V, the transform's output, Z or the two
   // B2 rows of its a active orbitals)
-  auto per_k = [&](int s) { return (4 * N + 2 * sd[s].a) * MW; };
-  const size_t per_j = (N + R + 3 * Rp) * MW;
+  // (the larger of the two potentials' aux counts sizes every buffer)
+  const size_t Mmax = std::max(MW, MV);
+  auto per_k = [&](int s) { return (4 * N + 2 * sd[s].a) * Mmax; };
+  const size_t per_j = (N + R + 3 * Rp) * Mmax;
   if (orbital_chunked) {
     for (int s = 0; s < ns; ++s) {
       const size_t o = sd[s].o, a = sd[s].a, c = sd[s].c;

@@ -116,19 +116,27 @@ const Consts& consts_for(int L) {
 thread_local int g_split_moduli = 0;
 thread_local double g_split_min_flops = kOzakiMinFlops;
 
-// device error flag (pipeline wait timed out), one per device
+// device error flags (a pipeline wait timed out): kOzakiErrorSlots ints per
+// device; a host thread uses the slot set by set_error_slot (0 by default), so
+// that concurrent evaluations on different threads (uw12c_fock_batched's
+// workers) read and clear only their own flag
+constexpr int kMaxDevices = 64;
 std::mutex g_err_mu;
-int* g_err_ptr[64] = {};
+int* g_err_ptr[kMaxDevices] = {};
+thread_local int t_err_slot = 0;
 
 int* err_flag() {
   int dev = 0;
   UW12_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices)
+    throw Error(kErrInvalid, "split-precision GEMM: device index beyond 63");
   std::lock_guard<std::mutex> lk(g_err_mu);
   if (!g_err_ptr[dev]) {
-    UW12_CUDA(cudaMalloc(reinterpret_cast<void**>(&g_err_ptr[dev]), sizeof(int)));
-    UW12_CUDA(cudaMemset(g_err_ptr[dev], 0, sizeof(int)));
+    UW12_CUDA(cudaMalloc(reinterpret_cast<void**>(&g_err_ptr[dev]),
+                         kOzakiErrorSlots * sizeof(int)));
+    UW12_CUDA(cudaMemset(g_err_ptr[dev], 0, kOzakiErrorSlots * sizeof(int)));
   }
-  return g_err_ptr[dev];
+  return g_err_ptr[dev] + t_err_slot;
 }
 
 // ---------------------------------------------------------------------------
@@ -1336,6 +1344,12 @@ void gemm_ozaki(const GemmDesc& d, int n_moduli) {
            s);
   run_slabs(d, cs, beta, s);
   tm.stop();
+}
+
+int set_error_slot(int slot) {
+  const int prev = t_err_slot;
+  t_err_slot = ((slot % kOzakiErrorSlots) + kOzakiErrorSlots) % kOzakiErrorSlots;
+  return prev;
 }
 
 int ozaki_error_read_and_clear() {

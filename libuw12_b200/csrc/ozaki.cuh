@@ -54,5 +54,10 @@ int ozaki_bits(int n_moduli, long long k_total);
 // out; read_and_clear returns it (0 = none) and resets it (synchronises the
 // current stream).
 int ozaki_error_read_and_clear();
+// Error-flag slot of the calling host thread (0 .. kOzakiErrorSlots-1);
+// returns the previous slot.  Threads that evaluate concurrently use
+// different slots so that each reads and clears only its own kernels' flag.
+constexpr int kOzakiErrorSlots = 64;
+int set_error_slot(int slot);
 
 }  // namespace uw12b

@@ -73,6 +73,7 @@ def lib(timing: bool = False):
         if timing:
             L.uw12ref_timing_set.argtypes = [C.c_int]
             L.uw12ref_timing_read.argtypes = [_dp, C.POINTER(C.c_long), C.POINTER(C.c_long)]
+            L.uw12ref_timing_rotation.argtypes = [C.c_int, C.c_int]
         _libs[path] = L
     return _libs[path]
 
@@ -162,12 +163,15 @@ class RefProblem:
                                         C.byref(e), _ptr(T), C.byref(sec)), self.timing)
         return e.value, F, T, sec.value
 
-    def timed_evaluate(self, rounds: int, *args, **kw):
+    def timed_evaluate(self, rounds: int, *args, rotation: int = 0, phase: int = 0, **kw):
         """Timing build only: one evaluation with every top-level loop sampled
-        at ``rounds`` iterations per thread (0 = every iteration). Returns
-        (estimated seconds, measured seconds, sampled loops, full loops)."""
+        at ``rounds`` iterations per thread (0 = every iteration); with
+        ``rotation`` S > 0 only the loops q with q % S == phase are measured,
+        the others booked at their last estimate (``rotation=0`` clears those).
+        Returns (estimated seconds, measured seconds, measured loops, full loops)."""
         if not self.timing:
             raise ValueError("timed_evaluate needs the timing build")
+        self._L.uw12ref_timing_rotation(int(rotation), int(phase))
         self._L.uw12ref_timing_set(int(rounds))
         _, _, _, sec = self.evaluate(*args, **kw)
         extra = C.c_double(0.0)

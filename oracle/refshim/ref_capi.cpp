@@ -212,12 +212,23 @@ int uw12ref_abs_blocks(const double* S, size_t n_ao, size_t n_ri,
 }
 
 #ifdef UW12REF_TIMING_BUILD
-// Sampled loops (rounds > 0) or every iteration (0); resets the counters.
+// Sampled loops (rounds > 0) or every iteration (0); resets the counters of
+// the next evaluation (the per-loop estimates of the rotation are kept).
 void uw12ref_timing_set(int rounds) {
   uw12ref_timing::sample_rounds = rounds;
   uw12ref_timing::extra_seconds = 0.0;
   uw12ref_timing::sampled_loops = 0;
   uw12ref_timing::full_loops = 0;
+  uw12ref_timing::loop_index = 0;
+}
+
+// Rotation over the sampled loops: of S consecutive evaluations, evaluation
+// `phase` measures the loops q with q % S == phase (S = 0: all, and the cache
+// of loop estimates is cleared).
+void uw12ref_timing_rotation(int S, int phase) {
+  uw12ref_timing::rotation = S;
+  uw12ref_timing::phase = S > 0 ? phase % S : 0;
+  if (S == 0) uw12ref_timing::cached.clear();
 }
 
 // Extrapolated seconds of the iterations skipped since the last set, and the

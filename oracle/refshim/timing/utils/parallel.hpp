@@ -21,9 +21,15 @@
 //     ceil(n / T) (resp. ceil(n1 / T) * n2) iteration times with every thread
 //     busy; the sample measures r such iteration times under the same memory
 //     contention. Loop results are then partial sums; only the time is used.
+//   * rotation (rotation = S > 0, with sampling): the sampled loops of an
+//     evaluation are numbered in the order they run; loop q is measured (as
+//     above) only when q % S == phase and otherwise skipped, its estimate
+//     taken from the last evaluation that measured it. S consecutive
+//     evaluations (phase 0 .. S-1) measure every loop once, each at about
+//     1/S of the sampled cost; the code outside the loops runs every time.
 //
-// The sampled estimate is checked against full evaluations of the parity
-// build (bench.py --validate-reference-sampler).
+// The estimates are checked against full evaluations of the parity build by
+// oracle/validate_sampler.py.
 #ifndef UW12_PARALLEL_HPP
 #define UW12_PARALLEL_HPP
 
@@ -37,6 +43,10 @@ inline int sample_rounds = 0;       // 0: every iteration runs
 inline double extra_seconds = 0.0;  // extrapolated time of skipped iterations
 inline long sampled_loops = 0;      // top-level loops that were sampled
 inline long full_loops = 0;         // top-level loops that ran every iteration
+inline int rotation = 0;            // 0: every sampled loop measured each time
+inline int phase = 0;               // loops q with q % rotation == phase measured
+inline long loop_index = 0;         // sampled loops seen in this evaluation
+inline std::vector<double> cached;  // last estimate per loop index (< 0: none)
 
 inline size_t ceil_div(size_t a, size_t b) { return (a + b - 1) / b; }
 
@@ -58,16 +68,25 @@ inline std::vector<size_t> spaced(size_t n, size_t k) {
 
 // Runs body(slot, item) for every sampled item, r per thread, and books the
 // extrapolated remainder: the full loop takes `rounds_full` iteration times,
-// the sample took r of them.
+// the sample took r of them. Under rotation a loop not due for measurement
+// runs no iteration and books its cached estimate.
 template <typename Body>
 void run_sample(const std::vector<size_t>& items, size_t r, double rounds_full,
                 Body&& body) {
+  const long q_loop = loop_index++;
+  if (cached.size() <= static_cast<size_t>(q_loop)) cached.resize(q_loop + 1, -1.0);
+  if (rotation > 0 && q_loop % rotation != phase && cached[q_loop] >= 0.0) {
+    extra_seconds += cached[q_loop];
+    return;
+  }
   const double t0 = omp_get_wtime();
 #pragma omp parallel for schedule(static, 1)
   for (long q = 0; q < static_cast<long>(items.size()); ++q)
     body(static_cast<size_t>(q), items[static_cast<size_t>(q)]);
   const double dt = omp_get_wtime() - t0;
-  extra_seconds += dt * (rounds_full / static_cast<double>(r) - 1.0);
+  const double estimate = dt * rounds_full / static_cast<double>(r);
+  cached[q_loop] = estimate;
+  extra_seconds += estimate - dt;
   ++sampled_loops;
 }
 }  // namespace uw12ref_timing

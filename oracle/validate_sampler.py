@@ -1,7 +1,7 @@
 """Checks the sampled CPU-baseline timer against full evaluations -- TEST
 INFRASTRUCTURE ONLY.
 
-    python oracle/validate_sampler.py --config c1s --reps 3 [--rounds 1,2]
+    python oracle/validate_sampler.py --config c1s --reps 3 [--rounds 1] [--rotation 8]
 
 For one workload shape (the c1 generators at a reduced size) this times, on
 all host threads, in separate processes:
@@ -9,7 +9,10 @@ all host threads, in separate processes:
     (oracle/_ref/libuw12_ref.so, every loop iteration run);
   * sampled evaluations of the timing build (oracle/_ref/libuw12_ref_timing.so:
     every top-level loop runs `rounds` iterations per thread, the rest is
-    extrapolated), the estimator bench.py's reference arm uses;
+    extrapolated);
+  * with --rotation S, the estimator bench.py's reference arm uses: one primed
+    sampled evaluation, then S evaluations each measuring every S-th loop
+    (the others at their last estimate), reporting every step's estimate;
 and prints one JSON line: medians, the estimate's ratio to the full time, the
 host's CPU model and thread count.
 """
@@ -57,6 +60,12 @@ def child(args):
     if args.mode == "full":
         e, _, _, sec = p.evaluate(*a)
         out = {"mode": "full", "seconds": sec, "energy": e}
+    elif args.mode.startswith("rot"):
+        S = int(args.mode[3:])
+        p.timed_evaluate(1, *a, rotation=S, phase=0)  # primes every loop estimate
+        steps = [p.timed_evaluate(1, *a, rotation=S, phase=q) for q in range(1, S + 1)]
+        out = {"mode": args.mode, "estimates": [x[0] for x in steps],
+               "measured": [x[1] for x in steps], "measured_loops": [x[2] for x in steps]}
     else:
         est, sec, ns, nf = p.timed_evaluate(int(args.mode), *a)
         out = {"mode": f"sampled{args.mode}", "estimate": est, "measured": sec,
@@ -68,7 +77,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", default="c1s", choices=sorted(SHAPES))
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--rounds", default="1,2")
+    ap.add_argument("--rounds", default="1")
+    ap.add_argument("--rotation", type=int, default=8)
     ap.add_argument("--s-os", dest="s_os", type=float, default=1.0)
     ap.add_argument("--s-ss", dest="s_ss", type=float, default=0.5)
     ap.add_argument("--mode", default="")
@@ -78,6 +88,8 @@ def main():
         return
     runs = {}
     modes = ["full"] + [r.strip() for r in args.rounds.split(",") if r.strip()]
+    if args.rotation > 0:
+        modes.append(f"rot{args.rotation}")
     env = dict(os.environ, OPENBLAS_NUM_THREADS="1")
     for _ in range(args.reps):
         for m in modes:
@@ -90,6 +102,12 @@ def main():
            "cpu_model": cpu_model(), "threads": os.cpu_count(), "reps": args.reps,
            "full_seconds": [x["seconds"] for x in runs["full"]], "full_median": full}
     for m in modes[1:]:
+        if m.startswith("rot"):
+            ests = [e for x in runs[m] for e in x["estimates"]]
+            rec[m] = {"estimates": ests, "measured": [t for x in runs[m] for t in x["measured"]],
+                      "estimate_median": statistics.median(ests),
+                      "ratio_to_full": statistics.median(ests) / full}
+            continue
         est = statistics.median(x["estimate"] for x in runs[m])
         rec[f"sampled{m}"] = {"estimates": [x["estimate"] for x in runs[m]],
                               "measured": [x["measured"] for x in runs[m]],
