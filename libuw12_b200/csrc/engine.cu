@@ -1405,6 +1405,8 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
   FockRequest rq = rq_in;
   if (rq.n_shards > 1) throw Error(kErrInvalid, "the adjoint evaluates unsharded");
   form_fock(rq);
+  PhaseClock clock;
+  clock.mark("adj_recompute");
 
   const IntegralsHandle& W = *rq.W;
   const IntegralsHandle& V = *rq.V;
@@ -1508,6 +1510,7 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
              LL(MW));
   }
 
+  clock.mark("adj_t_x");
   // ---- adjoints of t and X
   std::vector<DevBuf> tbar(ns), Xbar(ns);
   for (int s = 0; s < ns; ++s) {
@@ -1544,6 +1547,7 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
   //   B2_V,k-bar = (G_Z^T SW_V) L_V;  A_W += Wst_W^T T_Y, A_V += SW_V^T T_Z;
   //   G_W4 = -1/2 s esf P4(V4): B2_W-bar += 2 (G_W4 B2_W) L_W,
   //   A_W += B2_W^T G_W4 B2_W (and W <-> V with P4(W4)).
+  clock.mark("adj_same_spin");
   const bool same_spin = rq.indirect && rq.s_ss != 0.0;
   std::vector<DevBuf> ssB2b[2], ssWsb[2];
   DevBuf ssA[2];
@@ -1652,6 +1656,7 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
     }
   }
 
+  clock.mark("adj_three_index");
   // ---- dE/dJ3_0 and dE/dJ3_ri_0 of W and V
   for (int which = 0; which < 2; ++which) {
     const IntegralsHandle& X = which == 0 ? W : V;
@@ -1770,6 +1775,7 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
     }
   }
 
+  clock.mark("adj_metric");
   // ---- metric gradients of W and V: -sym(Q A Q^T), Q = P2 L
   for (int which = 0; which < 2; ++which) {
     double* g2 = gJ2[which];
@@ -1836,6 +1842,7 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
   // active orbitals, two_electron.cpp:87-132): B2-bar = -s esf B2 L,
   // B1-bar = Ca B2-bar, then P2^T and the packed symmetric sum per aux
   // function with Ca; A_WV = -1/2 s esf B2^T B2
+  clock.mark("adj_wv");
   const GradSink& s3x = out.sink3[2];
   std::vector<DevBuf> ssX10(ns);  // B1-bar_0 of WV per spin (N a x MX)
   DevBuf ssAX;
@@ -1959,10 +1966,13 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
     }
   }
 
+  clock.mark("adj_copy_out");
   for (auto& sg : staged)
     UW12_CUDA(cudaMemcpyAsync(sg.second, sg.first.get(), sg.first.size() * sizeof(double),
                               cudaMemcpyDeviceToHost, st));
+  clock.mark("adj_end");
   UW12_CUDA(cudaStreamSynchronize(st));
+  clock.finish();
 }
 
 std::string phase_profile_read() {

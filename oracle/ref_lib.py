@@ -74,6 +74,8 @@ def lib(timing: bool = False):
             L.uw12ref_timing_set.argtypes = [C.c_int]
             L.uw12ref_timing_read.argtypes = [_dp, C.POINTER(C.c_long), C.POINTER(C.c_long)]
             L.uw12ref_timing_rotation.argtypes = [C.c_int, C.c_int]
+            L.uw12ref_timing_loops.argtypes = [_dp, C.c_long]
+            L.uw12ref_timing_loops.restype = C.c_long
         _libs[path] = L
     return _libs[path]
 
@@ -177,6 +179,9 @@ class RefProblem:
         extra = C.c_double(0.0)
         ns, nf = C.c_long(0), C.c_long(0)
         self._L.uw12ref_timing_read(C.byref(extra), C.byref(ns), C.byref(nf))
+        buf = np.zeros(3 * 4096)
+        n = self._L.uw12ref_timing_loops(buf.ctypes.data_as(_dp), 4096)
+        self.loop_log = buf[:3 * min(n, 4096)].reshape(-1, 3)
         self._L.uw12ref_timing_set(0)
         return sec + extra.value, sec, int(ns.value), int(nf.value)
 

@@ -220,6 +220,19 @@ void uw12ref_timing_set(int rounds) {
   uw12ref_timing::sampled_loops = 0;
   uw12ref_timing::full_loops = 0;
   uw12ref_timing::loop_index = 0;
+  uw12ref_timing::loop_log.clear();
+}
+
+// The loop log of the last evaluation: up to max records of (iterations,
+// sampled, seconds) into out (3 doubles each); returns the record count.
+long uw12ref_timing_loops(double* out, long max) {
+  const auto& lg = uw12ref_timing::loop_log;
+  for (long i = 0; i < max && i < static_cast<long>(lg.size()); ++i) {
+    out[3 * i] = static_cast<double>(lg[i].n);
+    out[3 * i + 1] = lg[i].sampled;
+    out[3 * i + 2] = lg[i].seconds;
+  }
+  return static_cast<long>(lg.size());
 }
 
 // Rotation over the sampled loops: of S consecutive evaluations, evaluation

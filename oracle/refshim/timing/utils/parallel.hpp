@@ -47,6 +47,14 @@ inline int rotation = 0;            // 0: every sampled loop measured each time
 inline int phase = 0;               // loops q with q % rotation == phase measured
 inline long loop_index = 0;         // sampled loops seen in this evaluation
 inline std::vector<double> cached;  // last estimate per loop index (< 0: none)
+// every top-level loop of the evaluation in order: iterations, 1 if sampled,
+// seconds (the estimate when sampled, the measured time otherwise)
+struct LoopRecord {
+  size_t n;
+  int sampled;
+  double seconds;
+};
+inline std::vector<LoopRecord> loop_log;
 
 inline size_t ceil_div(size_t a, size_t b) { return (a + b - 1) / b; }
 
@@ -88,6 +96,17 @@ void run_sample(const std::vector<size_t>& items, size_t r, double rounds_full,
   cached[q_loop] = estimate;
   extra_seconds += estimate - dt;
   ++sampled_loops;
+  loop_log.push_back({items.size(), 1, estimate});
+}
+
+// Times a top-level loop that runs every iteration (for the loop log).
+template <typename F>
+auto timed_full(size_t n, F&& f) {
+  if (omp_in_parallel()) return f();
+  const double t0 = omp_get_wtime();
+  auto out = f();
+  loop_log.push_back({n, 0, omp_get_wtime() - t0});
+  return out;
 }
 }  // namespace uw12ref_timing
 
@@ -107,13 +126,16 @@ inline void parallel_for(size_t start, size_t stop,
     return;
   }
   if (!omp_in_parallel()) ++ts::full_loops;
-  if (parallel) {
+  ts::timed_full(n, [&] {
+    if (parallel) {
 #pragma omp parallel for
-    for (long i = static_cast<long>(start); i < static_cast<long>(stop); ++i)
-      func(static_cast<size_t>(i));
-  } else {
-    for (size_t i = start; i < stop; ++i) func(i);
-  }
+      for (long i = static_cast<long>(start); i < static_cast<long>(stop); ++i)
+        func(static_cast<size_t>(i));
+    } else {
+      for (size_t i = start; i < stop; ++i) func(i);
+    }
+    return 0;
+  });
 }
 
 // Sum over every iteration with one partial result per thread, added up at
@@ -158,7 +180,7 @@ ReturnType parallel_sum(const size_t start, const size_t stop,
     return part[0];
   }
   if (!omp_in_parallel()) ++ts::full_loops;
-  return full_sum(start, stop, identity, func, parallel);
+  return ts::timed_full(n, [&] { return full_sum(start, stop, identity, func, parallel); });
 }
 
 template <typename ReturnType>
@@ -188,7 +210,8 @@ ReturnType parallel_sum_2d(
     for (size_t j = start2; j < stop2; ++j) result += func(i, j);
     return result;
   };
-  return full_sum(start1, stop1, identity, outer, parallel);
+  return ts::timed_full(n1 * n2,
+                        [&] { return full_sum(start1, stop1, identity, outer, parallel); });
 }
 
 template <typename Func>
