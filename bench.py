@@ -487,6 +487,10 @@ def main():
                          "the device by the library's synthetic producer at every use (inputs "
                          "larger than device memory, --config c2); three-index gradients "
                          "streamed in aux blocks to a squared-norm sink")
+    ap.add_argument("--no-fp64-forward", action="store_true",
+                    help="skip the FP64 energy + Fock arm")
+    ap.add_argument("--no-profile", action="store_true",
+                    help="skip the profiled pass (roofline and phase split)")
     ap.add_argument("--batched", action="store_true", help="add the 64-molecule batch")
     ap.add_argument("--batched-steps", type=int, default=2)
     ap.add_argument("--gemm", default="",
@@ -663,9 +667,11 @@ def main():
         return L.form_fock(W, V, WV, A, orbs, occs, act, indirect, True, args.s_os, args.s_ss,
                            fock_out=fock_dev.data_ptr())[0]
 
-    nf = max(1, min(3, args.steps))
-    elf, e_fwd = timed(forward, 1, nf)
-    s_fwd = elf / nf
+    s_fwd, e_fwd = None, None
+    if not args.no_fp64_forward:
+        nf = max(1, min(3, args.steps))
+        elf, e_fwd = timed(forward, 1, nf)
+        s_fwd = elf / nf
 
     # ---- further moduli counts
     extra = []
@@ -680,47 +686,49 @@ def main():
                                                 np.max(np.abs(fr)))})
 
     # ---- profiled pass (separate from every timed loop): kernel classes
-    L.set_precision(args.moduli)
-    L.profile_enable(True)
-    for kind in L.PROFILE_KINDS:
-        L.profile_read_kind(kind)
-    L.profile_phases()
-    L.profile_read()
-    step(g_split)
-    torch.cuda.synchronize(device)
-    kinds = {k: L.profile_read_kind(k) for k in L.PROFILE_KINDS}
-    phases_split = L.profile_phases()
-    L.set_precision(0)
-    L.profile_read()
-    forward()
-    torch.cuda.synchronize(device)
-    prof64 = L.profile_read()
-    phases_fwd = L.profile_phases()
-    L.profile_enable(False)
-    i8 = kinds["i8_mma"]
-    i8_tops = i8["work"] / (i8["ms"] / 1e3) / 1e12 if i8["ms"] else None
-    bpg = read_traffic("i8_mma_traffic.txt", "traffic_bytes_per_gop")
-    roofline = {"bound": "tensor", "kernel": "k_i8_mma (tcgen05.mma kind::i8, TMA-fed)",
-                "achieved": i8_tops, "peak": i8_peak, "unit": "TOPS",
-                "frac": i8_tops / i8_peak if i8_tops else None, "peak_source": i8_src,
-                "traffic": (bpg * i8["work"] / max(1, i8["launches"]) / 1e9) if bpg else None,
-                "launches": i8["launches"], "kernel_ms": i8["ms"],
-                "share_of_step": i8["ms"] / 1e3 / (elapsed / args.steps) if elapsed > 0 else None,
-                "ms_per_step_by_class": {"i8_mma": i8["ms"],
-                                         "operand_prep": kinds["split_prep"]["ms"],
-                                         "crt": kinds["split_crt"]["ms"],
-                                         "fp64_dmma": kinds["dgemm"]["ms"],
-                                         "producer": kinds["producer"]["ms"]}}
-    gemm_tf = prof64["flops"] / (prof64["ms"] / 1e3) / 1e12 if prof64["ms"] > 0 else None
-    bpg64 = read_traffic("dgemm_dmma_traffic.txt", "traffic_bytes_per_gflop")
-    roofline_fp64 = {"bound": "tensor", "kernel": "dgemm_dmma (mma.sync m16n8k4 f64)",
-                     "achieved": gemm_tf, "peak": fp64_peak, "unit": "TFLOP/s",
-                     "frac": gemm_tf / fp64_peak if gemm_tf else None,
-                     "peak_source": "cuBLAS DGEMM 8192^3 burst measured in this run",
-                     "traffic": (bpg64 * prof64["flops"] / max(1, prof64["launches"]) / 1e9)
-                     if bpg64 else None,
-                     "launches": prof64["launches"], "kernel_ms": prof64["ms"],
-                     "share_of_forward": prof64["ms"] / 1e3 / s_fwd if s_fwd > 0 else None}
+    roofline = roofline_fp64 = phases_split = phases_fwd = None
+    if not args.no_profile:
+        L.set_precision(args.moduli)
+        L.profile_enable(True)
+        for kind in L.PROFILE_KINDS:
+            L.profile_read_kind(kind)
+        L.profile_phases()
+        L.profile_read()
+        step(g_split)
+        torch.cuda.synchronize(device)
+        kinds = {k: L.profile_read_kind(k) for k in L.PROFILE_KINDS}
+        phases_split = L.profile_phases()
+        L.set_precision(0)
+        L.profile_read()
+        forward()
+        torch.cuda.synchronize(device)
+        prof64 = L.profile_read()
+        phases_fwd = L.profile_phases()
+        L.profile_enable(False)
+        i8 = kinds["i8_mma"]
+        i8_tops = i8["work"] / (i8["ms"] / 1e3) / 1e12 if i8["ms"] else None
+        bpg = read_traffic("i8_mma_traffic.txt", "traffic_bytes_per_gop")
+        roofline = {"bound": "tensor", "kernel": "k_i8_mma (tcgen05.mma kind::i8, TMA-fed)",
+                    "achieved": i8_tops, "peak": i8_peak, "unit": "TOPS",
+                    "frac": i8_tops / i8_peak if i8_tops else None, "peak_source": i8_src,
+                    "traffic": (bpg * i8["work"] / max(1, i8["launches"]) / 1e9) if bpg else None,
+                    "launches": i8["launches"], "kernel_ms": i8["ms"],
+                    "share_of_step": i8["ms"] / 1e3 / (elapsed / args.steps) if elapsed > 0 else None,
+                    "ms_per_step_by_class": {"i8_mma": i8["ms"],
+                                             "operand_prep": kinds["split_prep"]["ms"],
+                                             "crt": kinds["split_crt"]["ms"],
+                                             "fp64_dmma": kinds["dgemm"]["ms"],
+                                             "producer": kinds["producer"]["ms"]}}
+        gemm_tf = prof64["flops"] / (prof64["ms"] / 1e3) / 1e12 if prof64["ms"] > 0 else None
+        bpg64 = read_traffic("dgemm_dmma_traffic.txt", "traffic_bytes_per_gflop")
+        roofline_fp64 = {"bound": "tensor", "kernel": "dgemm_dmma (mma.sync m16n8k4 f64)",
+                         "achieved": gemm_tf, "peak": fp64_peak, "unit": "TFLOP/s",
+                         "frac": gemm_tf / fp64_peak if gemm_tf else None,
+                         "peak_source": "cuBLAS DGEMM 8192^3 burst measured in this run",
+                         "traffic": (bpg64 * prof64["flops"] / max(1, prof64["launches"]) / 1e9)
+                         if bpg64 else None,
+                         "launches": prof64["launches"], "kernel_ms": prof64["ms"],
+                         "share_of_forward": prof64["ms"] / 1e3 / s_fwd if s_fwd else None}
 
     # ---- end to end through the public API from pinned host buffers
     e2e = None
@@ -790,8 +798,8 @@ def main():
                     "split precision" + (", integral-direct" if args.direct else ""),
             "fp64": {"s_per_step": s64, "speedup": s64 / (elapsed / args.steps),
                      "accuracy_of_split": accuracy},
-            "fp64_forward": {"s_per_eval": s_fwd, "energy": e_fwd,
-                             "tflops_canonical": flops_fwd / s_fwd / 1e12},
+            "fp64_forward": ({"s_per_eval": s_fwd, "energy": e_fwd,
+                              "tflops_canonical": flops_fwd / s_fwd / 1e12} if s_fwd else None),
             "extra_moduli": extra,
             "canonical_flops_forward": flops_fwd,
             "tflops_canonical_forward_per_step": flops_fwd / (elapsed / args.steps) / 1e12,

@@ -1609,6 +1609,10 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
           scale_rc(Bt.get(), LL(a * nk), LL(a * nk), LL(MV), nullptr, V.lam.get(), 1.0,
                    ssB2b[1][s].get() + a * k0, LL(ao));
         }
+        Tmp = DevBuf();  // the chunk buffers are done: their memory goes to Wst-bar
+        GY = DevBuf();
+        GZ = DevBuf();
+        Bt = DevBuf();
         GemmDesc g = gemm_nn(LL(MW), LL(MW), LL(Ra), 1.0, XW.Wst[s].get(), LL(Ra), TY.get(),
                              LL(Ra), 1.0, ssA[0].get(), LL(MW));
         g.a_kcontig = true;
@@ -1617,13 +1621,14 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
                     ssA[1].get(), LL(MV));
         g.a_kcontig = true;
         gemm(g);
-        ssWsb[0][s].alloc(Ra * MW);
-        scale_rc(TY.get(), LL(Ra), LL(Ra), LL(MW), nullptr, W.lam.get(), 1.0,
-                 ssWsb[0][s].get(), LL(Ra));
+        // Wst_W-bar = T_Y L_W in place; Wst_V-bar = (I (x) S^-1) (T_Z L_V)
+        scale_rc(TY.get(), LL(Ra), LL(Ra), LL(MW), nullptr, W.lam.get(), 1.0, TY.get(), LL(Ra));
+        ssWsb[0][s] = std::move(TY);
         scale_rc(TZ.get(), LL(Ra), LL(Ra), LL(MV), nullptr, V.lam.get(), 1.0, TZ.get(), LL(Ra));
         ssWsb[1][s].alloc(Ra * MV);
         gemm(gemm_nn(LL(Rp), LL(a * MV), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp), TZ.get(), LL(Rp),
                      0.0, ssWsb[1][s].get(), LL(Rp)));
+        TZ = DevBuf();
       }
       // four-electron
       {

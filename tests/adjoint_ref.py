@@ -370,3 +370,74 @@ def indirect_adjoint(Wb, Vb, WVb, abs_p, orbitals, occ, n_active):
         Q = Xi.P2 * lam[None, :]
         out[key] = -sym(Q @ A @ Q.T)
     return out
+
+
+def blocked_three_index_adjoint(Wb, Vb, abs_p, orbitals, occ, n_active, s_os, s_ss, nb):
+    """dE/dJ3_0 and dE/dJ3_ri_0 of W and V (the direct terms, as
+    ``direct_adjoint``) computed per block of ``nb`` aux functions of the
+    gradient, without any stacked (R' a x M) or B1-sized intermediate:
+    for gradient block b of potential X (the other potential Y),
+      t path:   B1bar_0[:, b] = Ca (B2_Y (tbar' P2_X^T[:, b]))         (N x o per column)
+      Wst path: Z_b = P2_Y (Xbar' P2_X^T[:, b]),  G_b = J3_0^Y Z_b,  H_b = J3_ri_0^Y Z_b,
+                Q_b = [sq(G_b) Ca ; H_b Ca] (R' x a per column),  SQ_b = S^-1 Q_b;
+      dE/dJ3_0[:, A]    = packed symmetric sum of (B1bar_0[:, A] + SQ_b AO rows at the
+                          active orbitals) Co^T,
+      dE/dJ3_ri_0[:, A] = SQ_b RI rows Ca^T,
+    with tbar' = tbar^T, Xbar' = Xbar^T for X = W and tbar, Xbar for X = V.
+    X and t come from orbital chunks (schedule_model.chunked_xab_t)."""
+    from tests import schedule_model as K
+    ns = len(orbitals)
+    Co = O.occupation_weighted_orbitals(orbitals, occ)
+    Ca = O.freeze_core(Co, n_active)
+    W = O.Integrals(Wb, Co, Ca)
+    V = O.Integrals(Vb, Co, Ca)
+    N, M, R = Wb.n_ao, Wb.n_df, Wb.n_ri
+    Rp = N + R
+    F = np.array([[spin_factor(ns, s, sp, s_os, s_ss) for sp in range(ns)] for s in range(ns)])
+    lw, lv = W.df_vals, V.df_vals
+    Sinv = np.block([[abs_p.s_inv_ao_ao, abs_p.s_inv_ao_ri], [abs_p.s_inv_ri_ao, abs_p.s_inv_ri_ri]])
+    X, t = [], []
+    for s in range(ns):
+        xs, ts = K.chunked_xab_t(Wb, Vb, Sinv, Co[s], Ca[s], max(1, Ca[s].shape[1]))
+        X.append(xs)
+        t.append(ts)
+    tt = [lw[:, None] * t[s] * lv[None, :] for s in range(ns)]
+    tbar, Xbar = [], []
+    for s in range(ns):
+        tb = sum(0.5 * F[s, sp] * tt[sp] for sp in range(ns))
+        ttb = sum(F[sp, s] * (0.5 * t[sp] - X[sp]) for sp in range(ns))
+        tbar.append(tb + lw[:, None] * ttb * lv[None, :])
+        Xbar.append(-sum(F[s, sp] * tt[sp] for sp in range(ns)))
+    out = {}
+    for which, (Xi, Yi, Xo, Yo) in enumerate(((Wb, Vb, W, V), (Vb, Wb, V, W))):
+        P2x, P2y = Xi.P2, Yi.P2
+        Mx = P2x.shape[0]
+        g3 = np.zeros((N * (N + 1) // 2, Mx))
+        g3ri = np.zeros((R * N, Mx))
+        for s in range(ns):
+            o, a = Co[s].shape[1], Ca[s].shape[1]
+            c = o - a
+            if a == 0:
+                continue
+            tb = tbar[s].T if which == 0 else tbar[s]     # M_Y x M_X
+            xb = Xbar[s].T if which == 0 else Xbar[s]
+            B2y = Yo.get_X3idx_two_trans()[s]              # a o x M_Y
+            for b0 in range(0, Mx, nb):
+                b1 = min(Mx, b0 + nb)
+                cols = b1 - b0
+                Pt = P2x.T[:, b0:b1]                       # M_X x cols: P2_X^T[:, b]
+                Dt = B2y @ (tb @ Pt)                       # a o x cols
+                Zb = P2y @ (xb @ Pt)                       # M_Y x cols
+                Gb = Yi.J3_0 @ Zb                          # Np x cols
+                Hb = Yi.J3_ri_0 @ Zb                       # R N x cols
+                for q in range(cols):
+                    b1t = Ca[s] @ Dt[:, q].reshape((a, o), order="F")        # N x o
+                    Qao = O.square(Gb[:, q]) @ Ca[s]                          # N x a
+                    Qri = Hb[:, q].reshape((R, N), order="F") @ Ca[s]         # R x a
+                    SQ = Sinv @ np.vstack([Qao, Qri])                          # R' x a
+                    b1t[:, c:] += SQ[:N]
+                    g3[:, b0 + q] += _pack_sym_sum(b1t @ Co[s].T)
+                    g3ri[:, b0 + q] += (SQ[N:] @ Ca[s].T).reshape(-1, order="F")
+        out["W3" if which == 0 else "V3"] = g3
+        out["W3_ri" if which == 0 else "V3_ri"] = g3ri
+    return out
