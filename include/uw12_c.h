@@ -235,15 +235,30 @@ int uw12c_energy(const uw12c_integrals* W, const uw12c_integrals* V, const uw12c
 int uw12c_set_stream(void* stream);
 int uw12c_set_memory_budget(size_t bytes);
 /* Splits the following evaluations of this host thread into n_shards parts
- * and computes part `shard` only (no counterpart in libuw12): the loops of
- * the t~ dX Fock term (over aux functions) and of the same-spin
- * three-electron energy and Fock (over occupied orbitals k) run over a
- * contiguous, balanced part of their range; every other contribution is
- * computed by shard 0.  Energies and
- * Fock matrices of the n_shards parts sum to the full result (one GPU per
- * shard, summed with an all-reduce).  uw12c_set_shard(0, 1) restores full
- * evaluations. */
+ * and computes part `shard` only (no counterpart in libuw12; one GPU per
+ * shard).  Aux functions are dealt out in contiguous, balanced ranges: the
+ * fitted densities, the MO transforms of the three-index tensors (W, V, WV)
+ * and the 2-el Fock run over this shard's aux range, and their partial sums
+ * are completed by the all-reduce hook (uw12c_set_allreduce) before use; the
+ * t~ dX Fock term runs over this shard's range of W's aux functions.  The
+ * occupied orbitals are dealt out likewise: X_AB and t (their M x M partials
+ * all-reduced), the direct Fock and the same-spin three-electron energy and
+ * Fock.  The remaining small terms (the energies built from the reduced
+ * intermediates, the same-spin 2-el and 4-el terms) come from shard 0.
+ * Energies and Fock matrices of the n_shards parts sum to the full result
+ * (the caller's final all-reduce).  uw12c_set_shard(0, 1) restores full
+ * evaluations; the adjoint evaluates unsharded. */
 int uw12c_set_shard(size_t shard, size_t n_shards);
+/* The all-reduce of sharded evaluations on this host thread: fn(data, count,
+ * stream, user) must replace the `count` doubles at device pointer `data` by
+ * their sum over the shards, ordered after the work already queued on
+ * `stream` (a cudaStream_t) and before any work queued on it afterwards, and
+ * return 0 (non-zero fails the evaluation).  Every shard calls it at the same
+ * points with the same counts.  fn = NULL removes it; a sharded evaluation
+ * without one fails with UW12C_ERR_INVALID.  (torch.distributed.all_reduce over
+ * NCCL on the given stream is one such function: libuw12_b200.distributed.) */
+typedef int (*uw12c_allreduce_fn)(double* data, size_t count, void* stream, void* user);
+int uw12c_set_allreduce(uw12c_allreduce_fn fn, void* user);
 /* The library keeps device memory freed by one call reserved for the next
  * (its own stream-ordered pool); this returns the unused part to the system. */
 int uw12c_trim_memory(void);

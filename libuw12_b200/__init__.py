@@ -13,8 +13,9 @@ from __future__ import annotations
 
 import ctypes
 import os
+import threading
 from pathlib import Path
-from typing import List, Optional, Sequence, Tuple
+from typing import Callable, List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -108,6 +109,7 @@ def lib():
     L.uw12c_set_stream.argtypes = [P]
     L.uw12c_set_memory_budget.argtypes = [c_sz]
     L.uw12c_set_shard.argtypes = [c_sz, c_sz]
+    L.uw12c_set_allreduce.argtypes = [ALLREDUCE_FN, P]
     L.uw12c_launch_count.restype = ctypes.c_ulonglong
     L.uw12c_profile_enable.argtypes = [ctypes.c_int]
     L.uw12c_profile_read.argtypes = [ctypes.POINTER(ctypes.c_ulonglong), PD, PD]
@@ -686,8 +688,40 @@ def set_stream(stream_ptr: int):
 
 def set_shard(shard: int, n_shards: int):
     """Evaluate only part `shard` of `n_shards` in subsequent calls on this thread
-    (partial energies and Fock matrices sum to the full result)."""
+    (partial energies and Fock matrices sum to the full result; a sharded
+    evaluation needs an all-reduce, set_allreduce)."""
     _check(lib().uw12c_set_shard(int(shard), int(n_shards)))
+
+
+# fn(data, count, stream, user) -> 0: sums `count` doubles at device address
+# `data` over the shards, ordered on the cudaStream_t `stream`
+ALLREDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                                ctypes.c_void_p)
+_allreduce_keep = threading.local()
+
+
+def set_allreduce(fn: Optional[Callable[[int, int, int], None]]):
+    """The all-reduce of sharded evaluations on this host thread
+    (uw12c_set_allreduce): ``fn(data_ptr, count, stream_ptr)`` replaces the
+    ``count`` float64 values at device address ``data_ptr`` by their sum over
+    the shards, ordered on the CUDA stream ``stream_ptr``; an exception fails
+    the evaluation.  None removes it."""
+    if fn is None:
+        _check(lib().uw12c_set_allreduce(ALLREDUCE_FN(), None))
+        _allreduce_keep.cb = None
+        return
+
+    def tramp(data, count, stream, user):
+        try:
+            fn(int(data or 0), int(count), int(stream or 0))
+            return 0
+        except Exception as exc:  # reported through the evaluation's status
+            _allreduce_keep.error = exc
+            return 1
+
+    cb = ALLREDUCE_FN(tramp)
+    _check(lib().uw12c_set_allreduce(cb, None))
+    _allreduce_keep.cb = cb  # the C side holds only the pointer
 
 
 def trim_memory():

@@ -33,6 +33,8 @@ std::atomic<size_t> g_budget{0};
 // Per-thread budget of the worker threads of a batched evaluation (0 = none).
 thread_local size_t g_budget_override = 0;
 thread_local size_t g_shard = 0, g_n_shards = 1;
+thread_local uw12c_allreduce_fn g_allreduce = nullptr;
+thread_local void* g_allreduce_user = nullptr;
 thread_local int g_last_status = UW12C_OK;
 thread_local std::string g_last_msg;
 }  // namespace
@@ -206,6 +208,8 @@ void run_form_fock(const uw12c_integrals* W, const uw12c_integrals* V, const uw1
   rq.mem_budget = uw12b::g_budget_override ? uw12b::g_budget_override : uw12b::g_budget.load();
   rq.shard = uw12b::g_shard;
   rq.n_shards = uw12b::g_n_shards;
+  rq.allreduce = uw12b::g_allreduce;
+  rq.allreduce_user = uw12b::g_allreduce_user;
   DeviceGuard dg(w.device);
   if (adjoint)
     uw12b::form_fock_adjoint(rq, *adjoint);
@@ -375,6 +379,13 @@ int uw12c_set_shard(size_t shard, size_t n_shards) {
     need(n_shards >= 1 && shard < n_shards, "shard must be < n_shards, n_shards >= 1");
     uw12b::g_shard = shard;
     uw12b::g_n_shards = n_shards;
+  });
+}
+
+int uw12c_set_allreduce(uw12c_allreduce_fn fn, void* user) {
+  return guarded([&] {
+    uw12b::g_allreduce = fn;
+    uw12b::g_allreduce_user = fn ? user : nullptr;
   });
 }
 

@@ -22,6 +22,7 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <exception>
 #include <vector>
 #include <thread>
@@ -518,14 +519,18 @@ double spin_factor(int ns, int s, int sp, double s_os, double s_ss) {
 }
 
 // XDr (M x ns) = J3_0^T dmat: the unscaled fitted densities of libuw12's
-// get_X_D (integrals.cpp:347-378), over aux blocks.
+// get_X_D (integrals.cpp:347-378), over aux blocks; only the rows of aux
+// functions [a_lo, a_hi) are formed (the others are zero).
 void fitted_density_raw(const IntegralsHandle& X, const double* dmat, int ns, double* XDr,
-                        size_t budget) {
+                        size_t budget, size_t a_lo = 0, size_t a_hi = SIZE_MAX) {
   const size_t M = X.n_df, np = packed_size(X.n_ao);
+  a_hi = std::min(a_hi, M);
+  if (a_lo > 0 || a_hi < M)
+    UW12_CUDA(cudaMemsetAsync(XDr, 0, M * ns * sizeof(double), current_stream()));
   DevBuf scratch;
   const size_t step = aux_step(X, false, budget);
-  for (size_t b0 = 0; b0 < M; b0 += step) {
-    const size_t nb = std::min(step, M - b0);
+  for (size_t b0 = a_lo; b0 < a_hi; b0 += step) {
+    const size_t nb = std::min(step, a_hi - b0);
     GemmDesc g = gemm_nn(LL(nb), ns, LL(np), 1.0, aux_block(X, false, b0, nb, scratch), LL(np),
                          dmat, LL(np), 0.0, XDr + b0, LL(M));
     g.a_kcontig = true;
@@ -533,17 +538,18 @@ void fitted_density_raw(const IntegralsHandle& X, const double* dmat, int ns, do
   }
 }
 
-// H2 (R*na x M) = [J3_ri_0[:,A] (R x N) Cm] for every A (transform_second_index,
-// transformations.hpp:130-158), over aux blocks.
+// H2 (R*na x (a_hi - a_lo)) = [J3_ri_0[:,A] (R x N) Cm] for A in [a_lo, a_hi)
+// (transform_second_index, transformations.hpp:130-158), over aux blocks.
 void ri_transform(const IntegralsHandle& X, const double* Cm, size_t na, double* H2,
-                  size_t budget) {
-  const size_t N = X.n_ao, R = X.n_ri, M = X.n_df;
+                  size_t budget, size_t a_lo = 0, size_t a_hi = SIZE_MAX) {
+  const size_t N = X.n_ao, R = X.n_ri;
+  a_hi = std::min(a_hi, X.n_df);
   DevBuf scratch;
   const size_t step = aux_step(X, true, budget);
-  for (size_t b0 = 0; b0 < M; b0 += step) {
-    const size_t nb = std::min(step, M - b0);
+  for (size_t b0 = a_lo; b0 < a_hi; b0 += step) {
+    const size_t nb = std::min(step, a_hi - b0);
     GemmDesc g = gemm_nn(LL(R), LL(na), LL(N), 1.0, aux_block(X, true, b0, nb, scratch), LL(R),
-                         Cm, LL(N), 0.0, H2 + R * na * b0, LL(R));
+                         Cm, LL(N), 0.0, H2 + R * na * (b0 - a_lo), LL(R));
     g.nbo1 = LL(nb);
     g.sAo1 = LL(R * N);
     g.sCo1 = LL(R * na);
@@ -551,19 +557,22 @@ void ri_transform(const IntegralsHandle& X, const double* Cm, size_t na, double*
   }
 }
 
-// H (N*nc x M) = [sq(J3_0[:,A]) Cm] for every A, chunked over A.
+// H (N*nc x (a_hi - a_lo)) = [sq(J3_0[:,A]) Cm] for A in [a_lo, a_hi), chunked
+// over A.
 void transform_ao(const IntegralsHandle& X, const double* Cm, size_t nc, double* H,
-                  size_t budget) {
+                  size_t budget, size_t a_lo = 0, size_t a_hi = SIZE_MAX) {
   const size_t N = X.n_ao, M = X.n_df, np = packed_size(N);
-  if (nc == 0) return;
-  const size_t ac = std::max<size_t>(1, std::min(M, budget / (N * N + (X.J3_0.get() ? 0 : np))));
+  a_hi = std::min(a_hi, M);
+  if (nc == 0 || a_hi <= a_lo) return;
+  const size_t ac =
+      std::max<size_t>(1, std::min(a_hi - a_lo, budget / (N * N + (X.J3_0.get() ? 0 : np))));
   DevBuf U(N * N * ac), scratch;
-  for (size_t a0 = 0; a0 < M; a0 += ac) {
-    const size_t na = std::min(ac, M - a0);
+  for (size_t a0 = a_lo; a0 < a_hi; a0 += ac) {
+    const size_t na = std::min(ac, a_hi - a0);
     unpack_sym(aux_block(X, false, a0, na, scratch), LL(np), LL(N), LL(na), U.get(), LL(N),
                LL(N * N));
     GemmDesc g = gemm_nn(LL(N), LL(nc), LL(N), 1.0, U.get(), LL(N), Cm, LL(N), 0.0,
-                         H + N * nc * a0, LL(N));
+                         H + N * nc * (a0 - a_lo), LL(N));
     g.nbo1 = LL(na);
     g.sAo1 = LL(N * N);
     g.sCo1 = LL(N * nc);
@@ -662,15 +671,29 @@ void form_fock(const FockRequest& rq) {
   const double kap4 = 2.0 * half;
   cudaStream_t st = current_stream();
   size_t budget = auto_budget_doubles(rq.mem_budget);
-  // Sharding: the chunk loops (t~ dX over aux functions, same-spin 3-el
-  // energy and Fock over occupied k) run over a contiguous, balanced part of
-  // their index range per shard; all other contributions come from shard 0
-  // only.  The caller sums the partial energies and Fock matrices over shards.
+  // Sharding: aux functions and occupied orbitals are dealt out in
+  // contiguous, balanced ranges (part).  The fitted densities, the MO
+  // transforms and the 2-el Fock run over this shard's aux range, and the
+  // partial intermediates (fitted densities, B1, the stacked RI rows) are
+  // summed over the shards by rq.allreduce before use; X_AB and t are summed
+  // from orbital ranges the same way.  The t~ dX Fock term runs over a range
+  // of W's aux functions, the direct Fock and the same-spin 3-el energy and
+  // Fock over ranges of occupied k.  The energies built from the reduced
+  // intermediates and the same-spin 2-el / 4-el terms come from shard 0.  The
+  // caller sums the partial energies and Fock matrices over the shards.
   const size_t n_shards = std::max<size_t>(1, rq.n_shards);
   const size_t shard = rq.shard;
   const bool lead = shard == 0;
+  const bool sharded = n_shards > 1;
   auto part = [&](size_t total) {
     return std::make_pair(total * shard / n_shards, total * (shard + 1) / n_shards);
+  };
+  if (sharded && !rq.allreduce)
+    throw Error(kErrInvalid, "a sharded evaluation needs an all-reduce (uw12c_set_allreduce)");
+  auto allreduce = [&](double* buf, size_t count) {
+    if (!sharded || count == 0) return;
+    if (rq.allreduce(buf, count, st, rq.allreduce_user) != 0)
+      throw Error(kErrInvalid, "the all-reduce of a sharded evaluation failed");
   };
 
   std::vector<SpinDims> sd;
@@ -693,10 +716,13 @@ void form_fock(const FockRequest& rq) {
   // two-electron term (two_electron.cpp:11-153), WV integrals, active orbitals
   // =====================================================================
   clock.mark("two_electron");
-  if (lead) {
+  {
+    // fitted densities and the 2-el Fock over this shard's aux range of WV
+    const auto [xlo, xhi] = part(MX);
     DevBuf dmat(np * ns), XDr(MX * ns), XD(MX * ns);
     for (int s = 0; s < ns; ++s) pack_density(Ca_s(s), LL(N), LL(N), LL(sd[s].a), two, dmat.get() + np * s);
-    fitted_density_raw(WV, dmat.get(), ns, XDr.get(), budget);
+    fitted_density_raw(WV, dmat.get(), ns, XDr.get(), budget, xlo, xhi);
+    allreduce(XDr.get(), MX * ns);
     GemmDesc g = gemm_nn(LL(MX), ns, LL(MX), 0.5 * ns, WV.P2.get(), LL(MX), XDr.get(), LL(MX), 0.0,
                          XD.get(), LL(MX));
     g.a_kcontig = true;
@@ -706,8 +732,9 @@ void form_fock(const FockRequest& rq) {
       for (int sp = 0; sp < ns; ++sp) {
         const double f = spin_factor(ns, s, sp, s_os, s_ss);
         if (f == 0.0) continue;
-        wdot(XD.get() + MX * s, LL(MX), XD.get() + MX * sp, LL(MX), LL(MX), 1, WV.lam.get(),
-             nullptr, 0.5 * f, acc.get(), kE2d);
+        if (lead)
+          wdot(XD.get() + MX * s, LL(MX), XD.get() + MX * sp, LL(MX), LL(MX), 1, WV.lam.get(),
+               nullptr, 0.5 * f, acc.get(), kE2d);
         coef[s * ns + sp] = 0.5 * ns * f;
       }
     if (calc) {
@@ -716,27 +743,32 @@ void form_fock(const FockRequest& rq) {
       gemm(gemm_nn(LL(MX), ns, LL(MX), 1.0, WV.P2.get(), LL(MX), vc.get(), LL(MX), 0.0, u.get(),
                    LL(MX)));
       {
-        // gv = J3_0 u, accumulated over aux blocks
+        // gv = J3_0 u over this shard's aux blocks
         DevBuf scratch;
         const size_t step = aux_step(WV, false, budget);
-        for (size_t b0 = 0; b0 < MX; b0 += step) {
-          const size_t nb = std::min(step, MX - b0);
+        if (xhi == xlo) gv.zero();
+        for (size_t b0 = xlo; b0 < xhi; b0 += step) {
+          const size_t nb = std::min(step, xhi - b0);
           gemm(gemm_nn(LL(np), ns, LL(nb), 1.0, aux_block(WV, false, b0, nb, scratch), LL(np),
-                       u.get() + b0, LL(MX), b0 ? 1.0 : 0.0, gv.get(), LL(np)));
+                       u.get() + b0, LL(MX), b0 > xlo ? 1.0 : 0.0, gv.get(), LL(np)));
         }
       }
       for (int s = 0; s < ns; ++s)
         unpack_sym(gv.get() + np * s, LL(np), LL(N), 1, Fp[s].get(), LL(N), 0, 1.0, 1.0);
     }
     if (do_ind && a_tot > 0) {
-      DevBuf H(N * a_tot * MX);
-      transform_ao(WV, Ca.get(), a_tot, H.get(), budget / 2);
+      // B1 of the active orbitals: the shard's aux range of sq(J3_0) Ca times
+      // the matching rows of P2, summed over the shards
+      DevBuf H(N * a_tot * (xhi - xlo));
+      transform_ao(WV, Ca.get(), a_tot, H.get(), budget / 2, xlo, xhi);
       for (int s = 0; s < ns; ++s) {
         const size_t a = sd[s].a;
         if (!a) continue;
         DevBuf B1(N * a * MX), B2(a * a * MX);
-        gemm(gemm_nn(LL(N * a), LL(MX), LL(MX), 1.0, H.get() + N * sd[s].aoff, LL(N * a_tot),
-                     WV.P2.get(), LL(MX), 0.0, B1.get(), LL(N * a)));
+        gemm(gemm_nn(LL(N * a), LL(MX), LL(xhi - xlo), 1.0, H.get() + N * sd[s].aoff,
+                     LL(N * a_tot), WV.P2.get() + xlo, LL(MX), 0.0, B1.get(), LL(N * a)));
+        allreduce(B1.get(), N * a * MX);
+        if (!lead) continue;
         GemmDesc g3 = gemm_nn(LL(a), LL(a * MX), LL(N), 1.0, Ca_s(s), LL(N), B1.get(), LL(N), 0.0,
                               B2.get(), LL(a));
         g3.a_kcontig = true;
@@ -773,7 +805,18 @@ void form_fock(const FockRequest& rq) {
   size_t whole = 0;
   for (int s = 0; s < ns; ++s)
     whole += 2 * (N * sd[s].o * MW + sd[s].a * sd[s].o * MW) + 3 * Rp * sd[s].a * MW;
-  const bool orbital_chunked = !do_ind && whole > budget;
+  bool orbital_chunked = !do_ind && whole > budget;
+  if (sharded && !do_ind) {
+    // every shard takes the same branch (the budgets may differ)
+    DevBuf flag(1);
+    const double one = orbital_chunked ? 1.0 : 0.0;
+    UW12_CUDA(cudaMemcpyAsync(flag.get(), &one, sizeof(double), cudaMemcpyHostToDevice, st));
+    allreduce(flag.get(), 1);
+    double any = 0.0;
+    UW12_CUDA(cudaMemcpyAsync(&any, flag.get(), sizeof(double), cudaMemcpyDeviceToHost, st));
+    UW12_CUDA(cudaStreamSynchronize(st));
+    orbital_chunked = any > 0.0;
+  }
   for (int which = 0; which < 2 && !orbital_chunked; ++which) {
     const IntegralsHandle& X = which == 0 ? W : V;
     PerX& P = which == 0 ? XW : XV;
@@ -783,19 +826,23 @@ void form_fock(const FockRequest& rq) {
     P.B2.resize(ns);
     P.Wst.resize(ns);
     P.SV.resize(ns);
+    // this shard's aux functions [xlo, xhi): B1 and the stacked RI rows are
+    // partial products H[:, xlo:xhi] P2[xlo:xhi, :], summed over the shards
+    const auto [xlo, xhi] = part(M);
     {
-      DevBuf H(N * o_tot * M);
-      transform_ao(X, Co.get(), o_tot, H.get(), budget / 2);
+      DevBuf H(N * o_tot * (xhi - xlo));
+      transform_ao(X, Co.get(), o_tot, H.get(), budget / 2, xlo, xhi);
       for (int s = 0; s < ns; ++s) {
         const size_t o = sd[s].o;
         if (!o) continue;
         P.B1[s].alloc(N * o * M);
-        gemm(gemm_nn(LL(N * o), LL(M), LL(M), 1.0, H.get() + N * sd[s].ooff, LL(N * o_tot),
-                     X.P2.get(), LL(M), 0.0, P.B1[s].get(), LL(N * o)));
+        gemm(gemm_nn(LL(N * o), LL(M), LL(xhi - xlo), 1.0, H.get() + N * sd[s].ooff,
+                     LL(N * o_tot), X.P2.get() + xlo, LL(M), 0.0, P.B1[s].get(), LL(N * o)));
+        allreduce(P.B1[s].get(), N * o * M);
       }
     }
-    DevBuf H2(R * a_tot * M);
-    if (a_tot) ri_transform(X, Ca.get(), a_tot, H2.get(), budget);
+    DevBuf H2(R * a_tot * (xhi - xlo));
+    if (a_tot) ri_transform(X, Ca.get(), a_tot, H2.get(), budget, xlo, xhi);
     for (int s = 0; s < ns; ++s) {
       const size_t o = sd[s].o, a = sd[s].a, c = sd[s].c;
       if (!a) continue;
@@ -805,14 +852,17 @@ void form_fock(const FockRequest& rq) {
       g3.a_kcontig = true;
       gemm(g3);
       P.Wst[s].alloc(Rp * a * M);
-      copy3d(P.B1[s].get() + N * c, LL(N), LL(N * o), P.Wst[s].get(), LL(Rp), LL(Rp * a), LL(N),
-             LL(a), LL(M));
-      GemmDesc g2 = gemm_nn(LL(R), LL(M), LL(M), 1.0, H2.get() + R * sd[s].aoff, LL(R * a_tot),
-                            X.P2.get(), LL(M), 0.0, P.Wst[s].get() + N, LL(Rp * a));
+      if (sharded) P.Wst[s].zero();  // AO rows stay zero through the sum
+      GemmDesc g2 = gemm_nn(LL(R), LL(M), LL(xhi - xlo), 1.0, H2.get() + R * sd[s].aoff,
+                            LL(R * a_tot), X.P2.get() + xlo, LL(M), 0.0, P.Wst[s].get() + N,
+                            LL(Rp * a));
       g2.nbo1 = LL(a);
       g2.sAo1 = LL(R);
       g2.sCo1 = LL(Rp);
       gemm(g2);
+      allreduce(P.Wst[s].get(), Rp * a * M);
+      copy3d(P.B1[s].get() + N * c, LL(N), LL(N * o), P.Wst[s].get(), LL(Rp), LL(Rp * a), LL(N),
+             LL(a), LL(M));
       if (which == 1 || need_sv_w) {
         P.SV[s].alloc(Rp * a * M);
         gemm(gemm_nn(LL(Rp), LL(a * M), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp), P.Wst[s].get(),
@@ -858,9 +908,11 @@ void form_fock(const FockRequest& rq) {
         continue;
       }
       // X_AB = sum over active-orbital chunks of Wst_W[j]^T S^-1 Wst_V[j]
-      const size_t jc = std::max<size_t>(1, std::min(a, budget / 2 / per_j));
-      for (size_t j0 = 0; j0 < a; j0 += jc) {
-        const size_t nj = std::min(jc, a - j0);
+      // (this shard's orbitals; summed over the shards below)
+      const auto [jlo, jhi] = part(a);
+      const size_t jc = std::max<size_t>(1, std::min(jhi - jlo, budget / 2 / per_j));
+      for (size_t j0 = jlo; j0 < jhi; j0 += jc) {
+        const size_t nj = std::min(jc, jhi - j0);
         DevBuf St[2];
         for (int which = 0; which < 2; ++which) {
           const IntegralsHandle& X = which == 0 ? W : V;
@@ -889,14 +941,16 @@ void form_fock(const FockRequest& rq) {
         gemm(gemm_nn(LL(Rp), LL(nj * MV), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp), St[1].get(),
                      LL(Rp), 0.0, SVj.get(), LL(Rp)));
         GemmDesc gx = gemm_nn(LL(MW), LL(MV), LL(Rp * nj), 1.0, St[0].get(), LL(Rp * nj),
-                              SVj.get(), LL(Rp * nj), j0 ? 1.0 : 0.0, Xab[s].get(), LL(MW));
+                              SVj.get(), LL(Rp * nj), 1.0, Xab[s].get(), LL(MW));
         gx.a_kcontig = true;
         gemm(gx);
       }
       // t = sum over occupied-orbital chunks of B2_W[k]^T B2_V[k], B2 = Ca^T B1
-      const size_t kc = std::max<size_t>(1, std::min(o, budget / 2 / per_k(s)));
-      for (size_t k0 = 0; k0 < o; k0 += kc) {
-        const size_t nk = std::min(kc, o - k0);
+      // (this shard's orbitals)
+      const auto [klo, khi] = part(o);
+      const size_t kc = std::max<size_t>(1, std::min(khi - klo, budget / 2 / per_k(s)));
+      for (size_t k0 = klo; k0 < khi; k0 += kc) {
+        const size_t nk = std::min(kc, khi - k0);
         DevBuf B1w, B1v, B2w(a * nk * MW), B2v(a * nk * MV);
         b1_chunk(W, s, k0, nk, B1w);
         b1_chunk(V, s, k0, nk, B1v);
@@ -909,10 +963,12 @@ void form_fock(const FockRequest& rq) {
         g3.a_kcontig = true;
         gemm(g3);
         GemmDesc gt = gemm_nn(LL(MW), LL(MV), LL(a * nk), 1.0, B2w.get(), LL(a * nk), B2v.get(),
-                              LL(a * nk), k0 ? 1.0 : 0.0, tab[s].get(), LL(MW));
+                              LL(a * nk), 1.0, tab[s].get(), LL(MW));
         gt.a_kcontig = true;
         gemm(gt);
       }
+      allreduce(Xab[s].get(), MW * MV);
+      allreduce(tab[s].get(), MW * MV);
       scale_rc(tab[s].get(), LL(MW), LL(MW), LL(MV), W.lam.get(), V.lam.get(), 1.0,
                ttl[s].get(), LL(MW));
     }
@@ -928,14 +984,22 @@ void form_fock(const FockRequest& rq) {
       ttl[s].zero();
       continue;
     }
-    GemmDesc gx = gemm_nn(LL(MW), LL(MV), LL(Rp * a), 1.0, XW.Wst[s].get(), LL(Rp * a),
-                          XV.SV[s].get(), LL(Rp * a), 0.0, Xab[s].get(), LL(MW));
+    // sums over this shard's orbitals (rows p + R' j of Wst / S^-1 Wst, rows
+    // i + a k of B2), completed over the shards
+    const auto [jlo, jhi] = part(a);
+    const auto [klo, khi] = part(o);
+    GemmDesc gx = gemm_nn(LL(MW), LL(MV), LL(Rp * (jhi - jlo)), 1.0, XW.Wst[s].get() + Rp * jlo,
+                          LL(Rp * a), XV.SV[s].get() + Rp * jlo, LL(Rp * a), 0.0, Xab[s].get(),
+                          LL(MW));
     gx.a_kcontig = true;
     gemm(gx);
-    GemmDesc gt = gemm_nn(LL(MW), LL(MV), LL(a * o), 1.0, XW.B2[s].get(), LL(a * o),
-                          XV.B2[s].get(), LL(a * o), 0.0, tab[s].get(), LL(MW));
+    GemmDesc gt = gemm_nn(LL(MW), LL(MV), LL(a * (khi - klo)), 1.0, XW.B2[s].get() + a * klo,
+                          LL(a * o), XV.B2[s].get() + a * klo, LL(a * o), 0.0, tab[s].get(),
+                          LL(MW));
     gt.a_kcontig = true;
     gemm(gt);
+    allreduce(Xab[s].get(), MW * MV);
+    allreduce(tab[s].get(), MW * MV);
     scale_rc(tab[s].get(), LL(MW), LL(MW), LL(MV), W.lam.get(), V.lam.get(), 1.0, ttl[s].get(),
              LL(MW));
   }
@@ -963,9 +1027,10 @@ void form_fock(const FockRequest& rq) {
   // =====================================================================
   if (calc) {
     clock.mark("direct_fock");
-    for (int s = 0; s < ns && lead; ++s) {
+    for (int s = 0; s < ns; ++s) {
       const size_t o = sd[s].o, a = sd[s].a, c = sd[s].c;
-      if (!o) continue;
+      const auto [klo, khi] = part(o);  // this shard's occupied orbitals
+      if (khi == klo) continue;
       const double* Tq[2] = {ttl[0].get(), ns > 1 ? ttl[1].get() : nullptr};
       const double* Xq[2] = {Xab[0].get(), ns > 1 ? Xab[1].get() : nullptr};
       double cT[2] = {0, 0}, cX[2] = {0, 0};
@@ -976,19 +1041,22 @@ void form_fock(const FockRequest& rq) {
       }
       DevBuf Y(MW * MV);
       combine_y(Y.get(), LL(MW), Tq, cT, Xq, cX, ns, W.lam.get(), V.lam.get());
-      // whole B1, or B1 of W and V recomputed for a chunk of occupied orbitals
-      const size_t kc =
-          orbital_chunked ? std::max<size_t>(1, std::min(o, budget / 2 / per_k(s))) : o;
-      for (size_t k0 = 0; k0 < o; k0 += kc) {
-        const size_t nk = std::min(kc, o - k0);
+      // whole B1 (rows of orbitals [klo, khi)), or B1 of W and V recomputed
+      // for a chunk of occupied orbitals
+      const size_t kc = orbital_chunked
+                            ? std::max<size_t>(1, std::min(khi - klo, budget / 2 / per_k(s)))
+                            : khi - klo;
+      for (size_t k0 = klo; k0 < khi; k0 += kc) {
+        const size_t nk = std::min(kc, khi - k0);
         DevBuf B1w, B1v, Z(N * nk * MV);
         if (orbital_chunked) {
           b1_chunk(W, s, k0, nk, B1w);
           b1_chunk(V, s, k0, nk, B1v);
         }
-        const double* bw = orbital_chunked ? B1w.get() : XW.B1[s].get();
-        const double* bv = orbital_chunked ? B1v.get() : XV.B1[s].get();
-        gemm(gemm_nn(LL(N * nk), LL(MV), LL(MW), 1.0, bw, LL(N * nk), Y.get(), LL(MW), 0.0,
+        const double* bw = orbital_chunked ? B1w.get() : XW.B1[s].get() + N * k0;
+        const double* bv = orbital_chunked ? B1v.get() : XV.B1[s].get() + N * k0;
+        const size_t ldb1 = orbital_chunked ? N * nk : N * o;
+        gemm(gemm_nn(LL(N * nk), LL(MV), LL(MW), 1.0, bw, LL(ldb1), Y.get(), LL(MW), 0.0,
                      Z.get(), LL(N * nk)));
         // active orbitals (k >= c) weighted 2
         const size_t a0 = std::max(c, k0), a1 = k0 + nk;
@@ -998,6 +1066,13 @@ void form_fock(const FockRequest& rq) {
         GemmDesc gf = gemm_nn(LL(N), LL(N), LL(nk * MV), 1.0, Z.get(), LL(N), bv, LL(N), 1.0,
                               Fp[s].get(), LL(N));
         gf.b_ncontig = true;
+        if (ldb1 != N * nk) {
+          // part of the whole B1: K = (k, A) as MV reduction batches of nk
+          gf.k = LL(nk);
+          gf.nbr1 = LL(MV);
+          gf.sAr1 = LL(N * nk);
+          gf.sBr1 = LL(ldb1);
+        }
         gemm(gf);
       }
     }

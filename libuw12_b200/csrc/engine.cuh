@@ -100,6 +100,11 @@ struct FockRequest {
   double* terms = nullptr;          // host: {E2, E3, E4} or null
   size_t mem_budget = 0;            // bytes for chunked intermediates (0 = auto)
   size_t shard = 0, n_shards = 1;   // partial evaluation: this shard's share only
+  // Sum over the shards of a device buffer (in place, ordered on `stream`),
+  // called at the same points, with the same counts, on every shard; needed
+  // when n_shards > 1.  Returns 0 on success.
+  int (*allreduce)(double* data, size_t count, void* stream, void* user) = nullptr;
+  void* allreduce_user = nullptr;
 };
 
 void form_fock(const FockRequest& rq);

@@ -167,18 +167,30 @@ __device__ __forceinline__ void tile_k_offsets(const OperandView& v, long long k
   }
 }
 
+// Shared-memory tile of 32 rows x 128 k, unpadded, element (r, c) at
+// r * 128 + (c ^ ((c >> 4) & 7) ^ (r & 15)).  The swizzle stays inside each
+// 16-element group and is a bijection per row; every warp access of the
+// kernels below touches all 16 8-byte bank pairs exactly twice (two
+// wavefronts for 256 bytes, the minimum): the column fill of 32 rows at one k,
+// the row fill of 32 consecutive k, and the compute reads (16 lanes per row,
+// lane t at k = 8 t + q for one q).
+__device__ __forceinline__ int tile_at(int r, int c) {
+  return r * 128 + (c ^ ((c >> 4) & 7) ^ (r & 15));
+}
+
 // Loads the 32 x 128 tile (rows row0.., k k0..) of one plane, zeros outside,
 // reading along whichever of rows / k is contiguous in memory.
 template <bool KCONTIG>
 __device__ __forceinline__ void load_tile(const OperandView& v, int plane, long long row0,
-                                          const long long* koff, double (*tile)[129]) {
+                                          const long long* koff, double* tile) {
   const double* pb = v.base + (plane % v.np1) * v.po1 + (plane / v.np1) * v.po2;
+#pragma unroll 4
   for (int e = threadIdx.x; e < 32 * 128; e += 256) {
     const int r = KCONTIG ? (e >> 7) : (e & 31);
     const int c = KCONTIG ? (e & 127) : (e >> 5);
     const long long row = row0 + r;
     const long long ko = koff[c];
-    tile[r][c] = (row < v.rows && ko >= 0) ? pb[row * v.rs + ko] : 0.0;
+    tile[tile_at(r, c)] = (row < v.rows && ko >= 0) ? pb[row * v.rs + ko] : 0.0;
   }
 }
 
@@ -291,15 +303,19 @@ __device__ __forceinline__ uint32_t residue_low(int vl, double v, double inv_p, 
 
 // Tile of 32 rows x 128 k of one plane -> L residue rows per row: row r of
 // modulus l of a plane is out row ((plane * tiles + r / T) * L + l) * T + r % T
-// (T = tile_rows, the MMA tile height of this operand), each k_pad bytes;
-// zeros in padding.  The L residue rows of a tile are T * k_pad bytes apart.
-// Grid: (row tiles, k tiles, planes).
+// (T = 2^tile_log2, the MMA tile height of this operand; tiles = rows_pad / T),
+// each k_pad bytes; zeros in padding.  The L residue rows of a tile are
+// T * k_pad bytes apart.  Thread (row pair rr, rr + 16; lane t of 16) converts
+// the 8 consecutive k 8t .. 8t+7 of each of its rows and stores 8 residue bytes
+// per modulus (16 lanes: 128 contiguous bytes per row and modulus).  The
+// moduli loop is unrolled to kOzakiMaxModuli, so that p and 1/p are
+// immediate constant-bank operands.  Grid: (row tiles, k tiles, planes).
 template <bool KCONTIG>
 __global__ void __launch_bounds__(256) k_residues(OperandView v, const int* __restrict__ shift,
-                                                  ResidueMods mods, int tile_rows,
-                                                  long long rows_pad, long long k_pad,
+                                                  ResidueMods mods, int tile_log2,
+                                                  long long tiles, long long k_pad,
                                                   uint8_t* __restrict__ out) {
-  __shared__ double tile[32][129];
+  __shared__ __align__(16) double tile[32 * 128];
   __shared__ long long koff[128];
   const int plane = blockIdx.z;
   const long long row0 = static_cast<long long>(blockIdx.x) * 32;
@@ -308,50 +324,48 @@ __global__ void __launch_bounds__(256) k_residues(OperandView v, const int* __re
   __syncthreads();
   load_tile<KCONTIG>(v, plane, row0, koff, tile);
   __syncthreads();
-  const int tid = threadIdx.x;
-  const int c4 = (tid & 31) * 4;
-  // Each lane takes its 4 consecutive k in an order rotated by rot = (lane /
-  // 4) mod 4, so that the warp's reads of tile[r][c4 + ...] fall in 16
-  // distinct 8-byte bank pairs (two wavefronts, the minimum for 256 bytes);
-  // the packed residue word is rotated back before the store.
-  const int rot = ((tid & 31) >> 2) & 3;
-  const int q0 = c4 + (rot & 3), q1 = c4 + ((rot + 1) & 3), q2 = c4 + ((rot + 2) & 3),
-            q3 = c4 + ((rot + 3) & 3);
-  for (int it = 0; it < 4; ++it) {
-    const int r = it * 8 + tid / 32;
+  const int t = threadIdx.x & 15;
+  const long long tmask = (1LL << tile_log2) - 1;
+  const long long lstep = k_pad << tile_log2;  // next modulus of the same row
+#pragma unroll 1
+  for (int it = 0; it < 2; ++it) {
+    const int r = (threadIdx.x >> 4) + 16 * it;
     const long long row = row0 + r;
     const int sh = row < v.rows ? shift[plane * v.rows + row] : 0;
-    // row of modulus 0 in the residue layout ((plane * tiles + tile) * L + l) * tile_rows + r
-    const long long tile_base =
-        ((plane * (rows_pad / tile_rows) + row / tile_rows) * mods.L) * tile_rows + row % tile_rows;
-    double x0, x1, x2, x3;  // elements k0 + q0 .. q3
+    double x[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) x[q] = tile[tile_at(r, 8 * t + q)];
     if (sh > -1000 && sh < 1000) {  // 2^sh is a normal double: scale by one multiply
       const double sc = ldexp(1.0, sh);
-      x0 = round_int(tile[r][q0] * sc);
-      x1 = round_int(tile[r][q1] * sc);
-      x2 = round_int(tile[r][q2] * sc);
-      x3 = round_int(tile[r][q3] * sc);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) x[q] = round_int(x[q] * sc);
     } else {
-      x0 = round_int(ldexp(tile[r][q0], sh));
-      x1 = round_int(ldexp(tile[r][q1], sh));
-      x2 = round_int(ldexp(tile[r][q2], sh));
-      x3 = round_int(ldexp(tile[r][q3], sh));
+#pragma unroll
+      for (int q = 0; q < 8; ++q) x[q] = round_int(ldexp(x[q], sh));
     }
-    const int v0 = int_of(x0), v1 = int_of(x1), v2 = int_of(x2), v3 = int_of(x3);
-    uint8_t* dst = out + tile_base * k_pad + k0 + c4;
-    const long long lstep = static_cast<long long>(tile_rows) * k_pad;
-#pragma unroll 4
-    for (int l = 0; l < mods.L; ++l) {
-      const double ip = mods.inv_p[l];
-      const int p = mods.pi[l];
-      const uint32_t lo =
-          __byte_perm(residue_low(v0, x0, ip, p), residue_low(v1, x1, ip, p), 0x0040);
-      const uint32_t hi =
-          __byte_perm(residue_low(v2, x2, ip, p), residue_low(v3, x3, ip, p), 0x0040);
-      // byte i holds element (i + rot) mod 4: rotate left by rot bytes
-      const uint32_t w = __byte_perm(lo, hi, 0x5410);
-      *reinterpret_cast<uint32_t*>(dst) = __funnelshift_l(w, w, 8 * rot);
-      dst += lstep;
+    int vl[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) vl[q] = int_of(x[q]);
+    // row of modulus 0 in the residue layout
+    const long long base_row =
+        (((plane * tiles + (row >> tile_log2)) * mods.L) << tile_log2) + (row & tmask);
+    uint8_t* dst = out + base_row * k_pad + k0 + 8 * t;
+#pragma unroll
+    for (int l = 0; l < kOzakiMaxModuli; ++l) {
+      if (l < mods.L) {
+        const double ip = mods.inv_p[l];
+        const int p = mods.pi[l];
+        const uint32_t b01 =
+            __byte_perm(residue_low(vl[0], x[0], ip, p), residue_low(vl[1], x[1], ip, p), 0x0040);
+        const uint32_t b23 =
+            __byte_perm(residue_low(vl[2], x[2], ip, p), residue_low(vl[3], x[3], ip, p), 0x0040);
+        const uint32_t b45 =
+            __byte_perm(residue_low(vl[4], x[4], ip, p), residue_low(vl[5], x[5], ip, p), 0x0040);
+        const uint32_t b67 =
+            __byte_perm(residue_low(vl[6], x[6], ip, p), residue_low(vl[7], x[7], ip, p), 0x0040);
+        *reinterpret_cast<uint2*>(dst + l * lstep) =
+            make_uint2(__byte_perm(b01, b23, 0x5410), __byte_perm(b45, b67, 0x5410));
+      }
     }
   }
 }
@@ -1040,10 +1054,12 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
       k_exponent_to_shift<<<static_cast<unsigned>((nsh + 255) / 256), 256, 0, s>>>(ep, nsh, beta,
                                                                                   sh);
       UW12_LAUNCHED();
+      const int tlog = tile_rows == 256 ? 8 : 7;
+      const long long tiles = rows_pad / tile_rows;
       if (v.ks == 1)
-        k_residues<true><<<g, 256, 0, s>>>(v, sh, mods, tile_rows, rows_pad, k_pad, out);
+        k_residues<true><<<g, 256, 0, s>>>(v, sh, mods, tlog, tiles, k_pad, out);
       else
-        k_residues<false><<<g, 256, 0, s>>>(v, sh, mods, tile_rows, rows_pad, k_pad, out);
+        k_residues<false><<<g, 256, 0, s>>>(v, sh, mods, tlog, tiles, k_pad, out);
       UW12_LAUNCHED();
     };
     prep(va, planes_a, m_pad, kTileI, sa, ea, ra);
