@@ -410,6 +410,15 @@ def gemm_probe(args):
                                     "work_per_s": r["work"] / (r["ms"] / 1e3) if r["ms"] else None}
     L.profile_enable(False)
     out["speedup"] = out["fp64_ms"] / out[f"split{Lm}_ms"]
+    # accuracy of one split call against the FP64 kernel (same C on input)
+    C0 = torch.randn(m * n, dtype=torch.float64, device=device, generator=g)
+    C.copy_(C0)
+    L.dgemm(*gargs)
+    ref = C.clone()
+    C.copy_(C0)
+    L.dgemm_split(*gargs, n_moduli=Lm)
+    torch.cuda.synchronize(device)
+    out[f"split{Lm}_max_rel_err"] = float((C - ref).abs().max() / ref.abs().max())
     print(json.dumps(out), flush=True)
 
 

@@ -864,9 +864,13 @@ void form_fock(const FockRequest& rq) {
       copy3d(P.B1[s].get() + N * c, LL(N), LL(N * o), P.Wst[s].get(), LL(Rp), LL(Rp * a), LL(N),
              LL(a), LL(M));
       if (which == 1 || need_sv_w) {
+        // S^-1 Wst (R' x a M): this shard's aux columns, gathered by the sum
         P.SV[s].alloc(Rp * a * M);
-        gemm(gemm_nn(LL(Rp), LL(a * M), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp), P.Wst[s].get(),
-                     LL(Rp), 0.0, P.SV[s].get(), LL(Rp)));
+        if (sharded) P.SV[s].zero();
+        gemm(gemm_nn(LL(Rp), LL(a * (xhi - xlo)), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp),
+                     P.Wst[s].get() + Rp * a * xlo, LL(Rp), 0.0, P.SV[s].get() + Rp * a * xlo,
+                     LL(Rp)));
+        allreduce(P.SV[s].get(), Rp * a * M);
       }
     }
   }

@@ -373,13 +373,25 @@ __global__ void __launch_bounds__(256) k_residues(OperandView v, const int* __re
 // ---------------------------------------------------------------------------
 // tcgen05 int8 product kernel
 // ---------------------------------------------------------------------------
+// Work-item tile: kJHalves x 128 output columns j by 256 output rows i.  One
+// half: the two 256-column TMEM accumulators are double-buffered across items;
+// two halves: both accumulators belong to one item (two MMAs per K step share
+// the i operand), so each K step moves 64 KiB for twice the products.
+#ifndef UW12_I8_JHALVES
+#define UW12_I8_JHALVES 1
+#endif
+constexpr int kJHalves = UW12_I8_JHALVES;
+static_assert(kJHalves == 1 || kJHalves == 2, "one or two j halves per work item");
 constexpr int kTileJ = 128;  // MMA M (TMEM lanes): output columns j
+constexpr int kItemJ = kTileJ * kJHalves;  // output columns j per work item
 constexpr int kTileI = 256;  // MMA N (TMEM columns): output rows i
 constexpr int kTileK = 128;  // bytes of K per pipeline stage (one 128-byte swizzle row)
-constexpr int kBytesJ = kTileJ * kTileK;  // 16 KiB
+constexpr int kBytesJ = kItemJ * kTileK;  // 16 or 32 KiB
 constexpr int kBytesI = kTileI * kTileK;  // 32 KiB
 constexpr int kMmaK = 32;                 // K of one kind::i8 MMA
-constexpr int kThreads = 192;
+constexpr int kAccBufs = 2 / kJHalves;    // accumulator sets (2 x 256 TMEM columns in all)
+constexpr int kEpiWarps = 4 * kJHalves;   // one per TMEM lane quarter and j half
+constexpr int kThreads = 64 + 32 * kEpiWarps;
 constexpr unsigned long long kWaitLimitNs = 4000000000ULL;  // 4 s
 
 struct MmaArgs {
@@ -531,7 +543,7 @@ __device__ __forceinline__ WorkItem decode_item(const MmaArgs& a, long long w) {
   it.nkb = min(a.kb_per_split, a.kb_total - it.kb0);
   // residue rows: ((plane * tiles + tile) * L + l) * tile_rows + row in tile
   it.yj = static_cast<int>(
-      ((static_cast<long long>(pb) * (a.n_pad / kTileJ) + it.tj) * a.L + it.l) * kTileJ);
+      ((static_cast<long long>(pb) * (a.n_pad / kItemJ) + it.tj) * a.L + it.l) * kItemJ);
   it.yi = static_cast<int>(
       ((static_cast<long long>(pa) * (a.m_pad / kTileI) + it.ti) * a.L + it.l) * kTileI);
   return it;
@@ -542,8 +554,9 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 }
 
 // Persistent: one CTA per SM walks the work items blockIdx.x, + gridDim.x, ...
-// through a STAGES-deep TMA ring; two TMEM accumulators (2 x 256 columns) let
-// the epilogue of one item overlap the MMAs of the next.
+// through a STAGES-deep TMA ring; with one j half per item the two TMEM
+// accumulators (2 x 256 columns) let the epilogue of one item overlap the MMAs
+// of the next, with two halves they hold the item's two halves.
 template <int STAGES>
 __global__ void __launch_bounds__(kThreads, 1)
     k_i8_mma(const __grid_constant__ CUtensorMap tm_j, const __grid_constant__ CUtensorMap tm_i,
@@ -551,7 +564,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                              ~static_cast<uintptr_t>(1023));
-  uint8_t* sj = base;                            // STAGES x 16 KiB
+  uint8_t* sj = base;                            // STAGES x kBytesJ
   uint8_t* si = base + STAGES * kBytesJ;         // STAGES x 32 KiB
   uint64_t* bars = reinterpret_cast<uint64_t*>(si + STAGES * kBytesI);
   uint64_t* full = bars;
@@ -569,7 +582,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(smem_u32(&acc_full[b]), 1);
-      mbar_init(smem_u32(&acc_empty[b]), 4);  // one arrival per epilogue warp
+      mbar_init(smem_u32(&acc_empty[b]), kEpiWarps);  // one arrival per epilogue warp
     }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -621,11 +634,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint32_t last_use = 0;
     for (long long w = blockIdx.x; w < a.n_items; w += gridDim.x, ++t) {
       const WorkItem it = decode_item(a, w);
-      const int buf = t & 1;
-      const uint32_t use = static_cast<uint32_t>(t >> 1);
+      const int buf = t % kAccBufs;
+      const uint32_t use = static_cast<uint32_t>(t / kAccBufs);
       if (!mbar_wait(smem_u32(&acc_empty[buf]), (use & 1) ^ 1, abort_flag, a.err, 2)) break;
       tc_fence_after();
-      const uint32_t d = tmem + static_cast<uint32_t>(buf * kTileI);
+      const uint32_t d = tmem + static_cast<uint32_t>(buf * kJHalves * kTileI);
       bool ok = true;
       for (int kb = 0; kb < it.nkb; ++kb) {
         const int s = static_cast<int>(pos % STAGES);
@@ -635,13 +648,18 @@ __global__ void __launch_bounds__(kThreads, 1)
           break;
         }
         tc_fence_after();
-        const uint64_t dj = sw128_desc(smem_u32(sj + s * kBytesJ));
         const uint64_t di = sw128_desc(smem_u32(si + s * kBytesI));
 #pragma unroll
-        for (int kk = 0; kk < kTileK / kMmaK; ++kk) {
-          // advance along K inside the swizzle row: +32 bytes = +2 in the
-          // 16-byte address field
-          mma_i8(d, dj + 2 * kk, di + 2 * kk, (kb | kk) != 0);
+        for (int h = 0; h < kJHalves; ++h) {
+          // j half h: rows 128 h .. of the stage, accumulator columns 256 h ..
+          const uint64_t dj = sw128_desc(smem_u32(sj + s * kBytesJ + h * kTileJ * kTileK));
+#pragma unroll
+          for (int kk = 0; kk < kTileK / kMmaK; ++kk) {
+            // advance along K inside the swizzle row: +32 bytes = +2 in the
+            // 16-byte address field
+            mma_i8(d + static_cast<uint32_t>(h * kTileI), dj + 2 * kk, di + 2 * kk,
+                   (kb | kk) != 0);
+          }
         }
         mma_commit(smem_u32(&empty[s]));
         ++pos;
@@ -655,22 +673,23 @@ __global__ void __launch_bounds__(kThreads, 1)
       (void)mbar_wait(smem_u32(&acc_full[last_buf]), last_use & 1, abort_flag, a.err, 4);
   } else if (warp >= 2) {
     // ---- epilogue: TMEM -> residues mod p -> uint8 rows
-    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    const int q = warp & 3;          // TMEM lane quarter this warp may access
+    const int h = (warp - 2) / 4;    // j half
     int t = 0;
     for (long long w = blockIdx.x; w < a.n_items; w += gridDim.x, ++t) {
       const WorkItem it = decode_item(a, w);
-      const int buf = t & 1;
-      const uint32_t use = static_cast<uint32_t>(t >> 1);
+      const int buf = t % kAccBufs;
+      const uint32_t use = static_cast<uint32_t>(t / kAccBufs);
       // warp-uniform, so that the .sync.aligned TMEM loads below are convergent
       const bool ok =
           __all_sync(0xffffffffu, mbar_wait(smem_u32(&acc_full[buf]), use & 1, abort_flag, a.err, 3));
       tc_fence_after();
       if (!ok) break;
       const uint32_t p = a.p[it.l], bm = a.barrett[it.l], off = a.off[it.l];
-      const long long j = static_cast<long long>(it.tj) * kTileJ + q * 32 + lane;
+      const long long j = static_cast<long long>(it.tj) * kItemJ + h * kTileJ + q * 32 + lane;
       uint8_t* rowp = a.R + residue_offset(a, it.split, it.b, j, it.l) +
                       static_cast<long long>(it.ti) * kTileI;
-      const uint32_t tq = tmem + static_cast<uint32_t>(buf * kTileI) +
+      const uint32_t tq = tmem + static_cast<uint32_t>((buf * kJHalves + h) * kTileI) +
                           (static_cast<uint32_t>(q * 32) << 16);
 #pragma unroll 1
       for (int c = 0; c < kTileI / 32; ++c) {
@@ -729,12 +748,13 @@ struct CrtArgs {
   int c_aligned;   // C, ldc and the batch strides allow 16-byte accesses
 };
 
-// One thread = 4 consecutive rows i of a column j of one batch; grid (row
-// blocks of 1024, columns strided by gridDim.y, batches).  The L residue words
-// of a column (and the 4 elements of C when beta != 0) are loaded before any
-// is used (one load per modulus and K chunk in flight per thread), the K-chunk
-// sums of the 4 bytes are kept as pairs of 16-bit lanes, the CRT runs on NCH
-// chunks of cw bits, and C is read and written 16 bytes at a time when aligned.
+// One thread = E (kCrtElems) consecutive rows i of a column j of one batch;
+// grid (row blocks of 256 E, columns strided by gridDim.y, batches).  The L
+// residue words of a column (and the E elements of C when beta != 0) are
+// loaded before any is used (one load per modulus and K chunk in flight per
+// thread), the K-chunk sums of the E bytes are kept as pairs of 16-bit lanes,
+// the CRT runs on NCH chunks of cw bits, and C is read and written 16 bytes at
+// a time when aligned.
 // x 2^e: one multiply by an exactly representable power of two when 2^e is a
 // normal double, ldexp otherwise.
 __device__ __forceinline__ double scale_pow2(double x, int e) {
@@ -787,11 +807,27 @@ __device__ __forceinline__ double small_to_double(uint32_t r) {
   return __dsub_rn(__hiloint2double(0x43300000, static_cast<int>(r)), 4503599627370496.0);
 }
 
+// Rows i per CRT thread: 4 (one 32-bit residue word per modulus) or 2 (one
+// 16-bit word; fewer registers, more resident warps).
+#ifndef UW12_CRT_ELEMS
+#define UW12_CRT_ELEMS 4
+#endif
+constexpr int kCrtElems = UW12_CRT_ELEMS;
+static_assert(kCrtElems == 2 || kCrtElems == 4, "2 or 4 rows per CRT thread");
+constexpr int kCrtMinBlocks = kCrtElems == 4 ? 3 : 4;
+
+template <int E>
+__device__ __forceinline__ uint32_t load_residues(const uint8_t* p) {
+  if (E == 4) return __ldg(reinterpret_cast<const uint32_t*>(p));
+  return __ldg(reinterpret_cast<const unsigned short*>(p));
+}
+
 // REDUCE: several K chunks, whose residue sums are reduced mod p; with one K
 // chunk the stored residues (already in [0, p)) enter the CRT sum directly.
 template <int NCH, bool REDUCE>
-__global__ void __launch_bounds__(256, REDUCE ? 2 : 3) k_crt(const CrtArgs a) {
-  const long long i0 = (static_cast<long long>(blockIdx.x) * 256 + threadIdx.x) * 4;
+__global__ void __launch_bounds__(256, REDUCE ? 2 : kCrtMinBlocks) k_crt(const CrtArgs a) {
+  constexpr int E = kCrtElems;
+  const long long i0 = (static_cast<long long>(blockIdx.x) * 256 + threadIdx.x) * E;
   if (i0 >= a.m) return;
   const int b = blockIdx.z;
   const int b1 = b % a.nbo1, b2 = b / a.nbo1;
@@ -800,37 +836,42 @@ __global__ void __launch_bounds__(256, REDUCE ? 2 : 3) k_crt(const CrtArgs a) {
   // residue layout of k_i8_mma: (((split * nbatch + b) * n_pad + j) * L + l) * m_pad + i
   const long long lstride = a.m_pad;                                             // next modulus
   const long long sstride = static_cast<long long>(a.nbatch) * a.n_pad * a.L * a.m_pad;  // K chunk
-  int sa[4];
+  int sa[E];
 #pragma unroll
-  for (int e = 0; e < 4; ++e)
+  for (int e = 0; e < E; ++e)
     sa[e] = i0 + e < a.m ? a.shift_a[pa * a.rows_a + i0 + e] : 0;
   const double chunk = __longlong_as_double(static_cast<long long>(a.cw + 1023) << 52);  // 2^cw
 
-  const bool vec = i0 + 3 < a.m && a.c_aligned;
+  const bool vec = i0 + E - 1 < a.m && a.c_aligned;
   for (long long j = blockIdx.y; j < a.n; j += gridDim.y) {
     const uint8_t* base = a.R + (static_cast<long long>(b) * a.n_pad + j) * a.L * a.m_pad + i0;
     double* Cb = a.C + b1 * a.sCo1 + b2 * a.sCo2 + j * a.ldc;
-    // one residue word (4 rows) per modulus and K chunk, and the 4 elements of
+    // one residue word (E rows) per modulus and K chunk, and the E elements of
     // C when they are accumulated into: all loads issued first
     uint32_t w0[kOzakiMaxModuli];
 #pragma unroll
     for (int l = 0; l < kOzakiMaxModuli; ++l)
-      if (l < a.L) w0[l] = __ldg(reinterpret_cast<const uint32_t*>(base + l * lstride));
-    double cold[4] = {0.0, 0.0, 0.0, 0.0};
+      if (l < a.L) w0[l] = load_residues<E>(base + l * lstride);
+    double cold[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) cold[e] = 0.0;
     if (a.beta != 0.0) {
       if (vec) {
-        const double2 c01 = *reinterpret_cast<const double2*>(Cb + i0);
-        const double2 c23 = *reinterpret_cast<const double2*>(Cb + i0 + 2);
-        cold[0] = c01.x; cold[1] = c01.y; cold[2] = c23.x; cold[3] = c23.y;
+#pragma unroll
+        for (int e = 0; e < E; e += 2) {
+          const double2 c2 = *reinterpret_cast<const double2*>(Cb + i0 + e);
+          cold[e] = c2.x;
+          cold[e + 1] = c2.y;
+        }
       } else {
 #pragma unroll
-        for (int e = 0; e < 4; ++e)
+        for (int e = 0; e < E; ++e)
           if (i0 + e < a.m) cold[e] = Cb[i0 + e];
       }
     }
-    double S[4][NCH];
+    double S[E][NCH];
 #pragma unroll
-    for (int e = 0; e < 4; ++e)
+    for (int e = 0; e < E; ++e)
 #pragma unroll
       for (int c = 0; c < NCH; ++c) S[e][c] = 0.0;
     if (!REDUCE) {
@@ -839,7 +880,7 @@ __global__ void __launch_bounds__(256, REDUCE ? 2 : 3) k_crt(const CrtArgs a) {
       for (int l = 0; l < kOzakiMaxModuli; ++l) {
         if (l < a.L) {
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
+          for (int e = 0; e < E; ++e) {
             const double r = byte_to_double(w0[l], e);
 #pragma unroll
             for (int c = 0; c < NCH; ++c) S[e][c] = fma(r, a.w[l][c], S[e][c]);
@@ -860,8 +901,7 @@ __global__ void __launch_bounds__(256, REDUCE ? 2 : 3) k_crt(const CrtArgs a) {
 #pragma unroll
         for (int l = 0; l < kOzakiMaxModuli; ++l) {
           if (l < a.L) {
-            const uint32_t w =
-                __ldg(reinterpret_cast<const uint32_t*>(base + sp * sstride + l * lstride));
+            const uint32_t w = load_residues<E>(base + sp * sstride + l * lstride);
             s02[l] += w & 0x00ff00ffu;
             s13[l] += (w >> 8) & 0x00ff00ffu;
           }
@@ -873,7 +913,7 @@ __global__ void __launch_bounds__(256, REDUCE ? 2 : 3) k_crt(const CrtArgs a) {
           const uint32_t p = a.p[l], bm = a.barrett[l];
           const uint32_t u[4] = {s02[l] & 0xffffu, s13[l] & 0xffffu, s02[l] >> 16, s13[l] >> 16};
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
+          for (int e = 0; e < E; ++e) {
             const double r = small_to_double(mod_u32(u[e], p, bm));
 #pragma unroll
             for (int c = 0; c < NCH; ++c) S[e][c] = fma(r, a.w[l][c], S[e][c]);
@@ -882,9 +922,9 @@ __global__ void __launch_bounds__(256, REDUCE ? 2 : 3) k_crt(const CrtArgs a) {
       }
     }
     const int sb = a.shift_b[pb * a.rows_b + j];
-    double out[4];
+    double out[E];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
+    for (int e = 0; e < E; ++e) {
       double approx = 0.0;
 #pragma unroll
       for (int c = NCH - 1; c >= 0; --c) approx = fma(approx, chunk, S[e][c]);
@@ -896,11 +936,12 @@ __global__ void __launch_bounds__(256, REDUCE ? 2 : 3) k_crt(const CrtArgs a) {
       if (a.beta != 0.0) out[e] = fma(a.beta, cold[e], out[e]);
     }
     if (vec) {
-      *reinterpret_cast<double2*>(Cb + i0) = make_double2(out[0], out[1]);
-      *reinterpret_cast<double2*>(Cb + i0 + 2) = make_double2(out[2], out[3]);
+#pragma unroll
+      for (int e = 0; e < E; e += 2)
+        *reinterpret_cast<double2*>(Cb + i0 + e) = make_double2(out[e], out[e + 1]);
     } else {
 #pragma unroll
-      for (int e = 0; e < 4; ++e)
+      for (int e = 0; e < E; ++e)
         if (i0 + e < a.m) Cb[i0 + e] = out[e];
     }
   }
@@ -945,7 +986,7 @@ CUtensorMap make_map(const uint8_t* base, long long rows, long long k_pad, int b
   return m;
 }
 
-constexpr int kStages = 4;  // 192 KiB of stages: one persistent CTA per SM, 512 TMEM columns
+constexpr int kStages = 4 / kJHalves + (kJHalves - 1);  // 4 x 48 or 3 x 64 KiB of stages
 constexpr size_t kMmaSmem =
     size_t(kStages) * (kBytesJ + kBytesI) + 1024 /*alignment*/ + 256 /*barriers*/;
 
@@ -987,7 +1028,7 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
   const long long nbo1 = d.nbo1, nbo2 = d.nbo2, nbatch = nbo1 * nbo2;
   const long long k_total = d.k * d.nbr1 * d.nbr2;
   const long long k_pad = round_up(k_total, kTileK);
-  const long long m_pad = round_up(d.m, kTileI), n_pad = round_up(d.n, kTileJ);
+  const long long m_pad = round_up(d.m, kTileI), n_pad = round_up(d.n, kItemJ);
   const int a_var1 = d.sAo1 != 0 && nbo1 > 1, a_var2 = d.sAo2 != 0 && nbo2 > 1;
   const int b_var1 = d.sBo1 != 0 && nbo1 > 1, b_var2 = d.sBo2 != 0 && nbo2 > 1;
   const int pa1 = a_var1 ? int(nbo1) : 1, pa2 = a_var2 ? int(nbo2) : 1;
@@ -997,7 +1038,7 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
   // K chunks: <= kMaxKChunk bytes each; more chunks when the tile grid alone
   // would leave SMs idle.
   const long long kb_total = k_pad / kTileK;
-  const long long tiles_j = n_pad / kTileJ, tiles_i = m_pad / kTileI;
+  const long long tiles_j = n_pad / kItemJ, tiles_i = m_pad / kTileI;
   const long long ctas = tiles_j * tiles_i * L * nbatch;
   long long splits = (k_pad + kMaxKChunk - 1) / kMaxKChunk;
   const long long want = (2 * num_sms() + ctas - 1) / ctas;
@@ -1063,7 +1104,7 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
       UW12_LAUNCHED();
     };
     prep(va, planes_a, m_pad, kTileI, sa, ea, ra);
-    prep(vb, planes_b, n_pad, kTileJ, sb, eb, rb);
+    prep(vb, planes_b, n_pad, kItemJ, sb, eb, rb);
     tm.stop();
   }
 
@@ -1082,7 +1123,7 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
         attr_set[dev] = true;
       }
     }
-    const CUtensorMap tmj = make_map(rb, L * planes_b * n_pad, k_pad, kTileJ);
+    const CUtensorMap tmj = make_map(rb, L * planes_b * n_pad, k_pad, kItemJ);
     const CUtensorMap tmi = make_map(ra, L * planes_a * m_pad, k_pad, kTileI);
     MmaArgs ma{};
     ma.tiles_j = static_cast<int>(tiles_j);
@@ -1145,7 +1186,7 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
     const double bytes = double(splits * L) * double(d.m * d.n * nbatch) +
                          8.0 * double(d.m * d.n * nbatch) * (d.beta != 0.0 ? 2.0 : 1.0);
     Timer tm(kProfSplitCrt, bytes, "crt", s);
-    const dim3 g(static_cast<unsigned>((d.m + 1023) / 1024),
+    const dim3 g(static_cast<unsigned>((d.m + 256 * kCrtElems - 1) / (256 * kCrtElems)),
                  static_cast<unsigned>(std::min<long long>(d.n, 65535)),
                  static_cast<unsigned>(nbatch));
     const bool reduce = splits > 1;
@@ -1167,7 +1208,7 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
 long long slab_bytes(long long L, long long m, long long n, long long k_total, long long nbatch,
                      long long planes_a, long long planes_b) {
   const long long k_pad = round_up(k_total, kTileK);
-  const long long m_pad = round_up(m, kTileI), n_pad = round_up(n, kTileJ);
+  const long long m_pad = round_up(m, kTileI), n_pad = round_up(n, kItemJ);
   const long long splits = std::max<long long>(1, (k_pad + kMaxKChunk - 1) / kMaxKChunk);
   return L * (planes_a * m_pad + planes_b * n_pad) * k_pad +
          std::max<long long>(splits, 4) * L * nbatch * m_pad * n_pad;
@@ -1220,7 +1261,7 @@ void run_slabs(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
   // first); row / column slabs would prepare each operand once per slab of
   // the other.  A large output is cut into row / column slabs instead (each
   // K range would reconstruct all of it).
-  const long long m_pad = round_up(d.m, kTileI), n_pad = round_up(d.n, kTileJ);
+  const long long m_pad = round_up(d.m, kTileI), n_pad = round_up(d.n, kItemJ);
   const long long op_bytes = L * (pa * m_pad + pb * n_pad) * round_up(k_total, kTileK);
   const long long out_bytes = 4 * L * nbatch * m_pad * n_pad;
   if (op_bytes > kSlabBudget / 2 && out_bytes <= kSlabBudget / 2 && k_total > kTileK) {
@@ -1267,8 +1308,8 @@ void run_slabs(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
   while (slab_bytes(L, ms, ns, k_total, nbatch, pa, pb) > kSlabBudget) {
     if (ms >= ns && ms > kTileI)
       ms = round_up(ms / 2, kTileI);
-    else if (ns > kTileJ)
-      ns = round_up(ns / 2, kTileJ);
+    else if (ns > kItemJ)
+      ns = round_up(ns / 2, kItemJ);
     else
       break;
   }

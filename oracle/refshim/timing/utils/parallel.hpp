@@ -16,11 +16,14 @@
 //     iterations (T = OpenMP threads) runs r x T evenly spaced iterations,
 //     r per thread, all threads at once, and adds the extrapolated time of the
 //     rest to extra_seconds. The reference's OpenMP schedule gives each thread
-//     a contiguous block of ceil(n / T) iterations (two-index loops: ceil(n1 /
-//     T) outer iterations of n2 inner ones each), so the whole loop takes
-//     ceil(n / T) (resp. ceil(n1 / T) * n2) iteration times with every thread
-//     busy; the sample measures r such iteration times under the same memory
-//     contention. Loop results are then partial sums; only the time is used.
+//     a contiguous block of n / T or n / T + 1 iterations (two-index loops:
+//     outer iterations of n2 inner ones each), so the whole loop takes
+//     floor(n / T) rounds with every thread busy and, when T does not divide
+//     n, one round with n mod T threads busy (two-index: floor(n1 / T) n2 and
+//     n2 rounds).  The sample measures r full rounds under the same memory
+//     contention, and the partial round by running n mod T iterations at once
+//     (fewer busy threads contend less, so a partial round is faster than a
+//     full one).  Loop results are then partial sums; only the time is used.
 //   * rotation (rotation = S > 0, with sampling): the sampled loops of an
 //     evaluation are numbered in the order they run; loop q is measured (as
 //     above) only when q % S == phase and otherwise skipped, its estimate
@@ -74,13 +77,15 @@ inline std::vector<size_t> spaced(size_t n, size_t k) {
   return idx;
 }
 
-// Runs body(slot, item) for every sampled item, r per thread, and books the
-// extrapolated remainder: the full loop takes `rounds_full` iteration times,
-// the sample took r of them. Under rotation a loop not due for measurement
-// runs no iteration and books its cached estimate.
+// Runs body(slot, item) for every sampled item, r per thread, then the
+// partial-round items at once, and books the extrapolated remainder: the full
+// loop takes `rounds_full` rounds with every thread busy (the sample ran r)
+// and `rounds_part` rounds with part.size() threads busy (the sample ran one).
+// Under rotation a loop not due for measurement runs no iteration and books
+// its cached estimate.
 template <typename Body>
 void run_sample(const std::vector<size_t>& items, size_t r, double rounds_full,
-                Body&& body) {
+                const std::vector<size_t>& part, double rounds_part, Body&& body) {
   const long q_loop = loop_index++;
   if (cached.size() <= static_cast<size_t>(q_loop)) cached.resize(q_loop + 1, -1.0);
   if (rotation > 0 && q_loop % rotation != phase && cached[q_loop] >= 0.0) {
@@ -91,10 +96,17 @@ void run_sample(const std::vector<size_t>& items, size_t r, double rounds_full,
 #pragma omp parallel for schedule(static, 1)
   for (long q = 0; q < static_cast<long>(items.size()); ++q)
     body(static_cast<size_t>(q), items[static_cast<size_t>(q)]);
-  const double dt = omp_get_wtime() - t0;
-  const double estimate = dt * rounds_full / static_cast<double>(r);
+  const double t1 = omp_get_wtime();
+  if (!part.empty()) {
+#pragma omp parallel for schedule(static, 1)
+    for (long q = 0; q < static_cast<long>(part.size()); ++q)
+      body(static_cast<size_t>(q), part[static_cast<size_t>(q)]);
+  }
+  const double t2 = omp_get_wtime();
+  const double estimate =
+      (t1 - t0) * rounds_full / static_cast<double>(r) + (t2 - t1) * rounds_part;
   cached[q_loop] = estimate;
-  extra_seconds += estimate - dt;
+  extra_seconds += estimate - (t2 - t0);
   ++sampled_loops;
   loop_log.push_back({items.size(), 1, estimate});
 }
@@ -120,8 +132,8 @@ inline void parallel_for(size_t start, size_t stop,
   if (ts::sampling_applies(n, parallel)) {
     const size_t T = static_cast<size_t>(omp_get_max_threads());
     const size_t r = static_cast<size_t>(ts::sample_rounds);
-    ts::run_sample(ts::spaced(n, r * T), r,
-                   static_cast<double>(ts::ceil_div(n, T)),
+    ts::run_sample(ts::spaced(n, r * T), r, static_cast<double>(n / T),
+                   ts::spaced(n, n % T), 1.0,
                    [&](size_t, size_t i) { func(start + i); });
     return;
   }
@@ -175,7 +187,7 @@ ReturnType parallel_sum(const size_t start, const size_t stop,
     const size_t r = static_cast<size_t>(ts::sample_rounds);
     const auto items = ts::spaced(n, r * T);
     std::vector<ReturnType> part(items.size(), identity);
-    ts::run_sample(items, r, static_cast<double>(ts::ceil_div(n, T)),
+    ts::run_sample(items, r, static_cast<double>(n / T), ts::spaced(n, n % T), 1.0,
                    [&](size_t q, size_t i) { part[q] += func(start + i); });
     return part[0];
   }
@@ -197,8 +209,12 @@ ReturnType parallel_sum_2d(
     const size_t r = static_cast<size_t>(ts::sample_rounds);
     const auto items = ts::spaced(n1 * n2, r * T);
     std::vector<ReturnType> part(items.size(), identity);
-    ts::run_sample(items, r, static_cast<double>(ts::ceil_div(n1, T) * n2),
-                   [&](size_t q, size_t p) {
+    // partial round: n1 mod T threads, one inner item each (outer iterations
+    // evenly spaced)
+    std::vector<size_t> rem;
+    for (size_t i : ts::spaced(n1, n1 % T)) rem.push_back(i * n2 + n2 / 2);
+    ts::run_sample(items, r, static_cast<double>((n1 / T) * n2), rem,
+                   static_cast<double>(n2), [&](size_t q, size_t p) {
                      part[q] += func(start1 + p / n2, start2 + p % n2);
                    });
     return part[0];

@@ -7,7 +7,8 @@ One shard of ``n_shards`` evaluates the partition the CUDA engine uses
   the fitted densities X_D of WV (partial J3_0[:, A]^T d, summed over the
   shards), the 2-el Fock (J3_0[:, A] u, partial), the MO transforms of W, V
   and WV (B1 = H[:, A] P2[A, :] and the stacked RI rows, partial products
-  summed over the shards) and the t~ dX Fock term (W's aux functions);
+  summed over the shards; S^-1 Wst over the shard's aux columns, gathered by
+  the same sum) and the t~ dX Fock term (W's aux functions);
 * occupied orbitals, ``part(n)``: X_AB and t (partial sums over rows of
   orbitals j / k, summed over the shards), the direct Fock, the same-spin
   three-electron energy and Fock (orbital k of the (j, k) pairs);
@@ -115,8 +116,11 @@ def form_fock_shard(W, V, WV, Sinv, orbitals, occ, n_active, indirect, s_os, s_s
             st3 = st.reshape((Rp, a, M), order='F')
             st3[:N] = b1.reshape((N, o, M), order='F')[:, c:, :]
             Wp[nm, s] = st3.reshape((Rp * a, M), order='F')
-            SVp[nm, s] = (Sinv @ Wp[nm, s].reshape(Rp, a * M, order='F')).reshape(
-                Rp * a, M, order='F')
+            # S^-1 Wst over this shard's aux columns, gathered by the sum
+            sv = np.zeros((Rp, a * M))
+            sv[:, a * lo:a * hi] = Sinv @ Wp[nm, s].reshape(Rp, a * M, order='F')[:, a * lo:a * hi]
+            allreduce(sv)
+            SVp[nm, s] = sv.reshape(Rp * a, M, order='F')
 
     # ---- X_AB and t over this shard's orbitals, summed
     lw, lv = W.df_vals, V.df_vals
