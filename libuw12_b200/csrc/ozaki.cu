@@ -179,19 +179,29 @@ __device__ __forceinline__ int tile_at(int r, int c) {
 }
 
 // Loads the 32 x 128 tile (rows row0.., k k0..) of one plane, zeros outside,
-// reading along whichever of rows / k is contiguous in memory.
+// reading along whichever of rows / k is contiguous in memory: 16 asynchronous
+// 8-byte copies per thread, all in flight at once (a copy of 0 source bytes
+// writes a zero), then waits for them.
 template <bool KCONTIG>
 __device__ __forceinline__ void load_tile(const OperandView& v, int plane, long long row0,
                                           const long long* koff, double* tile) {
   const double* pb = v.base + (plane % v.np1) * v.po1 + (plane / v.np1) * v.po2;
-#pragma unroll 4
-  for (int e = threadIdx.x; e < 32 * 128; e += 256) {
+#pragma unroll
+  for (int it = 0; it < 16; ++it) {
+    const int e = threadIdx.x + 256 * it;
     const int r = KCONTIG ? (e >> 7) : (e & 31);
     const int c = KCONTIG ? (e & 127) : (e >> 5);
     const long long row = row0 + r;
     const long long ko = koff[c];
-    tile[tile_at(r, c)] = (row < v.rows && ko >= 0) ? pb[row * v.rs + ko] : 0.0;
+    const bool in = row < v.rows && ko >= 0;
+    const double* src = in ? pb + row * v.rs + ko : pb;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(
+                     static_cast<unsigned>(__cvta_generic_to_shared(&tile[tile_at(r, c)]))),
+                 "l"(src), "r"(in ? 8 : 0)
+                 : "memory");
   }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
 // Per row: exponent e of its largest element (2^(e-1) <= max|x| < 2^e),
@@ -947,6 +957,124 @@ __global__ void __launch_bounds__(256, REDUCE ? 2 : kCrtMinBlocks) k_crt(const C
   }
 }
 
+// One K chunk, pipelined: a block owns 1024 rows i of a batch and walks its
+// columns j = blockIdx.y, + gridDim.y, ...; the L residue rows of the next
+// kCrtStages - 1 columns are copied into shared memory (16-byte cp.async.cg,
+// L x 1024 bytes per column) while the current one is reconstructed, so the
+// copies of a block stay in flight during its FP64 work.  Thread = 4 rows, as
+// in k_crt; the same arithmetic.
+constexpr int kCrtStages = 3;
+constexpr int kCrtRows = 1024;  // rows i per block
+
+template <int NCH>
+__global__ void __launch_bounds__(256, 3) k_crt_pipe(const CrtArgs a) {
+  extern __shared__ __align__(16) uint8_t crt_smem[];  // kCrtStages x L x kCrtRows bytes
+  const int L = a.L;
+  const long long iblk = static_cast<long long>(blockIdx.x) * kCrtRows;
+  const long long i0 = iblk + threadIdx.x * 4;
+  const int b = blockIdx.z;
+  const int b1 = b % a.nbo1, b2 = b / a.nbo1;
+  const int pa = (a.a_var1 ? b1 : 0) + (a.a_var1 ? a.nbo1 : 1) * (a.a_var2 ? b2 : 0);
+  const int pb = (a.b_var1 ? b1 : 0) + (a.b_var1 ? a.nbo1 : 1) * (a.b_var2 ? b2 : 0);
+  // bytes of this block's rows inside one residue row (a multiple of 256)
+  const long long row_bytes = min(static_cast<long long>(kCrtRows), a.m_pad - iblk);
+  const long long nj = (a.n - blockIdx.y + gridDim.y - 1) / gridDim.y;
+  const bool active = i0 < a.m;
+  int sa[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e)
+    sa[e] = i0 + e < a.m ? a.shift_a[pa * a.rows_a + i0 + e] : 0;
+  const double chunk = __longlong_as_double(static_cast<long long>(a.cw + 1023) << 52);  // 2^cw
+  const bool vec = i0 + 3 < a.m && a.c_aligned;
+
+  auto issue = [&](long long q, int slot) {
+    const long long j = blockIdx.y + q * gridDim.y;
+    const uint8_t* src0 = a.R + (static_cast<long long>(b) * a.n_pad + j) * L * a.m_pad + iblk;
+    uint8_t* dst0 = crt_smem + slot * L * kCrtRows;
+    for (int c = threadIdx.x; c < L * (kCrtRows / 16); c += 256) {
+      const int l = c / (kCrtRows / 16);
+      const int off = (c % (kCrtRows / 16)) * 16;
+      const bool in = off < row_bytes;
+      const uint8_t* src = in ? src0 + l * a.m_pad + off : src0;
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(
+                       static_cast<unsigned>(__cvta_generic_to_shared(dst0 + l * kCrtRows + off))),
+                   "l"(src), "r"(in ? 16 : 0)
+                   : "memory");
+    }
+  };
+
+#pragma unroll
+  for (int q = 0; q < kCrtStages - 1; ++q) {
+    if (q < nj) issue(q, q);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
+  for (long long q = 0; q < nj; ++q) {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(kCrtStages - 2) : "memory");
+    __syncthreads();  // column q landed; the slot refilled below is no longer read
+    {
+      const long long qn = q + kCrtStages - 1;
+      if (qn < nj) issue(qn, static_cast<int>(qn % kCrtStages));
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    if (!active) continue;
+    const long long j = blockIdx.y + q * gridDim.y;
+    const uint8_t* rs = crt_smem + static_cast<int>(q % kCrtStages) * L * kCrtRows + threadIdx.x * 4;
+    double* Cb = a.C + b1 * a.sCo1 + b2 * a.sCo2 + j * a.ldc;
+    double cold[4] = {0.0, 0.0, 0.0, 0.0};
+    if (a.beta != 0.0) {
+      if (vec) {
+        const double2 c01 = *reinterpret_cast<const double2*>(Cb + i0);
+        const double2 c23 = *reinterpret_cast<const double2*>(Cb + i0 + 2);
+        cold[0] = c01.x; cold[1] = c01.y; cold[2] = c23.x; cold[3] = c23.y;
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (i0 + e < a.m) cold[e] = Cb[i0 + e];
+      }
+    }
+    double S[4][NCH];
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+#pragma unroll
+      for (int c = 0; c < NCH; ++c) S[e][c] = 0.0;
+#pragma unroll
+    for (int l = 0; l < kOzakiMaxModuli; ++l) {
+      if (l < L) {
+        const uint32_t w = *reinterpret_cast<const uint32_t*>(rs + l * kCrtRows);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const double r = byte_to_double(w, e);
+#pragma unroll
+          for (int c = 0; c < NCH; ++c) S[e][c] = fma(r, a.w[l][c], S[e][c]);
+        }
+      }
+    }
+    const int sb = a.shift_b[pb * a.rows_b + j];
+    double out[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      double approx = 0.0;
+#pragma unroll
+      for (int c = NCH - 1; c >= 0; --c) approx = fma(approx, chunk, S[e][c]);
+      const double qq = round_int(approx * a.inv_m);  // |q| < 2^13
+      double dig[NCH];
+#pragma unroll
+      for (int c = 0; c < NCH; ++c) dig[c] = fma(-qq, a.mc[c], S[e][c]);  // exact
+      out[e] = a.alpha * scale_pow2(join_chunks<NCH>(dig, chunk), -(sa[e] + sb));
+      if (a.beta != 0.0) out[e] = fma(a.beta, cold[e], out[e]);
+    }
+    if (vec) {
+      *reinterpret_cast<double2*>(Cb + i0) = make_double2(out[0], out[1]);
+      *reinterpret_cast<double2*>(Cb + i0 + 2) = make_double2(out[2], out[3]);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (i0 + e < a.m) Cb[i0 + e] = out[e];
+    }
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -1190,6 +1318,26 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
                  static_cast<unsigned>(std::min<long long>(d.n, 65535)),
                  static_cast<unsigned>(nbatch));
     const bool reduce = splits > 1;
+    if (!reduce) {
+      // pipelined: about eight waves of 3 blocks per SM (a short tail), each
+      // block walking its share of the columns
+      const long long gx = (d.m + kCrtRows - 1) / kCrtRows;
+      const long long per_col = gx * nbatch;
+      const long long gy = std::min<long long>(
+          std::min<long long>(d.n, 65535),
+          std::max<long long>(1, (24LL * num_sms() + per_col - 1) / per_col));
+      const dim3 gp(static_cast<unsigned>(gx), static_cast<unsigned>(gy), g.z);
+      const size_t smem = size_t(kCrtStages) * L * kCrtRows;
+      switch (cs.nch) {
+        case 1: k_crt_pipe<1><<<gp, 256, smem, s>>>(ca); break;
+        case 2: k_crt_pipe<2><<<gp, 256, smem, s>>>(ca); break;
+        case 3: k_crt_pipe<3><<<gp, 256, smem, s>>>(ca); break;
+        default: k_crt_pipe<4><<<gp, 256, smem, s>>>(ca); break;
+      }
+      UW12_LAUNCHED();
+      tm.stop();
+      return;
+    }
     switch (cs.nch * 2 + (reduce ? 1 : 0)) {
       case 2: k_crt<1, false><<<g, 256, 0, s>>>(ca); break;
       case 3: k_crt<1, true><<<g, 256, 0, s>>>(ca); break;
