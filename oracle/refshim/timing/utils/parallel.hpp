@@ -13,17 +13,19 @@
 //     top level and serially inside an active parallel region, as in the
 //     reference's OpenMP build;
 //   * sampled (sample_rounds = r > 0): a top-level loop with more than r x T
-//     iterations (T = OpenMP threads) runs r x T evenly spaced iterations,
-//     r per thread, all threads at once, and adds the extrapolated time of the
-//     rest to extra_seconds. The reference's OpenMP schedule gives each thread
-//     a contiguous block of n / T or n / T + 1 iterations (two-index loops:
-//     outer iterations of n2 inner ones each), so the whole loop takes
-//     floor(n / T) rounds with every thread busy and, when T does not divide
-//     n, one round with n mod T threads busy (two-index: floor(n1 / T) n2 and
-//     n2 rounds).  The sample measures r full rounds under the same memory
-//     contention, and the partial round by running n mod T iterations at once
-//     (fewer busy threads contend less, so a partial round is faster than a
-//     full one).  Loop results are then partial sums; only the time is used.
+//     iterations (T = OpenMP threads) runs a sample and adds the extrapolated
+//     time of the rest to extra_seconds. The reference's OpenMP loops use the
+//     static schedule: thread t runs one contiguous block of n / T or n / T + 1
+//     iterations (the first n mod T threads the longer ones; two-index loops:
+//     blocks of outer iterations, n2 inner ones each), and the loop ends with
+//     its slowest thread. The sample runs r iterations from the middle of
+//     every thread's block, thread t its own, all threads at once (the same
+//     memory contention), times each on its thread, and estimates the loop as
+//     max over t of (block size of t) x (mean sampled iteration time of t).
+//     (Extrapolating one round's wall time instead -- the slowest of T
+//     iterations -- over all rounds overestimated loops whose iterations
+//     differ in cost by 10-22 %.) Loop results are then partial sums; only
+//     the time is used.
 //   * rotation (rotation = S > 0, with sampling): the sampled loops of an
 //     evaluation are numbered in the order they run; loop q is measured (as
 //     above) only when q % S == phase and otherwise skipped, its estimate
@@ -38,6 +40,7 @@
 
 #include <omp.h>
 
+#include <algorithm>
 #include <functional>
 #include <vector>
 
@@ -59,7 +62,6 @@ struct LoopRecord {
 };
 inline std::vector<LoopRecord> loop_log;
 
-inline size_t ceil_div(size_t a, size_t b) { return (a + b - 1) / b; }
 
 inline bool sampling_applies(size_t n, bool parallel) {
   return sample_rounds > 0 && parallel && !omp_in_parallel() &&
@@ -67,48 +69,79 @@ inline bool sampling_applies(size_t n, bool parallel) {
                  static_cast<size_t>(omp_get_max_threads());
 }
 
-// k evenly spaced indices of [0, n).
-inline std::vector<size_t> spaced(size_t n, size_t k) {
-  std::vector<size_t> idx(k);
-  for (size_t t = 0; t < k; ++t)
-    idx[t] = static_cast<size_t>((static_cast<double>(t) + 0.5) *
-                                 static_cast<double>(n) /
-                                 static_cast<double>(k));
-  return idx;
+// First iteration and size of thread t's block of the static schedule of n
+// iterations over T threads.
+inline void static_block(size_t n, size_t T, size_t t, size_t& first, size_t& size) {
+  size_t q = n / T, extra = n % T;
+  if (t < extra) {
+    ++q;
+    extra = 0;
+  }
+  first = q * t + extra;
+  size = q;
 }
 
-// Runs body(slot, item) for every sampled item, r per thread, then the
-// partial-round items at once, and books the extrapolated remainder: the full
-// loop takes `rounds_full` rounds with every thread busy (the sample ran r)
-// and `rounds_part` rounds with part.size() threads busy (the sample ran one).
-// Under rotation a loop not due for measurement runs no iteration and books
-// its cached estimate.
+// Sampled iterations: r per non-empty block (evenly spaced inside it), item
+// q belonging to block owner[q] of size block[owner[q]].
+struct Sample {
+  std::vector<size_t> items, owner, block;
+};
+
+inline Sample block_sample(size_t n, size_t T, size_t r) {
+  Sample smp;
+  smp.block.assign(T, 0);
+  for (size_t t = 0; t < T; ++t) {
+    size_t first = 0, size = 0;
+    static_block(n, T, t, first, size);
+    smp.block[t] = size;
+    if (size == 0) continue;
+    const size_t k = size < r ? size : r;
+    for (size_t u = 0; u < k; ++u) {
+      smp.items.push_back(first + static_cast<size_t>((static_cast<double>(u) + 0.5) *
+                                                      static_cast<double>(size) /
+                                                      static_cast<double>(k)));
+      smp.owner.push_back(t);
+    }
+  }
+  return smp;
+}
+
+// Runs body(slot, item) for every sampled item, all threads at once (item q
+// on thread q mod T), timing each item, and books the estimate
+// max_t units x block[t] x mean time of t's items (`units`: iterations per
+// block element, n2 for two-index loops). Under rotation a loop not due for
+// measurement runs no iteration and books its cached estimate.
 template <typename Body>
-void run_sample(const std::vector<size_t>& items, size_t r, double rounds_full,
-                const std::vector<size_t>& part, double rounds_part, Body&& body) {
+void run_sample(const Sample& smp, double units, Body&& body) {
   const long q_loop = loop_index++;
   if (cached.size() <= static_cast<size_t>(q_loop)) cached.resize(q_loop + 1, -1.0);
   if (rotation > 0 && q_loop % rotation != phase && cached[q_loop] >= 0.0) {
     extra_seconds += cached[q_loop];
     return;
   }
+  const long ni = static_cast<long>(smp.items.size());
+  std::vector<double> dt(smp.items.size(), 0.0);
   const double t0 = omp_get_wtime();
 #pragma omp parallel for schedule(static, 1)
-  for (long q = 0; q < static_cast<long>(items.size()); ++q)
-    body(static_cast<size_t>(q), items[static_cast<size_t>(q)]);
-  const double t1 = omp_get_wtime();
-  if (!part.empty()) {
-#pragma omp parallel for schedule(static, 1)
-    for (long q = 0; q < static_cast<long>(part.size()); ++q)
-      body(static_cast<size_t>(q), part[static_cast<size_t>(q)]);
+  for (long q = 0; q < ni; ++q) {
+    const double a = omp_get_wtime();
+    body(static_cast<size_t>(q), smp.items[static_cast<size_t>(q)]);
+    dt[static_cast<size_t>(q)] = omp_get_wtime() - a;
   }
-  const double t2 = omp_get_wtime();
-  const double estimate =
-      (t1 - t0) * rounds_full / static_cast<double>(r) + (t2 - t1) * rounds_part;
+  const double wall = omp_get_wtime() - t0;
+  std::vector<double> sum(smp.block.size(), 0.0), cnt(smp.block.size(), 0.0);
+  for (long q = 0; q < ni; ++q) {
+    sum[smp.owner[static_cast<size_t>(q)]] += dt[static_cast<size_t>(q)];
+    cnt[smp.owner[static_cast<size_t>(q)]] += 1.0;
+  }
+  double estimate = 0.0;
+  for (size_t t = 0; t < smp.block.size(); ++t)
+    if (cnt[t] > 0.0)
+      estimate = std::max(estimate, units * static_cast<double>(smp.block[t]) * sum[t] / cnt[t]);
   cached[q_loop] = estimate;
-  extra_seconds += estimate - (t2 - t0);
+  extra_seconds += estimate - wall;
   ++sampled_loops;
-  loop_log.push_back({items.size(), 1, estimate});
+  loop_log.push_back({smp.items.size(), 1, estimate});
 }
 
 // Times a top-level loop that runs every iteration (for the loop log).
@@ -132,9 +165,7 @@ inline void parallel_for(size_t start, size_t stop,
   if (ts::sampling_applies(n, parallel)) {
     const size_t T = static_cast<size_t>(omp_get_max_threads());
     const size_t r = static_cast<size_t>(ts::sample_rounds);
-    ts::run_sample(ts::spaced(n, r * T), r, static_cast<double>(n / T),
-                   ts::spaced(n, n % T), 1.0,
-                   [&](size_t, size_t i) { func(start + i); });
+    ts::run_sample(ts::block_sample(n, T, r), 1.0, [&](size_t, size_t i) { func(start + i); });
     return;
   }
   if (!omp_in_parallel()) ++ts::full_loops;
@@ -185,10 +216,9 @@ ReturnType parallel_sum(const size_t start, const size_t stop,
   if (ts::sampling_applies(n, parallel)) {
     const size_t T = static_cast<size_t>(omp_get_max_threads());
     const size_t r = static_cast<size_t>(ts::sample_rounds);
-    const auto items = ts::spaced(n, r * T);
-    std::vector<ReturnType> part(items.size(), identity);
-    ts::run_sample(items, r, static_cast<double>(n / T), ts::spaced(n, n % T), 1.0,
-                   [&](size_t q, size_t i) { part[q] += func(start + i); });
+    const ts::Sample smp = ts::block_sample(n, T, r);
+    std::vector<ReturnType> part(smp.items.size(), identity);
+    ts::run_sample(smp, 1.0, [&](size_t q, size_t i) { part[q] += func(start + i); });
     return part[0];
   }
   if (!omp_in_parallel()) ++ts::full_loops;
@@ -207,16 +237,14 @@ ReturnType parallel_sum_2d(
   if (ts::sampling_applies(n1 * n2, parallel)) {
     const size_t T = static_cast<size_t>(omp_get_max_threads());
     const size_t r = static_cast<size_t>(ts::sample_rounds);
-    const auto items = ts::spaced(n1 * n2, r * T);
-    std::vector<ReturnType> part(items.size(), identity);
-    // partial round: n1 mod T threads, one inner item each (outer iterations
-    // evenly spaced)
-    std::vector<size_t> rem;
-    for (size_t i : ts::spaced(n1, n1 % T)) rem.push_back(i * n2 + n2 / 2);
-    ts::run_sample(items, r, static_cast<double>((n1 / T) * n2), rem,
-                   static_cast<double>(n2), [&](size_t q, size_t p) {
-                     part[q] += func(start1 + p / n2, start2 + p % n2);
-                   });
+    // blocks of outer iterations; each sampled outer iteration runs one inner
+    // iteration (the middle one), an n2-th of its cost
+    ts::Sample smp = ts::block_sample(n1, T, r);
+    for (size_t& it : smp.items) it = it * n2 + n2 / 2;
+    std::vector<ReturnType> part(smp.items.size(), identity);
+    ts::run_sample(smp, static_cast<double>(n2), [&](size_t q, size_t p) {
+      part[q] += func(start1 + p / n2, start2 + p % n2);
+    });
     return part[0];
   }
   if (!omp_in_parallel()) ++ts::full_loops;
