@@ -1305,16 +1305,19 @@ void form_fock(const FockRequest& rq) {
         for (const IntegralsHandle* Xi : {&W, &V})
           xscr = std::max(xscr, (Xi->J3_0.get() ? 0 : np * aux_step(*Xi, false, budget / 2)) +
                                     (Xi->J3_ri_0.get() ? 0 : R * N * aux_step(*Xi, true, budget / 2)));
-        const size_t per_k = 3 * Rp * a * N + a * (N * N + R * N + np);
+        // two R' a N buffers per k: Z_W (term 1, done first), then W_k of the
+        // k-term in the same memory; Z_V (term 0) lives until the k-term
+        const size_t per_k = 2 * Rp * a * N + a * (N * N + R * N + np);
         const auto [klo, khi] = part(o);
         const size_t kavail = budget > xscr ? budget - xscr : 0;
         const size_t kc = tile_chunk(khi - klo, a,
                                      std::max<size_t>(1, std::min(khi - klo, kavail / per_k)));
         DevBuf ZYV(Rp * a * N * kc), ZYW(Rp * a * N * kc), gpk(np * a * kc), Gao(N * N * a * kc),
-            gri(R * N * a * kc), Wk(Rp * N * a * kc), scrX, scrXr;
+            gri(R * N * a * kc), scrX, scrXr;
+        double* const Wk = ZYW.get();  // after term 1 has used Z_W
         for (size_t k0 = klo; k0 < khi; k0 += kc) {
           const size_t nk = std::min(kc, khi - k0);
-          for (int term = 0; term < 2; ++term) {
+          for (int term : {1, 0}) {
             // term 0: fock_i(W, V) over (j, k); term 1: fock_i(V, W) over (i, k)
             const IntegralsHandle& Xi = term == 0 ? W : V;
             const double* xh = term == 0 ? xhW.get() : xhV.get();
@@ -1370,10 +1373,10 @@ void form_fock(const FockRequest& rq) {
             const size_t ni = static_cast<size_t>(i1 - i0);
             GemmDesc gw = gemm_nn(LL(Rp * ni), LL(N * a), LL(MW), 1.0,
                                   XW.Wst[s].get() + Rp * i0, LL(Rp * a), b1wl.get() + N * c,
-                                  LL(No), 0.0, Wk.get(), LL(Rp * ni));
+                                  LL(No), 0.0, Wk, LL(Rp * ni));
             gw.b_ncontig = true;
             gemm(gw);
-            GemmDesc fk = gemm_nn(LL(N), LL(N), LL(Rp), s_ss, Wk.get(), LL(Rp * ni),
+            GemmDesc fk = gemm_nn(LL(N), LL(N), LL(Rp), s_ss, Wk, LL(Rp * ni),
                                   ZYV.get() + Rp * a * N * (c + i0 - k0), LL(Rp * a), 1.0,
                                   Fp[s].get(), LL(N));
             fk.a_kcontig = true;
