@@ -58,6 +58,12 @@ import tempfile
 import time
 from pathlib import Path
 
+# The CPU baseline (libuw12 from its own sources) calls BLAS inside its OpenMP
+# loops, one BLAS call per thread: its BLAS runs single-threaded, which has to
+# be set before any BLAS library of this process is loaded (the sampler's
+# validation, oracle/validate_sampler.py, runs the same way).
+os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+
 import numpy as np
 
 ROOT = Path(__file__).resolve().parent

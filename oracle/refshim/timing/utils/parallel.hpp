@@ -18,14 +18,14 @@
 //     static schedule: thread t runs one contiguous block of n / T or n / T + 1
 //     iterations (the first n mod T threads the longer ones; two-index loops:
 //     blocks of outer iterations, n2 inner ones each), and the loop ends with
-//     its slowest thread. The sample runs r iterations from the middle of
-//     every thread's block, thread t its own, all threads at once (the same
-//     memory contention), times each on its thread, and estimates the loop as
-//     max over t of (block size of t) x (mean sampled iteration time of t).
-//     (Extrapolating one round's wall time instead -- the slowest of T
-//     iterations -- over all rounds overestimated loops whose iterations
-//     differ in cost by 10-22 %.) Loop results are then partial sums; only
-//     the time is used.
+//     its slowest thread. Thread t runs the first max(2, r) iterations of its
+//     own block, in order, all threads at once (the same memory contention),
+//     timing each: the first runs cold, the others warm, and the block is
+//     estimated as the sampled times plus its remaining iterations at the
+//     mean warm time; the loop as the slowest block. (Extrapolating one
+//     round's wall time -- the slowest of T cold first iterations -- over all
+//     rounds overestimated c1m by 18-22 %.) Loop results are then partial
+//     sums; only the time is used.
 //   * rotation (rotation = S > 0, with sampling): the sampled loops of an
 //     evaluation are numbered in the order they run; loop q is measured (as
 //     above) only when q % S == phase and otherwise skipped, its estimate
@@ -81,36 +81,36 @@ inline void static_block(size_t n, size_t T, size_t t, size_t& first, size_t& si
   size = q;
 }
 
-// Sampled iterations: r per non-empty block (evenly spaced inside it), item
-// q belonging to block owner[q] of size block[owner[q]].
+// Sampled iterations: the first k = min(size, max(2, r)) iterations of every
+// non-empty block, in order (block t run by thread t, as in the full loop).
 struct Sample {
-  std::vector<size_t> items, owner, block;
+  std::vector<std::vector<size_t>> items;  // per block
+  std::vector<size_t> block;               // block sizes
 };
 
 inline Sample block_sample(size_t n, size_t T, size_t r) {
   Sample smp;
+  smp.items.assign(T, {});
   smp.block.assign(T, 0);
+  const size_t want = r < 2 ? 2 : r;
   for (size_t t = 0; t < T; ++t) {
     size_t first = 0, size = 0;
     static_block(n, T, t, first, size);
     smp.block[t] = size;
-    if (size == 0) continue;
-    const size_t k = size < r ? size : r;
-    for (size_t u = 0; u < k; ++u) {
-      smp.items.push_back(first + static_cast<size_t>((static_cast<double>(u) + 0.5) *
-                                                      static_cast<double>(size) /
-                                                      static_cast<double>(k)));
-      smp.owner.push_back(t);
-    }
+    for (size_t u = 0; u < size && u < want; ++u) smp.items[t].push_back(first + u);
   }
   return smp;
 }
 
-// Runs body(slot, item) for every sampled item, all threads at once (item q
-// on thread q mod T), timing each item, and books the estimate
-// max_t units x block[t] x mean time of t's items (`units`: iterations per
-// block element, n2 for two-index loops). Under rotation a loop not due for
-// measurement runs no iteration and books its cached estimate.
+// Thread t runs its block's sampled iterations one after another, all threads
+// at once (the same memory contention as the full loop), timing each.  A
+// block's first iteration runs cold (the thread's first touch of its
+// temporaries), the later ones warm, so block t is estimated as its sampled
+// iterations plus the rest of its units x size iterations at the mean warm
+// time (`units`: inner iterations per block element, n2 for two-index loops,
+// whose sample runs one inner iteration per outer one), and the loop as the
+// slowest block.  Under rotation a loop not due for measurement runs no
+// iteration and books its cached estimate.
 template <typename Body>
 void run_sample(const Sample& smp, double units, Body&& body) {
   const long q_loop = loop_index++;
@@ -119,29 +119,33 @@ void run_sample(const Sample& smp, double units, Body&& body) {
     extra_seconds += cached[q_loop];
     return;
   }
-  const long ni = static_cast<long>(smp.items.size());
-  std::vector<double> dt(smp.items.size(), 0.0);
+  const long T = static_cast<long>(smp.block.size());
+  std::vector<double> est(smp.block.size(), 0.0);
   const double t0 = omp_get_wtime();
 #pragma omp parallel for schedule(static, 1)
-  for (long q = 0; q < ni; ++q) {
-    const double a = omp_get_wtime();
-    body(static_cast<size_t>(q), smp.items[static_cast<size_t>(q)]);
-    dt[static_cast<size_t>(q)] = omp_get_wtime() - a;
+  for (long t = 0; t < T; ++t) {
+    const std::vector<size_t>& its = smp.items[static_cast<size_t>(t)];
+    double first = 0.0, warm = 0.0;
+    for (size_t u = 0; u < its.size(); ++u) {
+      const double a = omp_get_wtime();
+      body(static_cast<size_t>(t), its[u]);
+      const double d = omp_get_wtime() - a;
+      if (u == 0) first = d; else warm += d;
+    }
+    const double k = static_cast<double>(its.size());
+    const double total = units * static_cast<double>(smp.block[static_cast<size_t>(t)]);
+    if (k > 1.0)
+      est[static_cast<size_t>(t)] = first + warm + (total - k) * warm / (k - 1.0);
+    else if (k > 0.0)
+      est[static_cast<size_t>(t)] = total * first;
   }
   const double wall = omp_get_wtime() - t0;
-  std::vector<double> sum(smp.block.size(), 0.0), cnt(smp.block.size(), 0.0);
-  for (long q = 0; q < ni; ++q) {
-    sum[smp.owner[static_cast<size_t>(q)]] += dt[static_cast<size_t>(q)];
-    cnt[smp.owner[static_cast<size_t>(q)]] += 1.0;
-  }
   double estimate = 0.0;
-  for (size_t t = 0; t < smp.block.size(); ++t)
-    if (cnt[t] > 0.0)
-      estimate = std::max(estimate, units * static_cast<double>(smp.block[t]) * sum[t] / cnt[t]);
+  for (double e : est) estimate = std::max(estimate, e);
   cached[q_loop] = estimate;
   extra_seconds += estimate - wall;
   ++sampled_loops;
-  loop_log.push_back({smp.items.size(), 1, estimate});
+  loop_log.push_back({smp.block.size(), 1, estimate});
 }
 
 // Times a top-level loop that runs every iteration (for the loop log).
@@ -217,7 +221,7 @@ ReturnType parallel_sum(const size_t start, const size_t stop,
     const size_t T = static_cast<size_t>(omp_get_max_threads());
     const size_t r = static_cast<size_t>(ts::sample_rounds);
     const ts::Sample smp = ts::block_sample(n, T, r);
-    std::vector<ReturnType> part(smp.items.size(), identity);
+    std::vector<ReturnType> part(T, identity);
     ts::run_sample(smp, 1.0, [&](size_t q, size_t i) { part[q] += func(start + i); });
     return part[0];
   }
@@ -240,8 +244,9 @@ ReturnType parallel_sum_2d(
     // blocks of outer iterations; each sampled outer iteration runs one inner
     // iteration (the middle one), an n2-th of its cost
     ts::Sample smp = ts::block_sample(n1, T, r);
-    for (size_t& it : smp.items) it = it * n2 + n2 / 2;
-    std::vector<ReturnType> part(smp.items.size(), identity);
+    for (auto& blk : smp.items)
+      for (size_t& it : blk) it = it * n2 + n2 / 2;
+    std::vector<ReturnType> part(T, identity);
     ts::run_sample(smp, static_cast<double>(n2), [&](size_t q, size_t p) {
       part[q] += func(start1 + p / n2, start2 + p % n2);
     });
