@@ -1497,12 +1497,26 @@ int ozaki_bits(int n_moduli, long long k_total) {
   return std::min(beta, 50);  // |A'| <= 2^50: the FP64 rounding tricks stay exact
 }
 
+#ifndef UW12_COST_FP64_TFS
+#define UW12_COST_FP64_TFS 26.0
+#endif
+#ifndef UW12_COST_PREP_TBS
+#define UW12_COST_PREP_TBS 3.2
+#endif
+#ifndef UW12_COST_CRT_TBS
+#define UW12_COST_CRT_TBS 2.0
+#endif
+#ifndef UW12_COST_I8_POPS
+#define UW12_COST_I8_POPS 2.2
+#endif
+
 bool ozaki_profitable(const GemmDesc& d, int n_moduli) {
   // Estimated times on a B200 (fitted to measured kernels): operand
   // preparation streams each operand element twice in FP64 and writes L
-  // residue bytes (~3.2 TB/s); the CRT reads L residue bytes (and C when
-  // beta != 0) and writes C (~2 TB/s); the int8 products run at ~2.2 POPS;
-  // the FP64 DMMA GEMM at ~26 TFLOP/s.  Split when it is clearly faster.
+  // residue bytes (UW12_COST_PREP_TBS TB/s); the CRT reads L residue bytes
+  // (and C when beta != 0) and writes C (UW12_COST_CRT_TBS); the int8
+  // products run at UW12_COST_I8_POPS; the FP64 DMMA GEMM at
+  // UW12_COST_FP64_TFS TFLOP/s.  Split when it is clearly faster.
   const double L = double(n_moduli);
   const double k_total = double(d.k) * double(d.nbr1) * double(d.nbr2);
   const double nbatch = double(d.nbo1) * double(d.nbo2);
@@ -1512,10 +1526,11 @@ bool ozaki_profitable(const GemmDesc& d, int n_moduli) {
                     double(d.sBo2 && d.nbo2 > 1 ? d.nbo2 : 1);
   const double m = double(d.m), n = double(d.n);
   const double flops = 2.0 * m * n * k_total * nbatch;
-  const double t_fp64 = flops / 26e12;
-  const double t_prep = (pa * m + pb * n) * k_total * (16.0 + L) / 3.2e12;
-  const double t_crt = nbatch * m * n * (L + 8.0 + (d.beta != 0.0 ? 8.0 : 0.0)) / 2.0e12;
-  const double t_i8 = flops * L / 2.2e15;
+  const double t_fp64 = flops / (UW12_COST_FP64_TFS * 1e12);
+  const double t_prep = (pa * m + pb * n) * k_total * (16.0 + L) / (UW12_COST_PREP_TBS * 1e12);
+  const double t_crt = nbatch * m * n * (L + 8.0 + (d.beta != 0.0 ? 8.0 : 0.0)) /
+                       (UW12_COST_CRT_TBS * 1e12);
+  const double t_i8 = flops * L / (UW12_COST_I8_POPS * 1e15);
   return t_prep + t_crt + t_i8 + 30e-6 < 0.9 * t_fp64;
 }
 
