@@ -341,8 +341,9 @@ def run_reference(args, rank, world):
     value = float(statistics.median(ests))
     sample = (f"{args.config} energy + Fock (libuw12 has no adjoint), libuw12's unmodified "
               f"sources (oracle/ref.mk, OpenMP, BLAS single-threaded inside its loops); every "
-              f"top-level loop over aux functions / orbital pairs measured on one iteration per "
-              f"thread under full contention and extrapolated by its OpenMP schedule, loops "
+              f"top-level loop over aux functions / orbital pairs sampled on every thread at "
+              f"once (the first two iterations of its static-schedule block, the rest at the "
+              f"warm iteration's time; the loop as its slowest block), loops "
               f"rotated over {S} steps (each step measures every {S}-th loop, the others at "
               f"their last estimate; primed by one full sample of {prime[1]:.1f} s); value = "
               f"median of {args.steps} step estimates (min {min(ests):.0f}, max "
@@ -794,8 +795,9 @@ def main():
                "sample": f"{args.config} energy + Fock (libuw12 has no adjoint) by libuw12's "
                          f"unmodified sources (oracle/ref.mk, OpenMP on {cores} threads): one "
                          f"evaluation with each of its {nloops} top-level loops over aux "
-                         f"functions / orbital pairs run on one iteration per thread and "
-                         f"extrapolated ({wall:.1f} s measured); setup excluded"}
+                         f"functions / orbital pairs sampled (the first two iterations of "
+                         f"every thread's static-schedule block, the rest at the warm "
+                         f"iteration's time; {wall:.1f} s measured); setup excluded"}
 
     batched = batched_report(L, args, args.moduli) if args.batched and world == 1 else None
 
