@@ -283,6 +283,16 @@ __global__ void k_exponent_to_shift(const unsigned* __restrict__ eplus, long lon
   if (t < n) shift[t] = eplus[t] ? beta - (static_cast<int>(eplus[t]) - 2048) : 0;
 }
 
+// x 2^e for exponents outside the normal range, out of line: kept off the
+// per-element paths (inlined, its branches would run predicated on every
+// element).
+__device__ __noinline__ double ldexp_slow(double x, int e) { return ldexp(x, e); }
+
+// 2^e as a double for -1022 <= e <= 1023 (exponent bits only).
+__device__ __forceinline__ double pow2(int e) {
+  return __longlong_as_double(static_cast<long long>(e + 1023) << 52);
+}
+
 struct ResidueMods {
   int L;
   int pi[kOzakiMaxModuli];
@@ -346,12 +356,11 @@ __global__ void __launch_bounds__(256) k_residues(OperandView v, const int* __re
 #pragma unroll
     for (int q = 0; q < 8; ++q) x[q] = tile[tile_at(r, 8 * t + q)];
     if (sh > -1000 && sh < 1000) {  // 2^sh is a normal double: scale by one multiply
-      const double sc = ldexp(1.0, sh);
+      const double sc = pow2(sh);
 #pragma unroll
       for (int q = 0; q < 8; ++q) x[q] = round_int(x[q] * sc);
     } else {
-#pragma unroll
-      for (int q = 0; q < 8; ++q) x[q] = round_int(ldexp(x[q], sh));
+      for (int q = 0; q < 8; ++q) x[q] = round_int(ldexp_slow(x[q], sh));
     }
     int vl[8];
 #pragma unroll
@@ -768,9 +777,8 @@ struct CrtArgs {
 // x 2^e: one multiply by an exactly representable power of two when 2^e is a
 // normal double, ldexp otherwise.
 __device__ __forceinline__ double scale_pow2(double x, int e) {
-  if (e >= -1022 && e <= 1023)
-    return x * __longlong_as_double(static_cast<long long>(e + 1023) << 52);
-  return ldexp(x, e);
+  if (e >= -1022 && e <= 1023) return x * pow2(e);
+  return ldexp_slow(x, e);
 }
 
 // s + e = a + b exactly (Knuth's TwoSum, six FP64 operations).
