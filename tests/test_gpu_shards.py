@@ -120,3 +120,30 @@ def test_sharded_evaluation_needs_an_allreduce(uw12lib, cuda_device):
             uw12lib.form_fock(W, V, WV, A, d.orbitals, d.occ, case.n_active, True, True, 1.0, 0.5)
     finally:
         uw12lib.set_shard(0, 1)
+
+
+def test_failing_allreduce_fails_the_evaluation(uw12lib, cuda_device):
+    """An exception in the hook (a rank that left, a collective that timed
+    out) ends the evaluation with an error instead of a wrong result."""
+    case = CASES[2]
+    d = make_case(case)
+    W = uw12lib.setup_base_integrals(d.W3, d.W2, d.W3_ri)
+    V = uw12lib.setup_base_integrals(d.V3, d.V2, d.V3_ri)
+    WV = uw12lib.setup_base_integrals(d.WV3, d.WV2)
+    A = uw12lib.setup_abs_projectors(d.S, case.n_ao, case.n_ri)
+
+    def broken(ptr, count, stream):
+        raise RuntimeError("peer rank gone")
+
+    uw12lib.set_shard(0, 2)
+    uw12lib.set_allreduce(broken)
+    try:
+        with pytest.raises(uw12lib.UW12Error, match="all-reduce"):
+            uw12lib.form_fock(W, V, WV, A, d.orbitals, d.occ, case.n_active, True, True, 1.0, 0.5)
+    finally:
+        uw12lib.set_allreduce(None)
+        uw12lib.set_shard(0, 1)
+    # the thread is usable again: an unsharded evaluation succeeds
+    e, _, _ = uw12lib.form_fock(W, V, WV, A, d.orbitals, d.occ, case.n_active, True, True,
+                                1.0, 0.5)
+    assert np.isfinite(e)
