@@ -8,13 +8,15 @@ all host threads, in separate processes:
   * full evaluations of libuw12 built with its own loop dispatcher
     (oracle/_ref/libuw12_ref.so, every loop iteration run);
   * sampled evaluations of the timing build (oracle/_ref/libuw12_ref_timing.so:
-    every top-level loop runs `rounds` iterations per thread, the rest is
-    extrapolated);
+    every thread runs the first max(2, rounds) iterations of its own block of
+    each top-level loop's static schedule, the rest of the block is
+    extrapolated at the warm iterations' time, the loop is its slowest block);
   * with --rotation S, the estimator bench.py's reference arm uses: one primed
     sampled evaluation, then S evaluations each measuring every S-th loop
     (the others at their last estimate), reporting every step's estimate;
 and prints one JSON line: medians, the estimate's ratio to the full time, the
-host's CPU model and thread count.
+host's CPU model and thread count.  Every child runs with OPENBLAS_NUM_THREADS=1
+(BLAS single-threaded inside libuw12's OpenMP loops), as bench.py does.
 """
 from __future__ import annotations
 
