@@ -330,7 +330,7 @@ __device__ __forceinline__ uint32_t residue_low(int vl, double v, double inv_p, 
 // per modulus (16 lanes: 128 contiguous bytes per row and modulus).  The
 // moduli loop is unrolled to kOzakiMaxModuli, so that p and 1/p are
 // immediate constant-bank operands.  Grid: (row tiles, k tiles, planes).
-template <bool KCONTIG>
+template <bool KCONTIG, int LM>
 __global__ void __launch_bounds__(256) k_residues(OperandView v, const int* __restrict__ shift,
                                                   ResidueMods mods, int tile_log2,
                                                   long long tiles, long long k_pad,
@@ -370,8 +370,8 @@ __global__ void __launch_bounds__(256) k_residues(OperandView v, const int* __re
         (((plane * tiles + (row >> tile_log2)) * mods.L) << tile_log2) + (row & tmask);
     uint8_t* dst = out + base_row * k_pad + k0 + 8 * t;
 #pragma unroll
-    for (int l = 0; l < kOzakiMaxModuli; ++l) {
-      if (l < mods.L) {
+    for (int l = 0; l < (LM ? LM : kOzakiMaxModuli); ++l) {
+      if (LM || l < mods.L) {
         const double ip = mods.inv_p[l];
         const int p = mods.pi[l];
         const uint32_t b01 =
@@ -974,7 +974,7 @@ __global__ void __launch_bounds__(256, REDUCE ? 2 : kCrtMinBlocks) k_crt(const C
 constexpr int kCrtStages = 3;
 constexpr int kCrtRows = 1024;  // rows i per block
 
-template <int NCH>
+template <int NCH, int LM>
 __global__ void __launch_bounds__(256, 3) k_crt_pipe(const CrtArgs a) {
   extern __shared__ __align__(16) uint8_t crt_smem[];  // kCrtStages x L x kCrtRows bytes
   const int L = a.L;
@@ -1046,8 +1046,8 @@ __global__ void __launch_bounds__(256, 3) k_crt_pipe(const CrtArgs a) {
 #pragma unroll
       for (int c = 0; c < NCH; ++c) S[e][c] = 0.0;
 #pragma unroll
-    for (int l = 0; l < kOzakiMaxModuli; ++l) {
-      if (l < L) {
+    for (int l = 0; l < (LM ? LM : kOzakiMaxModuli); ++l) {
+      if (LM || l < L) {
         const uint32_t w = *reinterpret_cast<const uint32_t*>(rs + l * kCrtRows);
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
@@ -1233,10 +1233,15 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
       UW12_LAUNCHED();
       const int tlog = tile_rows == 256 ? 8 : 7;
       const long long tiles = rows_pad / tile_rows;
-      if (v.ks == 1)
-        k_residues<true><<<g, 256, 0, s>>>(v, sh, mods, tlog, tiles, k_pad, out);
+      // the default modulus count runs a fully unrolled, unguarded moduli loop
+      if (v.ks == 1 && L == kOzakiDefaultModuli)
+        k_residues<true, kOzakiDefaultModuli><<<g, 256, 0, s>>>(v, sh, mods, tlog, tiles, k_pad, out);
+      else if (v.ks == 1)
+        k_residues<true, 0><<<g, 256, 0, s>>>(v, sh, mods, tlog, tiles, k_pad, out);
+      else if (L == kOzakiDefaultModuli)
+        k_residues<false, kOzakiDefaultModuli><<<g, 256, 0, s>>>(v, sh, mods, tlog, tiles, k_pad, out);
       else
-        k_residues<false><<<g, 256, 0, s>>>(v, sh, mods, tlog, tiles, k_pad, out);
+        k_residues<false, 0><<<g, 256, 0, s>>>(v, sh, mods, tlog, tiles, k_pad, out);
       UW12_LAUNCHED();
     };
     prep(va, planes_a, m_pad, kTileI, sa, ea, ra);
@@ -1336,11 +1341,15 @@ void run_core(const GemmDesc& d, const Consts& cs, int beta, cudaStream_t s) {
           std::max<long long>(1, (24LL * num_sms() + per_col - 1) / per_col));
       const dim3 gp(static_cast<unsigned>(gx), static_cast<unsigned>(gy), g.z);
       const size_t smem = size_t(kCrtStages) * L * kCrtRows;
-      switch (cs.nch) {
-        case 1: k_crt_pipe<1><<<gp, 256, smem, s>>>(ca); break;
-        case 2: k_crt_pipe<2><<<gp, 256, smem, s>>>(ca); break;
-        case 3: k_crt_pipe<3><<<gp, 256, smem, s>>>(ca); break;
-        default: k_crt_pipe<4><<<gp, 256, smem, s>>>(ca); break;
+      if (L == kOzakiDefaultModuli && cs.nch == 3) {
+        k_crt_pipe<3, kOzakiDefaultModuli><<<gp, 256, smem, s>>>(ca);
+      } else {
+        switch (cs.nch) {
+          case 1: k_crt_pipe<1, 0><<<gp, 256, smem, s>>>(ca); break;
+          case 2: k_crt_pipe<2, 0><<<gp, 256, smem, s>>>(ca); break;
+          case 3: k_crt_pipe<3, 0><<<gp, 256, smem, s>>>(ca); break;
+          default: k_crt_pipe<4, 0><<<gp, 256, smem, s>>>(ca); break;
+        }
       }
       UW12_LAUNCHED();
       tm.stop();

@@ -24,6 +24,10 @@
 namespace uw12b {
 
 constexpr int kOzakiMaxModuli = 16;
+// The modulus count of FP64-level accuracy (about 48 bits kept per operand
+// element at K = 1500); its residue and CRT kernels are compiled with the
+// moduli loop fully unrolled and unguarded.
+constexpr int kOzakiDefaultModuli = 14;
 
 // Number of moduli of the split-precision GEMMs of this host thread
 // (0 = plain FP64 DMMA GEMMs).  gemm() routes GEMMs of at least
