@@ -1525,12 +1525,68 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
   double* gJ2[3] = {target(out.dJ2[0], MW * MW), target(out.dJ2[1], MV * MV),
                     target(out.dJ2[2], MX * MX)};
 
+  // Without same-spin terms every recomputed intermediate enters the gradients
+  // through sums over orbitals: X_AB and t over active / occupied orbitals,
+  // B2-bar of occupied orbital k from the other potential's B2 of k alone, and
+  // Wst-bar of active orbital j from the other potential's S^-1 Wst of j alone.
+  // When the whole intermediates (B2, Wst and S^-1 Wst of W and V per spin,
+  // and the transforms they come from) would not fit -- an explicit budget,
+  // or 90 % of the free device memory -- they are formed for a chunk of
+  // orbitals at a time instead (orbital_chunked), and only the gradient
+  // factors B1-bar (N o x M) and, when the RI gradient is wanted, Bri-bar
+  // (R a x M) are held whole.
+  const bool same_spin = rq.indirect && rq.s_ss != 0.0;
+  const size_t Mmax = std::max(MW, MV);
+  size_t whole = (N * o_tot + R * a_tot) * Mmax;
+  for (int s = 0; s < ns; ++s)
+    whole += 2 * (sd[s].a * sd[s].o + 2 * Rp * sd[s].a) * Mmax;
+  const bool orbital_chunked = !same_spin && whole > auto_budget_doubles(rq.mem_budget, 0.9);
+  // B1 (N*nk x M) of occupied orbitals [k0, k0 + nk) of spin s for potential X:
+  // sq(J3_0[:, A]) Co[:, k] P2
+  auto b1_chunk = [&](const IntegralsHandle& X, int s, size_t k0, size_t nk, DevBuf& dst) {
+    const size_t M = X.n_df;
+    DevBuf H(N * nk * M);
+    transform_ao(X, Co.get() + N * (sd[s].ooff + k0), nk, H.get(), budget / 2);
+    dst.alloc(N * nk * M);
+    gemm(gemm_nn(LL(N * nk), LL(M), LL(M), 1.0, H.get(), LL(N * nk), X.P2.get(), LL(M), 0.0,
+                 dst.get(), LL(N * nk)));
+  };
+  // Wst (R' nj x M) of active orbitals [j0, j0 + nj) of spin s for potential
+  // X: per orbital the AO rows sq(J3_0) Co[:, c + j] P2, then the RI rows
+  // J3ri_0 Ca[:, j] P2
+  auto wst_chunk = [&](const IntegralsHandle& X, int s, size_t j0, size_t nj, double* St) {
+    const size_t M = X.n_df;
+    {
+      DevBuf H(N * nj * M);
+      transform_ao(X, Co.get() + N * (sd[s].ooff + sd[s].c + j0), nj, H.get(), budget / 2);
+      GemmDesc ga = gemm_nn(LL(N), LL(M), LL(M), 1.0, H.get(), LL(N * nj), X.P2.get(), LL(M),
+                            0.0, St, LL(Rp * nj));
+      ga.nbo1 = LL(nj);
+      ga.sAo1 = LL(N);
+      ga.sCo1 = LL(Rp);
+      gemm(ga);
+    }
+    DevBuf H2(R * nj * M);
+    ri_transform(X, Ca_s(s) + N * j0, nj, H2.get(), budget);
+    GemmDesc gr = gemm_nn(LL(R), LL(M), LL(M), 1.0, H2.get(), LL(R * nj), X.P2.get(), LL(M), 0.0,
+                          St + N, LL(Rp * nj));
+    gr.nbo1 = LL(nj);
+    gr.sAo1 = LL(R);
+    gr.sCo1 = LL(Rp);
+    gemm(gr);
+  };
+  // occupied orbitals per chunk (B1 and its transform, B2 of the chunk and its
+  // adjoint) and active orbitals per chunk (the transforms, Wst of the chunk,
+  // S^-1 Wst and Wst-bar), as in form_fock's chunked X_AB and t passes
+  auto per_k = [&](int s) { return (4 * N + 2 * sd[s].a) * Mmax; };
+  const size_t per_j = (N + R + 3 * Rp) * Mmax;
+
   // ---- forward intermediates (as in form_fock): B2, Wst, (I (x) S^-1) Wst per X, spin
   struct PerX {
     std::vector<DevBuf> B2, Wst, SW;
   };
   PerX XW, XV;
-  for (int which = 0; which < 2; ++which) {
+  for (int which = 0; which < 2 && !orbital_chunked; ++which) {
     const IntegralsHandle& X = which == 0 ? W : V;
     PerX& P = which == 0 ? XW : XV;
     const size_t M = X.n_df;
@@ -1578,6 +1634,49 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
       Xab[s].zero();
       tab[s].zero();
       ttl[s].zero();
+      continue;
+    }
+    if (orbital_chunked) {
+      // X_AB = sum over active-orbital chunks of Wst_W[j]^T S^-1 Wst_V[j];
+      // t = sum over occupied-orbital chunks of B2_W[k]^T B2_V[k]
+      Xab[s].zero();
+      tab[s].zero();
+      const size_t jc = std::max<size_t>(1, std::min(a, budget / 2 / per_j));
+      for (size_t j0 = 0; j0 < a; j0 += jc) {
+        const size_t nj = std::min(jc, a - j0);
+        DevBuf Sw(Rp * nj * MW), SVj(Rp * nj * MV);
+        {
+          DevBuf Sv(Rp * nj * MV);
+          wst_chunk(V, s, j0, nj, Sv.get());
+          gemm(gemm_nn(LL(Rp), LL(nj * MV), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp), Sv.get(),
+                       LL(Rp), 0.0, SVj.get(), LL(Rp)));
+        }
+        wst_chunk(W, s, j0, nj, Sw.get());
+        GemmDesc gx = gemm_nn(LL(MW), LL(MV), LL(Rp * nj), 1.0, Sw.get(), LL(Rp * nj), SVj.get(),
+                              LL(Rp * nj), 1.0, Xab[s].get(), LL(MW));
+        gx.a_kcontig = true;
+        gemm(gx);
+      }
+      const size_t kc = std::max<size_t>(1, std::min(o, budget / 2 / per_k(s)));
+      for (size_t k0 = 0; k0 < o; k0 += kc) {
+        const size_t nk = std::min(kc, o - k0);
+        DevBuf B2w(a * nk * MW), B2v(a * nk * MV);
+        for (int which = 0; which < 2; ++which) {
+          const IntegralsHandle& X = which == 0 ? W : V;
+          DevBuf B1;
+          b1_chunk(X, s, k0, nk, B1);
+          GemmDesc g3 = gemm_nn(LL(a), LL(nk * X.n_df), LL(N), 1.0, Ca_s(s), LL(N), B1.get(),
+                                LL(N), 0.0, (which == 0 ? B2w : B2v).get(), LL(a));
+          g3.a_kcontig = true;
+          gemm(g3);
+        }
+        GemmDesc gt = gemm_nn(LL(MW), LL(MV), LL(a * nk), 1.0, B2w.get(), LL(a * nk), B2v.get(),
+                              LL(a * nk), 1.0, tab[s].get(), LL(MW));
+        gt.a_kcontig = true;
+        gemm(gt);
+      }
+      scale_rc(tab[s].get(), LL(MW), LL(MW), LL(MV), W.lam.get(), V.lam.get(), 1.0,
+               ttl[s].get(), LL(MW));
       continue;
     }
     GemmDesc gx = gemm_nn(LL(MW), LL(MV), LL(Rp * a), 1.0, XW.Wst[s].get(), LL(Rp * a),
@@ -1630,7 +1729,6 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
   //   G_W4 = -1/2 s esf P4(V4): B2_W-bar += 2 (G_W4 B2_W) L_W,
   //   A_W += B2_W^T G_W4 B2_W (and W <-> V with P4(W4)).
   clock.mark("adj_same_spin");
-  const bool same_spin = rq.indirect && rq.s_ss != 0.0;
   std::vector<DevBuf> ssB2b[2], ssWsb[2];
   DevBuf ssA[2];
   if (same_spin) {
@@ -1744,8 +1842,137 @@ void form_fock_adjoint(const FockRequest& rq_in, const AdjointOutputs& out) {
   }
 
   clock.mark("adj_three_index");
-  // ---- dE/dJ3_0 and dE/dJ3_ri_0 of W and V
-  for (int which = 0; which < 2; ++which) {
+  // ---- dE/dJ3_0 and dE/dJ3_ri_0 of W and V, orbital-chunked: B2-bar of
+  // occupied orbitals k (B2-bar_W = B2_V t-bar^T, B2-bar_V = B2_W t-bar) and
+  // Wst-bar of active orbitals j (Wst-bar_W = S^-1 Wst_V X-bar^T,
+  // Wst-bar_V = S^-1 Wst_W X-bar) from the other potential's intermediates of
+  // those orbitals, formed afresh per chunk, into the whole B1-bar (and
+  // Bri-bar); then B1-bar P2^T per block of aux functions
+  for (int which = 0; which < 2 && orbital_chunked; ++which) {
+    const IntegralsHandle& X = which == 0 ? W : V;
+    const IntegralsHandle& Y = which == 0 ? V : W;  // the other potential
+    const size_t M = X.n_df, MY = Y.n_df;
+    double* g3 = gJ3[which];
+    double* g3ri = gJ3ri[which];
+    const GradSink& s3 = out.sink3[which];
+    const GradSink& s3ri = out.sink3_ri[which];
+    const bool want3 = g3 || s3, want_ri = g3ri || s3ri;
+    if (!want3 && !want_ri) continue;
+    DevBuf Bb1(N * o_tot * M), Bbri;
+    Bb1.zero();  // the columns of spins without active orbitals stay zero
+    if (want_ri && a_tot) Bbri.alloc(R * a_tot * M);
+    budget = auto_budget_doubles(rq.mem_budget);
+    for (int s = 0; s < ns; ++s) {
+      const size_t o = sd[s].o, a = sd[s].a, c = sd[s].c;
+      if (!a) continue;
+      // B1-bar[:, k] = Ca B2-bar[:, k] over chunks of occupied k (written)
+      const size_t kc = std::max<size_t>(1, std::min(o, budget / 2 / per_k(s)));
+      for (size_t k0 = 0; k0 < o; k0 += kc) {
+        const size_t nk = std::min(kc, o - k0);
+        DevBuf B2y(a * nk * MY), B2b(a * nk * M);
+        {
+          DevBuf B1y;
+          b1_chunk(Y, s, k0, nk, B1y);
+          GemmDesc g3y = gemm_nn(LL(a), LL(nk * MY), LL(N), 1.0, Ca_s(s), LL(N), B1y.get(),
+                                 LL(N), 0.0, B2y.get(), LL(a));
+          g3y.a_kcontig = true;
+          gemm(g3y);
+        }
+        GemmDesc gb = gemm_nn(LL(a * nk), LL(M), LL(MY), 1.0, B2y.get(), LL(a * nk),
+                              tbar[s].get(), LL(MW), 0.0, B2b.get(), LL(a * nk));
+        gb.b_ncontig = which == 0;  // t-bar is MW x MV
+        gemm(gb);
+        GemmDesc g1 = gemm_nn(LL(N), LL(nk), LL(a), 1.0, Ca_s(s), LL(N), B2b.get(), LL(a), 0.0,
+                              Bb1.get() + N * (sd[s].ooff + k0), LL(N));
+        g1.nbo1 = LL(M);
+        g1.sBo1 = LL(a * nk);
+        g1.sCo1 = LL(N * o_tot);
+        gemm(g1);
+      }
+      // Wst-bar of active orbitals j: AO rows added to B1-bar[:, c + j], RI
+      // rows into Bri-bar[:, j]
+      const size_t jc = std::max<size_t>(1, std::min(a, budget / 2 / per_j));
+      for (size_t j0 = 0; j0 < a; j0 += jc) {
+        const size_t nj = std::min(jc, a - j0);
+        DevBuf SYj(Rp * nj * MY);
+        {
+          DevBuf Sy(Rp * nj * MY);
+          wst_chunk(Y, s, j0, nj, Sy.get());
+          gemm(gemm_nn(LL(Rp), LL(nj * MY), LL(Rp), 1.0, AB.Sinv.get(), LL(Rp), Sy.get(),
+                       LL(Rp), 0.0, SYj.get(), LL(Rp)));
+        }
+        DevBuf Wsb(Rp * nj * M);
+        GemmDesc gw = gemm_nn(LL(Rp * nj), LL(M), LL(MY), 1.0, SYj.get(), LL(Rp * nj),
+                              Xbar[s].get(), LL(MW), 0.0, Wsb.get(), LL(Rp * nj));
+        gw.b_ncontig = which == 0;  // X-bar is MW x MV
+        gemm(gw);
+        copy3d(Wsb.get(), LL(Rp), LL(Rp * nj), Bb1.get() + N * (sd[s].ooff + c + j0), LL(N),
+               LL(N * o_tot), LL(N), LL(nj), LL(M), 1.0, 1.0);
+        if (Bbri.size())
+          copy3d(Wsb.get() + N, LL(Rp), LL(Rp * nj), Bbri.get() + R * (sd[s].aoff + j0), LL(R),
+                 LL(R * a_tot), LL(R), LL(nj), LL(M));
+      }
+    }
+    if (want3) {
+      // per block of aux functions: B1-bar_0 = B1-bar P2^T (the block's
+      // columns), then per aux function the packed symmetric sum of B1-bar_0 Co^T
+      const size_t ac = std::max<size_t>(1, std::min(M, budget / (2 * N * N + N * o_tot)));
+      DevBuf Bb10(N * o_tot * ac), G(N * N * ac), Pk;
+      if (!g3) Pk.alloc(np * ac);  // one streamed block
+      for (size_t a0 = 0; a0 < M; a0 += ac) {
+        const size_t na = std::min(ac, M - a0);
+        GemmDesc gp = gemm_nn(LL(N * o_tot), LL(na), LL(M), 1.0, Bb1.get(), LL(N * o_tot),
+                              X.P2.get() + a0, LL(M), 0.0, Bb10.get(), LL(N * o_tot));
+        gp.b_ncontig = true;
+        gemm(gp);
+        GemmDesc g = gemm_nn(LL(N), LL(N), LL(o_tot), 1.0, Bb10.get(), LL(N), Co.get(), LL(N), 0.0,
+                             G.get(), LL(N));
+        g.b_ncontig = true;
+        g.nbo1 = LL(na);
+        g.sAo1 = LL(N * o_tot);
+        g.sCo1 = LL(N * N);
+        gemm(g);
+        pack_sym_sum(G.get(), LL(N), LL(na), g3 ? g3 + np * a0 : Pk.get(), LL(np));
+        if (!g3) s3(a0, na, Pk.get(), np, st);
+      }
+    }
+    if (want_ri) {
+      // as in the whole form: one batched GEMM into the whole gradient, or
+      // aux blocks of at most a quarter of the budget when streamed
+      const size_t rows = R * N;
+      const size_t step = g3ri ? M : std::max<size_t>(1, std::min(M, budget / (4 * rows)));
+      DevBuf Rk;
+      if (!g3ri) Rk.alloc(rows * step);
+      if (a_tot == 0) {
+        if (g3ri) {
+          UW12_CUDA(cudaMemsetAsync(g3ri, 0, R * N * M * sizeof(double), st));
+        } else {
+          Rk.zero();
+          for (size_t b0 = 0; b0 < M; b0 += step) s3ri(b0, std::min(step, M - b0), Rk.get(), rows, st);
+        }
+      } else {
+        DevBuf Bbri0(R * a_tot * M);
+        GemmDesc gp = gemm_nn(LL(R * a_tot), LL(M), LL(M), 1.0, Bbri.get(), LL(R * a_tot),
+                              X.P2.get(), LL(M), 0.0, Bbri0.get(), LL(R * a_tot));
+        gp.b_ncontig = true;
+        gemm(gp);
+        Bbri = DevBuf();
+        for (size_t b0 = 0; b0 < M; b0 += step) {
+          const size_t nb = std::min(step, M - b0);
+          GemmDesc g = gemm_nn(LL(R), LL(N), LL(a_tot), 1.0, Bbri0.get() + R * a_tot * b0, LL(R),
+                               Ca.get(), LL(N), 0.0, g3ri ? g3ri + rows * b0 : Rk.get(), LL(R));
+          g.b_ncontig = true;
+          g.nbo1 = LL(nb);
+          g.sAo1 = LL(R * a_tot);
+          g.sCo1 = LL(R * N);
+          gemm(g);
+          if (!g3ri) s3ri(b0, nb, Rk.get(), rows, st);
+        }
+      }
+    }
+  }
+  // ---- dE/dJ3_0 and dE/dJ3_ri_0 of W and V, whole intermediates
+  for (int which = 0; which < 2 && !orbital_chunked; ++which) {
     const IntegralsHandle& X = which == 0 ? W : V;
     const size_t M = X.n_df;
     double* g3 = gJ3[which];
