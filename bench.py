@@ -459,6 +459,29 @@ def batched_report(L, args, moduli):
         dt = (time.perf_counter() - t0) / args.batched_steps
         out[f"s_per_batch_{n_streams}_streams"] = dt
     ref = L.fock_batched(mols, indirect, True, args.s_os, args.s_ss, n_streams=1)
+    # split-K autotuner: one batch on one stream tunes every new GEMM class
+    # (timed, so not counted), then the batch runs from the table
+    L.autotune_clear()
+    L.autotune(L.AUTOTUNE_TUNE)
+    t0 = time.perf_counter()
+    L.fock_batched(mols, indirect, True, args.s_os, args.s_ss, n_streams=1)
+    torch.cuda.synchronize()
+    tune_s = time.perf_counter() - t0
+    L.autotune(L.AUTOTUNE_USE)
+    tuned = {"classes": L.autotune_size(), "tuning_batch_s": tune_s}
+    for n_streams in (1, 8):
+        L.fock_batched(mols, indirect, True, args.s_os, args.s_ss, n_streams=n_streams)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.batched_steps):
+            res = L.fock_batched(mols, indirect, True, args.s_os, args.s_ss, n_streams=n_streams)
+        torch.cuda.synchronize()
+        tuned[f"s_per_batch_{n_streams}_streams"] = (time.perf_counter() - t0) / args.batched_steps
+    tuned["max_energy_rel_diff_vs_rule"] = max(abs(r[0] - q[0]) / abs(q[0])
+                                               for r, q in zip(res, ref))
+    L.autotune(L.AUTOTUNE_OFF)
+    L.autotune_clear()
+    out["autotuned_split_k"] = tuned
     L.set_precision(moduli)
     L.fock_batched(mols, indirect, True, args.s_os, args.s_ss, n_streams=1)
     torch.cuda.synchronize()
@@ -509,6 +532,8 @@ def main():
                     help="skip the profiled pass (roofline and phase split)")
     ap.add_argument("--batched", action="store_true", help="add the 64-molecule batch")
     ap.add_argument("--batched-steps", type=int, default=2)
+    ap.add_argument("--batched-only", action="store_true",
+                    help="only the 64-molecule batch (FP64, autotuned split-K, split precision)")
     ap.add_argument("--gemm", default="",
                     help="instead of the workload: time one GEMM shape 'm,n,k[,beta]' on the "
                          "FP64 path and the split path with --moduli (kernel profiling probe)")
@@ -539,6 +564,10 @@ def main():
     L.lib()
     stream = torch.cuda.current_stream(device)
     L.set_stream(stream.cuda_stream)
+    if args.batched_only:
+        if rank == 0:
+            print(json.dumps({"batched": batched_report(L, args, args.moduli)}))
+        return
 
     w = workload_of(args)
     N, M, R, occ = w.n_ao, w.n_df, w.n_ri, list(w.n_occ)

@@ -343,6 +343,35 @@ int uw12c_dgemm_split(long long m, long long n, long long k, double alpha, const
  * library's stream, host producers' staging included). */
 int uw12c_profile_read_kind(int kind, unsigned long long* launches, double* ms, double* work);
 
+/* Split-K autotuner of the FP64 GEMM engine (no counterpart in libuw12, which
+ * leaves its BLAS to choose its own blocking).  The engine splits the
+ * contraction of a GEMM whose output has too few tiles to fill the GPU; by
+ * default a wave-occupancy rule picks the split.  mode 1 (tune): the first
+ * GEMM with beta = 0 and an automatic split of each shape class (output CTA
+ * count, power-of-two bucket of the k tiles over all reduction batches; output
+ * CTA counts of at least 8 waves never split) is launched once with each
+ * candidate split (1 .. 64, at least 4 k tiles per part), each timed on the
+ * library's stream, which synchronises it; the fastest is recorded and the
+ * GEMM's result is that of a launch with it.  mode 2 (use): the table's split
+ * for every class it has, the rule otherwise, no timing.  mode 0: the rule
+ * (default).  When path names an existing file (written by
+ * uw12c_autotune_save: a comment line, then "output_ctas k_tile_bucket split
+ * ms" per class) its classes are merged into the table first; a malformed file
+ * is UW12C_ERR_INVALID.  The table and the mode are process-wide and apply to
+ * every thread and device; tune on one device of the kind that will use the
+ * table, with one evaluation at a time (timings overlapped by other work are
+ * not representative).  Splits change the summation order only: results agree
+ * to rounding with the rule's.  uw12c_dgemm_noalloc and the int8 products of
+ * split precision do not use the table (GEMMs that split precision leaves in
+ * FP64 do). */
+int uw12c_autotune(int mode, const char* path);
+int uw12c_autotune_save(const char* path);
+int uw12c_autotune_clear(void);
+int uw12c_autotune_size(long long* n_classes);
+/* The table's split for a GEMM of this shape (0: its class is not in the table). */
+int uw12c_autotune_lookup(long long m, long long n, long long k, long long nbo, long long nbr,
+                          int* split);
+
 /* Deterministic synthetic three-index tensors written on the device (no
  * counterpart in libuw12; benchmark input generation).  Element e of the
  * stream (seed, tag) is the Box-Muller normal of two SplitMix64 draws, times

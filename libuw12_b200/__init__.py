@@ -126,6 +126,10 @@ def lib():
     L.uw12c_split_bits.argtypes = [ctypes.c_int, LL, ctypes.POINTER(ctypes.c_int)]
     L.uw12c_profile_read_kind.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong),
                                           ctypes.POINTER(c_d), ctypes.POINTER(c_d)]
+    L.uw12c_autotune.argtypes = [ctypes.c_int, ctypes.c_char_p]
+    L.uw12c_autotune_save.argtypes = [ctypes.c_char_p]
+    L.uw12c_autotune_size.argtypes = [ctypes.POINTER(LL)]
+    L.uw12c_autotune_lookup.argtypes = [LL, LL, LL, LL, LL, ctypes.POINTER(ctypes.c_int)]
     _lib = L
     return L
 
@@ -786,6 +790,39 @@ def split_bits(n_moduli: int, k_total: int) -> int:
     b = ctypes.c_int()
     _check(lib().uw12c_split_bits(int(n_moduli), int(k_total), ctypes.byref(b)))
     return b.value
+
+
+AUTOTUNE_OFF, AUTOTUNE_TUNE, AUTOTUNE_USE = 0, 1, 2
+
+
+def autotune(mode: int, path: Optional[str] = None):
+    """Split-K autotuner of the FP64 GEMM engine (``uw12c_autotune``): mode 0
+    the wave rule, 1 time every candidate split of each new shape class and
+    keep the fastest, 2 use the table only; ``path`` (a table written by
+    ``autotune_save``) is merged into the table first when it exists."""
+    _check(lib().uw12c_autotune(int(mode), os.fsencode(path) if path else None))
+
+
+def autotune_save(path: str):
+    _check(lib().uw12c_autotune_save(os.fsencode(path)))
+
+
+def autotune_clear():
+    _check(lib().uw12c_autotune_clear())
+
+
+def autotune_size() -> int:
+    n = ctypes.c_longlong()
+    _check(lib().uw12c_autotune_size(ctypes.byref(n)))
+    return n.value
+
+
+def autotune_lookup(m: int, n: int, k: int, nbo: int = 1, nbr: int = 1) -> int:
+    """The table's split for a GEMM of this shape (0: not in the table)."""
+    s = ctypes.c_int()
+    _check(lib().uw12c_autotune_lookup(int(m), int(n), int(k), int(nbo), int(nbr),
+                                       ctypes.byref(s)))
+    return s.value
 
 
 PROFILE_KINDS = ("dgemm", "split_gemm", "i8_mma", "split_prep", "split_crt", "producer")

@@ -886,6 +886,33 @@ int uw12c_profile_read_kind(int kind, unsigned long long* launches, double* ms, 
   });
 }
 
+int uw12c_autotune(int mode, const char* path) {
+  return guarded([&] { uw12b::autotune_set(mode, path); });
+}
+
+int uw12c_autotune_save(const char* path) {
+  return guarded([&] { uw12b::autotune_save(path); });
+}
+
+int uw12c_autotune_clear(void) {
+  return guarded([&] { uw12b::autotune_clear(); });
+}
+
+int uw12c_autotune_size(long long* n_classes) {
+  return guarded([&] {
+    need(n_classes != nullptr, "null output");
+    *n_classes = uw12b::autotune_size();
+  });
+}
+
+int uw12c_autotune_lookup(long long m, long long n, long long k, long long nbo, long long nbr,
+                          int* split) {
+  return guarded([&] {
+    need(split != nullptr, "null output");
+    *split = uw12b::autotune_lookup(m, n, k, nbo, nbr);
+  });
+}
+
 int uw12c_dgemm_noalloc(long long m, long long n, long long k, double alpha, const double* A,
                         long long lda, int a_kcontig, const double* B, long long ldb,
                         int b_ncontig, double beta, double* C, long long ldc, long long nbo1,

@@ -6,8 +6,10 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <map>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "gemm_f64.cuh"
 #include "ozaki.cuh"
@@ -550,6 +552,169 @@ void profile_record(int kind, cudaEvent_t a, cudaEvent_t b, double work, std::st
   g_prof_recs.push_back({a, b, work, std::move(shape), kind});
 }
 
+// ---- split-K autotuner ------------------------------------------------------
+//
+// choose_split's wave heuristic picks the split-K factor of a launch from its
+// output CTA count alone.  The autotuner replaces it by measurement: a shape
+// class is (output CTAs = tiles x output batches, power-of-two bucket of the
+// k tiles over all reduction batches); in tuning mode the first automatic-split
+// GEMM of a class not yet in the table is launched once with every candidate
+// split (1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64 while each CTA keeps >= 4 k
+// tiles), each timed with CUDA events on the current stream, and the fastest
+// is recorded and launched last, so C holds its result.  Only GEMMs with
+// beta = 0 are tuned (their repeated launches overwrite C); the others, and
+// every GEMM in "use" mode, take the table's split for their class when it has
+// one and the heuristic otherwise.  Output CTA counts of at least 8 waves never
+// split and are not tuned.
+namespace {
+struct TuneKey {
+  long long ctas;
+  int kbucket;
+  bool operator<(const TuneKey& o) const {
+    return ctas != o.ctas ? ctas < o.ctas : kbucket < o.kbucket;
+  }
+};
+struct TuneEntry {
+  int split;
+  double ms;
+};
+std::mutex g_tune_mu;
+int g_tune_mode = 0;  // 0 off, 1 tune, 2 use
+std::map<TuneKey, TuneEntry> g_tune;
+
+int kbucket_of(long long ktiles_total) {
+  int b = 0;
+  while ((1LL << (b + 1)) <= ktiles_total) ++b;
+  return b;
+}
+
+TuneKey tune_key(long long m, long long n, long long k, long long nbo, long long nbr) {
+  const long long tiles = ((m + BM - 1) / BM) * ((n + BN - 1) / BN);
+  return TuneKey{tiles * nbo, kbucket_of(((k + BK - 1) / BK) * nbr)};
+}
+
+// the table's split for p's class, or 0
+int tuned_split(const KParams& p) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  if (g_tune_mode == 0) return 0;
+  auto it = g_tune.find(TuneKey{p.tiles_mn * p.nbo, kbucket_of(p.ktiles_total)});
+  return it == g_tune.end() ? 0 : it->second.split;
+}
+
+bool tuning_wanted(const GemmDesc& d, const KParams& p) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  if (g_tune_mode != 1 || d.split > 0 || d.beta != 0.0) return false;
+  if (p.tiles_mn * p.nbo >= 8 * kSMs) return false;
+  return g_tune.find(TuneKey{p.tiles_mn * p.nbo, kbucket_of(p.ktiles_total)}) == g_tune.end();
+}
+
+// Times every candidate split of d (beta = 0) on stream s, records the fastest
+// for the class and leaves C with the result of a launch with it.
+void tune_and_launch(const GemmDesc& d, KParams p, cudaStream_t s) {
+  std::vector<int> cands;
+  for (int c : {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64})
+    if (c == 1 || p.ktiles_total / c >= 4) cands.push_back(c);
+  const int heuristic = choose_split(p.tiles_mn * p.nbo, p.ktiles_total);
+  if (std::find(cands.begin(), cands.end(), heuristic) == cands.end()) cands.push_back(heuristic);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  UW12_CUDA(cudaEventCreate(&e0));
+  UW12_CUDA(cudaEventCreate(&e1));
+  int best = heuristic;
+  double best_ms = 1e300;
+  for (int c : cands) {
+    p.split = c;
+    DevBuf work;
+    if (c > 1) {
+      work.alloc(static_cast<size_t>(c) * p.nbo * d.m * d.n, s);
+      p.work = work.get();
+    }
+    launch(d, p, s);  // warm-up (caches, first-launch set-up)
+    UW12_CUDA(cudaEventRecord(e0, s));
+    launch(d, p, s);
+    launch(d, p, s);
+    UW12_CUDA(cudaEventRecord(e1, s));
+    UW12_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    UW12_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms / 2.0 < best_ms) {
+      best_ms = ms / 2.0;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[TuneKey{p.tiles_mn * p.nbo, kbucket_of(p.ktiles_total)}] = TuneEntry{best, best_ms};
+  }
+  p.split = best;
+  DevBuf work;
+  if (best > 1) {
+    work.alloc(static_cast<size_t>(best) * p.nbo * d.m * d.n, s);
+    p.work = work.get();
+  }
+  launch(d, p, s);
+}
+}  // namespace
+
+void autotune_set(int mode, const char* path) {
+  if (mode < 0 || mode > 2) throw Error(kErrInvalid, "autotune: mode must be 0, 1 or 2");
+  std::map<TuneKey, TuneEntry> loaded;
+  if (path && *path) {
+    if (FILE* f = std::fopen(path, "r")) {
+      char line[256];
+      int lineno = 0;
+      while (std::fgets(line, sizeof(line), f)) {
+        ++lineno;
+        if (line[0] == '#' || line[0] == '\n') continue;
+        long long ctas = 0;
+        int kb = 0, split = 0;
+        double ms = 0.0;
+        if (std::sscanf(line, "%lld %d %d %lf", &ctas, &kb, &split, &ms) != 4 || ctas <= 0 ||
+            kb < 0 || kb > 62 || split < 1 || split > 64) {
+          std::fclose(f);
+          throw Error(kErrInvalid, std::string("autotune: malformed line ") +
+                                       std::to_string(lineno) + " in " + path);
+        }
+        loaded[TuneKey{ctas, kb}] = TuneEntry{split, ms};
+      }
+      std::fclose(f);
+    }
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (const auto& kv : loaded) g_tune[kv.first] = kv.second;
+  g_tune_mode = mode;
+}
+
+void autotune_save(const char* path) {
+  if (!path || !*path) throw Error(kErrInvalid, "autotune: no path");
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  FILE* f = std::fopen(path, "w");
+  if (!f) throw Error(kErrInvalid, std::string("autotune: cannot write ") + path);
+  std::fprintf(f, "# output_ctas k_tile_bucket split ms\n");
+  for (const auto& kv : g_tune)
+    std::fprintf(f, "%lld %d %d %.6f\n", kv.first.ctas, kv.first.kbucket, kv.second.split,
+                 kv.second.ms);
+  std::fclose(f);
+}
+
+void autotune_clear() {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune.clear();
+}
+
+long long autotune_size() {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  return static_cast<long long>(g_tune.size());
+}
+
+int autotune_lookup(long long m, long long n, long long k, long long nbo, long long nbr) {
+  if (m <= 0 || n <= 0 || k <= 0 || nbo <= 0 || nbr <= 0) return 0;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(tune_key(m, n, k, nbo, nbr));
+  return it == g_tune.end() ? 0 : it->second.split;
+}
+
 void gemm(const GemmDesc& d) {
   const int L = split_moduli();
   if (L > 0) {
@@ -573,13 +738,21 @@ void gemm_dmma(const GemmDesc& d) {
     launch_scale_only(d, s);
     return;
   }
+  const bool prof = profile_enabled();
+  if (d.split <= 0) {
+    if (!prof && tuning_wanted(d, p)) {
+      tune_and_launch(d, p, s);
+      return;
+    }
+    if (const int t = tuned_split(p))
+      p.split = static_cast<int>(std::min<long long>(t, p.ktiles_total));
+  }
   DevBuf work;
   if (p.split > 1) {
     work.alloc(static_cast<size_t>(p.split) * p.nbo * d.m * d.n, s);
     p.work = work.get();
   }
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;
-  const bool prof = profile_enabled();
   if (prof) {
     UW12_CUDA(cudaEventCreate(&ev_a));
     UW12_CUDA(cudaEventCreate(&ev_b));

@@ -60,6 +60,21 @@ void gemm_dmma(const GemmDesc& d);
 constexpr long long kNoAllocScratchDoubles = 1LL << 21;
 void gemm_noalloc(const GemmDesc& d);
 
+// Split-K autotuner of gemm_dmma (off by default).  Mode 0: the wave
+// heuristic; 1: tune -- the first automatic-split GEMM with beta = 0 of a shape
+// class (output CTAs, power-of-two bucket of the k tiles) not yet in the table
+// is timed with every candidate split and the fastest recorded; 2: use the
+// table only.  In modes 1 and 2 automatic splits come from the table when it
+// has the class.  autotune_set also merges a table saved by autotune_save
+// (text, one "output_ctas k_tile_bucket split ms" line per class) when `path`
+// names an existing file; a malformed file throws.  The table is process-wide.
+void autotune_set(int mode, const char* path);
+void autotune_save(const char* path);
+void autotune_clear();
+long long autotune_size();
+// the table's split for a GEMM of this shape (0: the class is not in it)
+int autotune_lookup(long long m, long long n, long long k, long long nbo, long long nbr);
+
 // Convenience wrappers in BLAS terms (column-major, 'N'/'T').
 inline GemmDesc gemm_nn(long long m, long long n, long long k, double alpha, const double* A,
                         long long lda, const double* B, long long ldb, double beta, double* C,
