@@ -350,7 +350,8 @@ int uw12c_profile_read_kind(int kind, unsigned long long* launches, double* ms, 
  * GEMM with beta = 0 and an automatic split of each shape class (output CTA
  * count, power-of-two bucket of the k tiles over all reduction batches; output
  * CTA counts of at least 8 waves never split) is launched once with each
- * candidate split (1 .. 64, at least 4 k tiles per part), each timed on the
+ * candidate split (1 .. 64, at least 4 k tiles per part, split-K partials
+ * within 256 MiB or the rule's own), each timed on the
  * library's stream, which synchronises it; the fastest is recorded and the
  * GEMM's result is that of a launch with it.  mode 2 (use): the table's split
  * for every class it has, the rule otherwise, no timing.  mode 0: the rule

@@ -560,7 +560,7 @@ void profile_record(int kind, cudaEvent_t a, cudaEvent_t b, double work, std::st
 // k tiles over all reduction batches); in tuning mode the first automatic-split
 // GEMM of a class not yet in the table is launched once with every candidate
 // split (1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64 while each CTA keeps >= 4 k
-// tiles), each timed with CUDA events on the current stream, and the fastest
+// tiles and the partial tiles stay within 256 MiB or the rule's), each timed with CUDA events on the current stream, and the fastest
 // is recorded and launched last, so C holds its result.  Only GEMMs with
 // beta = 0 are tuned (their repeated launches overwrite C); the others, and
 // every GEMM in "use" mode, take the table's split for their class when it has
@@ -611,10 +611,14 @@ bool tuning_wanted(const GemmDesc& d, const KParams& p) {
 // Times every candidate split of d (beta = 0) on stream s, records the fastest
 // for the class and leaves C with the result of a launch with it.
 void tune_and_launch(const GemmDesc& d, KParams p, cudaStream_t s) {
+  const int heuristic = choose_split(p.tiles_mn * p.nbo, p.ktiles_total);
+  // a candidate's partial tiles stay within 2^25 doubles (256 MiB) or the
+  // rule's own, so tuning needs no more memory than the evaluation around it
+  const double per_split = double(p.nbo) * double(d.m) * double(d.n);
+  const double cap = std::max(double(1LL << 25), per_split * heuristic);
   std::vector<int> cands;
   for (int c : {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64})
-    if (c == 1 || p.ktiles_total / c >= 4) cands.push_back(c);
-  const int heuristic = choose_split(p.tiles_mn * p.nbo, p.ktiles_total);
+    if (c == 1 || (p.ktiles_total / c >= 4 && per_split * c <= cap)) cands.push_back(c);
   if (std::find(cands.begin(), cands.end(), heuristic) == cands.end()) cands.push_back(heuristic);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   UW12_CUDA(cudaEventCreate(&e0));
