@@ -7,14 +7,21 @@ checker for the CUDA path: only ``tests/``, ``__graft_entry__.smoke()`` and the
 ``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` may import it.  The
 product (``libuw12_b200``) never calls it and has no CPU fallback.
 
-Parity pinning.  libuw12 itself cannot be built here (it needs Armadillo or
-Eigen, BLAS/LAPACK and a CMake-generated ``config.hpp``) and its only absolute
-golden (the water fixture, ``tests/test_water.cpp``) lacks the RI tensors
-(``W3_ri.csv``/``V3_ri.csv`` are not shipped).  The totals are therefore
-"parity unpinned" against absolute goldens; the oracle is pinned instead
-against the reference's own known-answer and invariant tests (spin factors,
-square/lower, os+ss linearity, open==closed shell, W<->V symmetry, zero
-cases, analytic Fock == finite-difference dE/dD), see ``tests/test_oracle.py``.
+Parity pinning.  The oracle is pinned to libuw12 itself: ``oracle/ref.mk``
+compiles libuw12's unmodified sources (over this project's Armadillo-subset
+header, ``oracle/refshim/``) into ``oracle/_ref/libuw12_ref.so``, and
+``tests/golden/make_golden.py`` records that build's energies, per-term
+energies, Fock matrices, ABS+ projector blocks at the eigenvalue drop
+threshold and exception classes/messages in ``tests/golden/`` (with the
+SHA-256 of every reference source it compiled).  ``tests/test_reference_goldens.py``
+checks this module against every golden (tolerances 1e-12 relative on
+well-conditioned inputs and 1e-9 on the workload generators, whose metrics
+have condition numbers near 1e6; observed 1e-15 and 3e-11 to 6e-11).  The oracle is also checked against the reference's own
+known-answer and invariant tests (spin factors, square/lower, os+ss
+linearity, open==closed shell, W<->V symmetry, zero cases, analytic Fock ==
+finite-difference dE/dD) in ``tests/test_oracle.py``.  libuw12's one absolute
+golden, the water fixture (``tests/test_water.cpp``), cannot run: its RI
+tensors (``W3_ri.csv``/``V3_ri.csv``) are not shipped.
 
 Layout conventions follow Armadillo: matrices are column-major, every
 ``reshape`` reinterprets a column-major buffer (``order='F'``), packed
