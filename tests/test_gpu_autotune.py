@@ -8,8 +8,7 @@
   reloaded table: energy, terms and Fock agree with the rule's evaluation to
   1e-12 (relative to the magnitude of the run without the exchange term,
   which the same-spin terms cancel against) and with the oracle at the parity
-  tolerances; "use" runs from the same
-  table are identical.
+  tolerances; "use" runs from the same table are identical.
 """
 import numpy as np
 import pytest
