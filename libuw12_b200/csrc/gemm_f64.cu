@@ -620,9 +620,16 @@ void tune_and_launch(const GemmDesc& d, KParams p, cudaStream_t s) {
   for (int c : {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64})
     if (c == 1 || (p.ktiles_total / c >= 4 && per_split * c <= cap)) cands.push_back(c);
   if (std::find(cands.begin(), cands.end(), heuristic) == cands.end()) cands.push_back(heuristic);
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  UW12_CUDA(cudaEventCreate(&e0));
-  UW12_CUDA(cudaEventCreate(&e1));
+  struct Events {  // destroyed on every exit, a failed launch included
+    cudaEvent_t a = nullptr, b = nullptr;
+    ~Events() {
+      if (a) cudaEventDestroy(a);
+      if (b) cudaEventDestroy(b);
+    }
+  } ev;
+  UW12_CUDA(cudaEventCreate(&ev.a));
+  UW12_CUDA(cudaEventCreate(&ev.b));
+  cudaEvent_t e0 = ev.a, e1 = ev.b;
   int best = heuristic;
   double best_ms = 1e300;
   for (int c : cands) {
@@ -645,8 +652,6 @@ void tune_and_launch(const GemmDesc& d, KParams p, cudaStream_t s) {
       best = c;
     }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[TuneKey{p.tiles_mn * p.nbo, kbucket_of(p.ktiles_total)}] = TuneEntry{best, best_ms};
