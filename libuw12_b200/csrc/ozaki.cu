@@ -1129,9 +1129,12 @@ constexpr size_t kMmaSmem =
 long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
 
 int num_sms() {
-  static int n[64] = {};
+  static int n[kMaxDevices] = {};
+  static std::mutex mu;
   int dev = 0;
   UW12_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) throw Error(kErrInvalid, "device index out of range");
+  std::lock_guard<std::mutex> lk(mu);
   if (!n[dev]) UW12_CUDA(cudaDeviceGetAttribute(&n[dev], cudaDevAttrMultiProcessorCount, dev));
   return n[dev];
 }
