@@ -780,6 +780,37 @@ def set_precision(n_moduli: int):
     _check(lib().uw12c_set_precision(int(n_moduli)))
 
 
+def form_fock_split(W: BaseIntegrals, V: BaseIntegrals, WV: BaseIntegrals,
+                    abs_p: ABSProjectors, orbitals: Sequence[np.ndarray],
+                    occupations: Sequence[np.ndarray], n_active: Sequence[int],
+                    indirect_term: bool, calculate_fock: bool, scale_opp_spin: float,
+                    scale_same_spin: float, n_moduli: int = 14):
+    """``form_fock`` in split precision (``n_moduli`` moduli) with the error of
+    its result against the FP64 evaluation stated in Hartree.
+
+    Returns ``(energy, fock, (E2, E3, E4), errors)`` where ``errors`` holds
+    ``energy_Eh`` = |E_split - E_FP64|, ``terms_Eh`` (the same per term),
+    ``fock_max_Eh`` = max |F_split - F_FP64| over both spins (None without
+    Fock) and ``n_moduli``.  The FP64 result is the plain GPU path on the same
+    handles (libuw12's arithmetic in FP64), so the call costs one evaluation of
+    each kind.  The calling thread is left in FP64 mode (precision 0).
+    """
+    args = (W, V, WV, abs_p, orbitals, occupations, n_active, indirect_term, calculate_fock,
+            scale_opp_spin, scale_same_spin)
+    set_precision(n_moduli)
+    try:
+        e, f, t = form_fock(*args)
+    finally:
+        set_precision(0)
+    e64, f64, t64 = form_fock(*args)
+    errors = {"energy_Eh": abs(e - e64),
+              "terms_Eh": tuple(abs(a - b) for a, b in zip(t, t64)),
+              "fock_max_Eh": (max(float(np.max(np.abs(a - b))) for a, b in zip(f, f64))
+                              if f is not None else None),
+              "n_moduli": int(n_moduli)}
+    return e, f, t, errors
+
+
 def set_split_threshold(min_flops: float):
     """GEMMs below ``min_flops`` stay FP64 in split-precision mode (default 2e9)."""
     _check(lib().uw12c_set_split_threshold(float(min_flops)))
